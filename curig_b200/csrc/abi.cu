@@ -1,0 +1,294 @@
+// Exported entry points of libcurafft.so: the reference's C ABI
+// (src/astro/cugridder.cu:330-612), the multi-channel / FP32 one-shot calls,
+// the device-pointer plan API and the C++ gridder_* mirror.
+#include "plan.h"
+
+#include "../../include/curig.h"
+#include "../../include/cugridder.h"
+
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+
+using namespace curig;
+
+static thread_local std::string g_last_error;
+
+static int fail(int code, const std::string &msg) {
+    g_last_error = msg;
+    return code;
+}
+
+static Options to_options(const curig_opts *o) {
+    Options opt;
+    if (o) {
+        opt.precision = o->precision;
+        opt.window = o->window;
+        opt.bin_xy = o->bin_xy;
+        opt.sub = o->sub;
+        opt.smem_budget = o->smem_budget > 0 ? (size_t)o->smem_budget : 0;
+        opt.stream = (cudaStream_t)o->stream;
+    }
+    return opt;
+}
+
+extern "C" void curig_default_opts(curig_opts *o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+}
+
+extern "C" const char *curig_last_error(void) { return g_last_error.c_str(); }
+
+// One call with host buffers: allocate, copy in, plan, execute, copy out, free
+// (the reference's ms2dirty_exec / dirty2ms_exec life cycle, cugridder.cu:330-582).
+static int oneshot(int type, long long nrow, int nchan, int nx, int ny, double psx, double psy,
+                   const double *freq, const double *uvw, void *vis, const void *wgt, void *dirty,
+                   double eps, double sigma, int sign, const curig_opts *opts) {
+    if (nrow < 0 || nchan <= 0 || nx <= 0 || ny <= 0 || !freq || !dirty || (nrow > 0 && (!uvw || !vis)))
+        return fail(ERR_ARG, "invalid argument");
+    if (nrow == 0) {                      // no visibilities: empty sum / nothing to degrid
+        if (type == 1) std::memset(dirty, 0, (size_t)nx * ny * 2 * (opts && opts->precision ? 4 : 8));
+        return OK;
+    }
+    Options opt = to_options(opts);
+    cudaStream_t st = opt.stream ? opt.stream : cudaStreamPerThread;
+    opt.stream = st;
+    const size_t rs = opt.precision ? 4 : 8, cs = 2 * rs;
+    const size_t M = (size_t)nrow * nchan, npix = (size_t)nx * ny;
+    double *d_uvw = nullptr;
+    void *d_vis = nullptr, *d_wgt = nullptr, *d_dirty = nullptr;
+    Plan *p = nullptr;
+    int s = OK;
+    auto chk = [&](cudaError_t e) {
+        if (e != cudaSuccess && s == OK) {
+            s = e == cudaErrorMemoryAllocation ? ERR_NOMEM : ERR_CUDA;
+            g_last_error = cudaGetErrorString(e);
+        }
+        return s == OK;
+    };
+    if (chk(cudaMallocAsync((void **)&d_uvw, 3 * nrow * sizeof(double), st)) &&
+        chk(cudaMallocAsync(&d_vis, M * cs, st)) &&
+        (!wgt || chk(cudaMallocAsync(&d_wgt, M * rs, st))) &&
+        chk(cudaMallocAsync(&d_dirty, npix * cs, st)) &&
+        chk(cudaMemcpyAsync(d_uvw, uvw, 3 * nrow * sizeof(double), cudaMemcpyHostToDevice, st)) &&
+        (type != 1 || chk(cudaMemcpyAsync(d_vis, vis, M * cs, cudaMemcpyHostToDevice, st))) &&
+        (!wgt || chk(cudaMemcpyAsync(d_wgt, wgt, M * rs, cudaMemcpyHostToDevice, st))) &&
+        (type != 2 || chk(cudaMemcpyAsync(d_dirty, dirty, npix * cs, cudaMemcpyHostToDevice, st)))) {
+        s = plan_create(type, nx, ny, psx, psy, eps, sigma, sign, opt, &p);
+        if (s == OK) s = plan_setpts(p, nrow, nchan, d_uvw, d_uvw + 1, d_uvw + 2, 3, freq);
+        if (s == OK) s = plan_execute(p, d_vis, d_wgt, d_dirty);
+        if (s == OK) {
+            if (type == 1) chk(cudaMemcpyAsync(dirty, d_dirty, npix * cs, cudaMemcpyDeviceToHost, st));
+            else chk(cudaMemcpyAsync(vis, d_vis, M * cs, cudaMemcpyDeviceToHost, st));
+        }
+        if (p && s != OK && !p->last_error.empty()) g_last_error = p->last_error;
+        if (p) plan_destroy(p);
+    }
+    if (d_uvw) cudaFreeAsync(d_uvw, st);
+    if (d_vis) cudaFreeAsync(d_vis, st);
+    if (d_wgt) cudaFreeAsync(d_wgt, st);
+    if (d_dirty) cudaFreeAsync(d_dirty, st);
+    chk(cudaStreamSynchronize(st));
+    return s;
+}
+
+static void ref_pixsizes(double fov, int nx, int ny, double &psx, double &psy) {
+    const double PI = PI_D;                       // (PCS)M_PI, include/utils.h:97
+    psx = fov / 180.0 * PI / (double)nx;          // cugridder.cu:48
+    psy = fov / 180.0 * PI / (double)ny;          // cugridder.cu:49
+}
+
+extern "C" int ms2dirty_2(int nrow, int nxdirty, int nydirty, double fov, double freq, double *uvw,
+                          curig_cdouble *vis, double *wgt, curig_cdouble *dirty, double epsilon,
+                          double sigma, int sign) {
+    double psx, psy;
+    ref_pixsizes(fov, nxdirty, nydirty, psx, psy);
+    return oneshot(1, nrow, 1, nxdirty, nydirty, psx, psy, &freq, uvw, vis, wgt, dirty, epsilon, sigma,
+                   sign, nullptr);
+}
+
+extern "C" int ms2dirty_1(int nrow, int nxdirty, int nydirty, double fov, double freq, double *uvw,
+                          curig_cdouble *vis, curig_cdouble *dirty, double epsilon, double sigma,
+                          int sign) {
+    return ms2dirty_2(nrow, nxdirty, nydirty, fov, freq, uvw, vis, nullptr, dirty, epsilon, sigma, sign);
+}
+
+extern "C" int dirty2ms_2(int nrow, int nxdirty, int nydirty, double fov, double freq, double *uvw,
+                          curig_cdouble *vis, double *wgt, curig_cdouble *dirty, double epsilon,
+                          double sigma, int sign) {
+    double psx, psy;
+    ref_pixsizes(fov, nxdirty, nydirty, psx, psy);
+    return oneshot(2, nrow, 1, nxdirty, nydirty, psx, psy, &freq, uvw, vis, wgt, dirty, epsilon, sigma,
+                   sign, nullptr);
+}
+
+extern "C" int dirty2ms_1(int nrow, int nxdirty, int nydirty, double fov, double freq, double *uvw,
+                          curig_cdouble *vis, curig_cdouble *dirty, double epsilon, double sigma,
+                          int sign) {
+    return dirty2ms_2(nrow, nxdirty, nydirty, fov, freq, uvw, vis, nullptr, dirty, epsilon, sigma, sign);
+}
+
+extern "C" int curig_ms2dirty(int64_t nrow, int nchan, int nx, int ny, double psx, double psy,
+                              const double *freq, const double *uvw, const void *vis, const void *wgt,
+                              void *dirty, double eps, double sigma, int sign, const curig_opts *opts) {
+    return oneshot(1, nrow, nchan, nx, ny, psx, psy, freq, uvw, const_cast<void *>(vis), wgt, dirty, eps,
+                   sigma, sign, opts);
+}
+
+extern "C" int curig_dirty2ms(int64_t nrow, int nchan, int nx, int ny, double psx, double psy,
+                              const double *freq, const double *uvw, void *vis, const void *wgt,
+                              const void *dirty, double eps, double sigma, int sign,
+                              const curig_opts *opts) {
+    return oneshot(2, nrow, nchan, nx, ny, psx, psy, freq, uvw, vis, wgt, const_cast<void *>(dirty), eps,
+                   sigma, sign, opts);
+}
+
+// ------------------------------------------------------------------ plan API
+struct curig_plan_s {
+    Plan *p;
+};
+
+extern "C" int curig_makeplan(int type, int nx, int ny, double psx, double psy, double eps, double sigma,
+                              int sign, const curig_opts *opts, curig_plan *out) {
+    if (!out) return fail(ERR_ARG, "null plan pointer");
+    *out = nullptr;
+    Plan *p = nullptr;
+    int s = plan_create(type, nx, ny, psx, psy, eps, sigma, sign, to_options(opts), &p);
+    if (s != OK) return fail(s, "plan creation failed");
+    *out = new curig_plan_s{p};
+    return OK;
+}
+
+extern "C" int curig_setpts_uvw(curig_plan h, int64_t nrow, int nchan, const double *du, const double *dv,
+                                const double *dw, int stride, const double *freq) {
+    if (!h) return fail(ERR_ARG, "null plan");
+    int s = plan_setpts(h->p, nrow, nchan, du, dv, dw, stride, freq);
+    if (s != OK) return fail(s, h->p->last_error.empty() ? "setpts failed" : h->p->last_error);
+    return OK;
+}
+
+extern "C" int curig_setpts(curig_plan h, int64_t nrow, int nchan, const double *d_uvw, const double *freq) {
+    if (!d_uvw) return fail(ERR_ARG, "null uvw");
+    return curig_setpts_uvw(h, nrow, nchan, d_uvw, d_uvw + 1, d_uvw + 2, 3, freq);
+}
+
+extern "C" int curig_execute(curig_plan h, void *d_vis, const void *d_wgt, void *d_dirty) {
+    if (!h) return fail(ERR_ARG, "null plan");
+    int s = plan_execute(h->p, d_vis, d_wgt, d_dirty);
+    if (s != OK) return fail(s, h->p->last_error.empty() ? "execute failed" : h->p->last_error);
+    return OK;
+}
+
+extern "C" int curig_destroy(curig_plan h) {
+    if (!h) return OK;
+    plan_destroy(h->p);
+    delete h;
+    return OK;
+}
+
+extern "C" int curig_plan_info(curig_plan h, int *info, double *dinfo) {
+    if (!h || !h->p->ready) return fail(ERR_ARG, "plan has no points");
+    const Plan *p = h->p;
+    if (info) {
+        info[0] = p->gp.nf1; info[1] = p->gp.nf2; info[2] = p->gp.nf3; info[3] = p->gp.kp.kw;
+        info[4] = p->tg.bx; info[5] = p->tg.bz; info[6] = (int)p->tg.nbins(); info[7] = p->win.kind;
+    }
+    if (dinfo) {
+        dinfo[0] = p->gp.kp.beta; dinfo[1] = p->gp.gamma; dinfo[2] = p->gp.h;
+        dinfo[3] = p->gp.i_center; dinfo[4] = p->gp.i_half; dinfo[5] = p->gp.o_center;
+    }
+    return OK;
+}
+
+extern "C" int curig_set_window(int kw, int degree, const double *coef, double eps_reached) {
+    int s = registry_set_window(kw, degree, coef, eps_reached);
+    return s == OK ? OK : fail(s, "invalid window table");
+}
+
+extern "C" void curig_clear_windows(void) { registry_clear(); }
+
+extern "C" int curig_grid_params(int nx, int ny, double psx, double psy, double wmin, double wmax,
+                                 double eps, double sigma, int *iout, double *dout) {
+    GridParams gp;
+    int s = grid_params(nx, ny, psx, psy, wmin, wmax, eps, sigma, 1, gp);
+    if (s != OK) return fail(s, "invalid grid parameters");
+    if (iout) { iout[0] = gp.nf1; iout[1] = gp.nf2; iout[2] = gp.nf3; iout[3] = gp.kp.kw; }
+    if (dout) {
+        dout[0] = gp.kp.beta; dout[1] = gp.gamma; dout[2] = gp.h;
+        dout[3] = gp.i_center; dout[4] = gp.i_half; dout[5] = gp.o_center;
+    }
+    return OK;
+}
+
+extern "C" int curig_psi_hat(int nf, double eps, double sigma, double *out) {
+    KernelParams kp;
+    int s = setup_kernel(eps, sigma, kp);
+    if (s != OK) return fail(s, "invalid kernel parameters");
+    if (nf < 2 || !out) return fail(ERR_ARG, "invalid argument");
+    std::vector<double> v;
+    psi_hat_grid(nf, kp, Window(), v);
+    std::memcpy(out, v.data(), v.size() * sizeof(double));
+    return OK;
+}
+
+// ------------------------------------------------------------------ C++ gridder_* mirror
+int gridder_setting(int N1, int N2, int method, int kerevalmeth, int w_term_method, double tol,
+                    int direction, double sigma, int iflag, int batchsize, int M, int channel,
+                    double fov, visibility *pv, double *d_u, double *d_v, double *d_w,
+                    cuDoubleComplex *d_c, curafft_plan *plan, ragridder_plan *gplan) {
+    (void)kerevalmeth; (void)iflag; (void)batchsize;
+    if (!plan || !gplan || !pv || !pv->frequency || M <= 0) return ERR_ARG;
+    if (method != 0 || w_term_method != 1) return ERR_UNSUPPORTED;
+    double psx, psy;
+    ref_pixsizes(fov, N2, N1, psx, psy);
+    Options opt;
+    Plan *p = nullptr;
+    int s = plan_create(direction == 1 ? 1 : 2, N2, N1, psx, psy, tol, sigma, pv->sign, opt, &p);
+    if (s != OK) return s;
+    s = plan_setpts(p, M, 1, d_u, d_v, d_w, 1, pv->frequency);
+    if (s != OK) { plan_destroy(p); return s; }
+    plan->impl = p;
+    plan->d_c = d_c; plan->d_u = d_u; plan->d_v = d_v; plan->d_w = d_w;
+    plan->dim = 3; plan->type = direction == 1 ? 1 : 2; plan->M = M;
+    plan->nf1 = p->gp.nf1; plan->nf2 = p->gp.nf2; plan->nf3 = p->gp.nf3;
+    plan->ms = N1; plan->mt = N2; plan->mu = 1;
+    plan->iflag = direction == 1 ? 1 : -1; plan->batchsize = p->gp.nf3; plan->direction = direction;
+    gplan->kv = *pv;
+    gplan->fov = fov; gplan->pixelsize_x = psx; gplan->pixelsize_y = psy;
+    gplan->num_w = p->gp.nf3; gplan->width = N1; gplan->height = N2;
+    gplan->channel = channel; gplan->nrow = M; gplan->w_term_method = w_term_method;
+    gplan->speedoflight = 299792458;
+    return OK;
+}
+
+int gridder_execution(curafft_plan *plan, ragridder_plan *gplan) {
+    if (!plan || !plan->impl || !plan->fk || !plan->d_c) return ERR_ARG;
+    Plan *p = static_cast<Plan *>(plan->impl);
+    double *d_wgt = nullptr;
+    if (gplan && gplan->kv.weight) {               // ra_exec.cu:98-104 uploads per call
+        if (cudaMallocAsync((void **)&d_wgt, (size_t)p->nrow * sizeof(double), p->st) != cudaSuccess)
+            return ERR_NOMEM;
+        cudaMemcpyAsync(d_wgt, gplan->kv.weight, (size_t)p->nrow * sizeof(double), cudaMemcpyHostToDevice,
+                        p->st);
+    }
+    int s = plan_execute(p, plan->d_c, d_wgt, plan->fk);
+    if (d_wgt) cudaFreeAsync(d_wgt, p->st);
+    if (cudaStreamSynchronize(p->st) != cudaSuccess && s == OK) s = ERR_CUDA;
+    return s;
+}
+
+int gridder_destroy(curafft_plan *plan, ragridder_plan *gplan) {
+    if (plan && plan->impl) {
+        plan_destroy(static_cast<Plan *>(plan->impl));
+        plan->impl = nullptr;
+    }
+    if (gplan) {                                   // cugridder.cu:297-303
+        free(gplan->dirty_image); gplan->dirty_image = nullptr;
+        free(gplan->kv.u); free(gplan->kv.v); free(gplan->kv.w); free(gplan->kv.vis);
+        free(gplan->kv.frequency); free(gplan->kv.weight);
+        gplan->kv.u = gplan->kv.v = gplan->kv.w = nullptr;
+        gplan->kv.vis = nullptr; gplan->kv.frequency = nullptr; gplan->kv.weight = nullptr;
+    }
+    return OK;
+}

@@ -1,0 +1,749 @@
+// CUDA kernels of the B200 gridder (sm_100a).
+//
+// Replaces, on the ms2dirty / dirty2ms path of the reference:
+//   get_effective_coordinate + rescaling + pre_stage_1/2 + transpose
+//       (precomp.cu:48-79, utils.cu:56-154, cuft.cu:19-92)  -> k_bin_count / k_bin_scatter / k_vis_prep
+//   conv_3d_nputsdriven (conv.cu:144-228)                  -> k_spread (tile-binned)
+//   interp_3d_nputsdriven (interp.cu:143-227)              -> k_interp (tile-staged)
+//   w_term_dft + deconv_2d + w_term_deconv + div_n_lm
+//       (cuft.cu:520-572, deconv.cu:236-417, ra_exec.cu:22-52) -> k_correct_m2d (one pass)
+//   div_n_lm + w_term_deconv + deconv_2d + w_term_idft
+//       (ra_exec.cu:325-373, cuft.cu:575-612)              -> k_correct_d2m + k_zero_pad
+//   matrix_elementwise_multiply + shift_corr (utils.cu:156-192, ra_exec.cu:56-89) -> k_vis_out
+//   thrust min/max over w (utils.cu:42-53)                  -> k_wrange
+#include "kernels.cuh"
+
+#include <cub/cub.cuh>
+
+namespace curig {
+
+template <typename T> using C = typename cplx_t<T>::type;
+template <typename T> struct rec_t;
+template <> struct rec_t<float> { using type = float4; };
+template <> struct rec_t<double> { using type = double4; };
+template <typename T> using R = typename rec_t<T>::type;
+
+constexpr int NTHREADS = 256;
+constexpr int NWARPS = NTHREADS / 32;
+constexpr int KSTR = 32;                 // per-axis stride of the per-warp kernel-value scratch
+constexpr double TWO_PI = 2.0 * PI_D;
+
+// ------------------------------------------------------------------ helpers
+__device__ __forceinline__ unsigned long long ordered_key(double x) {
+    unsigned long long b = (unsigned long long)__double_as_longlong(x);
+    return (b & 0x8000000000000000ULL) ? ~b : (b | 0x8000000000000000ULL);
+}
+
+__device__ __forceinline__ int wrap3(int v, int n) {   // valid for -n <= v < 3n
+    if (v < 0) v += n;
+    if (v >= n) v -= n;
+    if (v >= n) v -= n;
+    return v;
+}
+
+__device__ __forceinline__ float pack_cell_f(int lx, int ly, int lz) {
+    return __int_as_float(lx | (ly << 10) | (lz << 20));
+}
+__device__ __forceinline__ double pack_cell_d(int lx, int ly, int lz) {
+    return __longlong_as_double((long long)(lx | (ly << 10) | (lz << 20)));
+}
+__device__ __forceinline__ int cell_bits(float w) { return __float_as_int(w); }
+__device__ __forceinline__ int cell_bits(double w) { return (int)__double_as_longlong(w); }
+
+// Grid coordinates of one visibility in the reference's operation order:
+// u,v,w *= f/c (w also * sign), *= 2 pi; u *= pixsize_x, v *= pixsize_y;
+// w' = (w - i_c)/gamma; g = (x/(2 pi) + 0.5) * nf with x <- v, y <- u, z <- w'.
+__device__ __forceinline__ bool vis_grid(const DevGeom &g, const double *__restrict__ uu,
+                                         const double *__restrict__ vv, const double *__restrict__ ww,
+                                         long long row, double foc, double &gx, double &gy,
+                                         double &gz) {
+    long long o = row * g.uvw_stride;
+    double u = uu[o], v = vv[o], w = ww[o];
+    double us = ((u * foc) * TWO_PI) * g.psx;
+    double vs = ((v * foc) * TWO_PI) * g.psy;
+    double we = (w * (foc * g.sign)) * TWO_PI;
+    double wp = (we - g.i_center) / g.gamma;
+    gx = (vs * INV_2PI + 0.5) * g.nf1;
+    gy = (us * INV_2PI + 0.5) * g.nf2;
+    gz = (wp * INV_2PI + 0.5) * g.nf3;
+    return isfinite(gx) && isfinite(gy) && isfinite(gz);
+}
+
+__device__ __forceinline__ double w_eff(const DevGeom &g, const double *__restrict__ ww, long long row,
+                                        double foc) {
+    return (ww[row * g.uvw_stride] * (foc * g.sign)) * TWO_PI;
+}
+
+// Periodic wrap into [0, nf), start cell ceil(g - kw/2), offset u = start-g+kw/2
+// in [0,1), bin index and start relative to the bin's tile origin.
+__device__ __forceinline__ void axis_loc(double gc, int nf, int B, int nb, int hkw, int kw, int &bin,
+                                         int &lstart, double &u) {
+    double gw = gc - (double)nf * floor(gc / (double)nf);
+    if (gw >= (double)nf) gw -= (double)nf;
+    if (gw < 0.0) gw = 0.0;
+    double sd = ceil(gw - 0.5 * kw);
+    u = (sd - gw) + 0.5 * kw;
+    if (u < 0.0) u = 0.0;
+    if (u >= 1.0) u = 0.99999999999999989;
+    bin = (int)(gw / (double)B);
+    if (bin >= nb) bin = nb - 1;
+    lstart = (int)sd - (bin * B - hkw);
+}
+
+struct VisLoc {
+    long long bin;
+    int lx, ly, lz;
+    double ux, uy, uz;
+};
+
+__device__ __forceinline__ int locate(const DevGeom &g, double gx, double gy, double gz, VisLoc &L) {
+    int bxi, byi, bzi;
+    axis_loc(gx, g.nf1, g.bx, g.nbx, g.hkw, g.kw, bxi, L.lx, L.ux);
+    axis_loc(gy, g.nf2, g.by, g.nby, g.hkw, g.kw, byi, L.ly, L.uy);
+    if (g.zpad) {
+        axis_loc(gz, g.nf3, g.bz, g.nbz, g.hkw, g.kw, bzi, L.lz, L.uz);
+    } else {
+        double sd = ceil(gz - 0.5 * g.kw);
+        double u = (sd - gz) + 0.5 * g.kw;
+        if (u < 0.0) u = 0.0;
+        if (u >= 1.0) u = 0.99999999999999989;
+        L.uz = u;
+        bzi = 0;
+        L.lz = (int)sd;
+        if (!(sd >= 0.0 && sd <= (double)(g.nf3 - g.kw))) return EF_RANGE;
+    }
+    if (L.lx < 0 || L.lx > g.tx - g.kw || L.ly < 0 || L.ly > g.ty - g.kw || L.lz < 0 ||
+        L.lz > g.tz - g.kw)
+        return EF_RANGE;
+    L.bin = ((long long)bzi * g.nby + byi) * g.nbx + bxi;
+    return 0;
+}
+
+// ------------------------------------------------------------------ w range
+__global__ void k_wrange(const double *__restrict__ w, int stride, long long nrow,
+                         unsigned long long *keys, int *err) {
+    double lo = INFINITY, hi = -INFINITY;
+    int bad = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nrow;
+         i += (long long)gridDim.x * blockDim.x) {
+        double x = w[i * stride];
+        if (!isfinite(x)) bad = 1;
+        else { lo = fmin(lo, x); hi = fmax(hi, x); }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (lo <= hi) {
+            atomicMin(&keys[0], ordered_key(lo));
+            atomicMax(&keys[1], ordered_key(hi));
+        }
+        if (bad) atomicOr(err, EF_NONFINITE);
+    }
+}
+
+// ------------------------------------------------------------------ binning
+__global__ void k_bin_count(DevGeom g, const double *__restrict__ uu, const double *__restrict__ vv,
+                            const double *__restrict__ ww, const double *__restrict__ foc,
+                            int *__restrict__ bin_count, int *__restrict__ rank, int *err) {
+    const long long M = g.nrow * g.nchan;
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < M;
+         j += (long long)gridDim.x * blockDim.x) {
+        long long row = j / g.nchan;
+        int ch = (int)(j - row * g.nchan);
+        double gx, gy, gz;
+        VisLoc L;
+        int e = vis_grid(g, uu, vv, ww, row, foc[ch], gx, gy, gz) ? locate(g, gx, gy, gz, L)
+                                                                  : EF_NONFINITE;
+        if (e) {
+            atomicOr(err, e);
+            rank[j] = -1;
+            continue;
+        }
+        rank[j] = atomicAdd(&bin_count[L.bin], 1);
+    }
+}
+
+__global__ void k_nsub(const int *__restrict__ count, int *__restrict__ nsub, long long nb, int sub) {
+    for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < nb;
+         b += (long long)gridDim.x * blockDim.x)
+        nsub[b] = (count[b] + sub - 1) / sub;
+}
+
+template <typename T>
+__global__ void k_bin_scatter(DevGeom g, const double *__restrict__ uu, const double *__restrict__ vv,
+                              const double *__restrict__ ww, const double *__restrict__ foc,
+                              const int *__restrict__ bin_start, const int *__restrict__ rank,
+                              R<T> *__restrict__ rec, int *__restrict__ perm) {
+    const long long M = g.nrow * g.nchan;
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < M;
+         j += (long long)gridDim.x * blockDim.x) {
+        int rk = rank[j];
+        if (rk < 0) { perm[j] = -1; continue; }
+        long long row = j / g.nchan;
+        int ch = (int)(j - row * g.nchan);
+        double gx, gy, gz;
+        VisLoc L;
+        vis_grid(g, uu, vv, ww, row, foc[ch], gx, gy, gz);
+        locate(g, gx, gy, gz, L);
+        int pos = bin_start[L.bin] + rk;
+        R<T> r;
+        r.x = (T)L.ux;
+        r.y = (T)L.uy;
+        r.z = (T)L.uz;
+        if constexpr (sizeof(T) == 4) r.w = pack_cell_f(L.lx, L.ly, L.lz);
+        else r.w = pack_cell_d(L.lx, L.ly, L.lz);
+        rec[pos] = r;
+        perm[j] = pos;
+    }
+}
+
+// c = vis * wgt * e^{i o_c w} in bin order (ra_exec.cu:98-104, cuft.cu:19-39).
+template <typename T>
+__global__ void k_vis_prep(DevGeom g, const double *__restrict__ ww, const double *__restrict__ foc,
+                           const C<T> *__restrict__ vis, const T *__restrict__ wgt,
+                           const int *__restrict__ perm, C<T> *__restrict__ cs) {
+    const long long M = g.nrow * g.nchan;
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < M;
+         j += (long long)gridDim.x * blockDim.x) {
+        int p = perm[j];
+        if (p < 0) continue;
+        long long row = j / g.nchan;
+        int ch = (int)(j - row * g.nchan);
+        double ph = g.o_center * w_eff(g, ww, row, foc[ch]);
+        double s, c;
+        sincos(ph, &s, &c);
+        C<T> v = vis[j];
+        double wt = wgt ? (double)wgt[j] : 1.0;
+        double vr = (double)v.x * wt, vi = (double)v.y * wt;
+        C<T> o;
+        o.x = (T)(vr * c - vi * s);
+        o.y = (T)(vr * s + vi * c);
+        cs[p] = o;
+    }
+}
+
+// vis = interp * wgt * e^{-i o_c w} in input order (ra_exec.cu:56-89; the
+// reference's weight "divide" invoker launches the multiply kernel, utils.cu:189).
+template <typename T>
+__global__ void k_vis_out(DevGeom g, const double *__restrict__ ww, const double *__restrict__ foc,
+                          const C<T> *__restrict__ os, const int *__restrict__ perm,
+                          const T *__restrict__ wgt, C<T> *__restrict__ vis) {
+    const long long M = g.nrow * g.nchan;
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < M;
+         j += (long long)gridDim.x * blockDim.x) {
+        int p = perm[j];
+        C<T> o;
+        if (p < 0) { o.x = 0; o.y = 0; vis[j] = o; continue; }
+        long long row = j / g.nchan;
+        int ch = (int)(j - row * g.nchan);
+        double ph = -g.o_center * w_eff(g, ww, row, foc[ch]);
+        double s, c;
+        sincos(ph, &s, &c);
+        C<T> v = os[p];
+        double wt = wgt ? (double)wgt[j] : 1.0;
+        double vr = (double)v.x * wt, vi = (double)v.y * wt;
+        o.x = (T)(vr * c - vi * s);
+        o.y = (T)(vr * s + vi * c);
+        vis[j] = o;
+    }
+}
+
+// ------------------------------------------------------------------ window
+template <typename T>
+__device__ __forceinline__ T win_eval(const DevGeom &g, const T *__restrict__ coef, T u, int d) {
+    if (g.wkind == 0) {
+        T t = u + (T)d - (T)0.5 * (T)g.kw;
+        T a = (T)1 - (T)g.c * t * t;
+        if (!(a > (T)0)) return (T)0;
+        // sqrt(a)-1 written as (a-1)/(sqrt(a)+1): no cancellation near t = 0
+        T e = ((T)g.c * t * t) / (sqrt(a) + (T)1);
+        return exp(-(T)g.beta * e);
+    }
+    const T *c = coef + d * (g.wdeg + 1);
+    T s = (T)2 * u - (T)1;
+    T v = c[0];
+    for (int i = 1; i <= g.wdeg; ++i) v = fma(v, s, c[i]);
+    return v;
+}
+
+template <typename T>
+__device__ __forceinline__ void warp_kernel_values(const DevGeom &g, const T *coef, T *ks, T ux, T uy,
+                                                   T uz, int kw, int lane) {
+    for (int q = lane; q < 3 * kw; q += 32) {
+        int ax = q >= 2 * kw ? 2 : (q >= kw ? 1 : 0);
+        int d = q - ax * kw;
+        T u = ax == 0 ? ux : (ax == 1 ? uy : uz);
+        ks[ax * KSTR + d] = win_eval<T>(g, coef, u, d);
+    }
+}
+
+__device__ __forceinline__ long long find_bin(const int *__restrict__ sub_end, long long nb, int s) {
+    long long lo = 0, hi = nb - 1;      // first b with sub_end[b] > s
+    while (lo < hi) {
+        long long mid = (lo + hi) >> 1;
+        if (sub_end[mid] > s) hi = mid;
+        else lo = mid + 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ void atomic_add_c(float2 *p, float2 v) { atomicAdd(p, v); }
+__device__ __forceinline__ void atomic_add_c(double2 *p, double2 v) {
+    atomicAdd(&p->x, v.x);
+    atomicAdd(&p->y, v.y);
+}
+
+// ------------------------------------------------------------------ spreader
+// One CTA per sub-problem (a bin and up to `sub` of its visibilities, persistent
+// grid-stride over sub-problems); the bin's tile (bin + kw halo, all w-planes or
+// a z-slab) is accumulated in shared memory with one warp per visibility (lanes
+// over the kw^3 taps: no intra-warp address collisions) and flushed once with
+// vector atomics.  KW > 0 fixes the width at compile time (0: runtime width).
+template <typename T, int KW>
+__global__ void __launch_bounds__(NTHREADS)
+k_spread(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__ bin_count,
+         const int *__restrict__ sub_end, const R<T> *__restrict__ rec, const C<T> *__restrict__ cs,
+         C<T> *__restrict__ grid, const double *__restrict__ wcoef) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int kw = KW > 0 ? KW : g.kw;
+    const int ntile = g.tx * g.ty * g.tz;
+    C<T> *tile = reinterpret_cast<C<T> *>(smem);
+    T *ksall = reinterpret_cast<T *>(tile + ntile);
+    T *coef = ksall + NWARPS * 3 * KSTR;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    T *ks = ksall + warp * 3 * KSTR;
+    if (g.wkind == 1)
+        for (int i = threadIdx.x; i < kw * (g.wdeg + 1); i += NTHREADS) coef[i] = (T)wcoef[i];
+    const int total = sub_end[g.nbins - 1];
+    const int kk = kw * kw, k3 = kk * kw;
+    const int txy = g.tx * g.ty;
+    for (int s = blockIdx.x; s < total; s += gridDim.x) {
+        long long b = find_bin(sub_end, g.nbins, s);
+        int cnt = bin_count[b];
+        int nsb = (cnt + g.sub - 1) / g.sub;
+        int chunk = s - (sub_end[b] - nsb);
+        int first = bin_start[b] + chunk * g.sub;
+        int last = min(first + g.sub, bin_start[b] + cnt);
+        for (int e = threadIdx.x; e < ntile; e += NTHREADS) tile[e] = C<T>{0, 0};
+        __syncthreads();
+        for (int i = first + warp; i < last; i += NWARPS) {
+            R<T> r = rec[i];
+            C<T> c = cs[i];
+            warp_kernel_values<T>(g, coef, ks, r.x, r.y, r.z, kw, lane);
+            __syncwarp();
+            int cb = cell_bits(r.w);
+            int base = ((cb >> 20) & 0xfff) * txy + ((cb >> 10) & 0x3ff) * g.tx + (cb & 0x3ff);
+            for (int t = lane; t < k3; t += 32) {
+                int dz = t / kk;
+                int rm = t - dz * kk;
+                int dy = rm / kw;
+                int dx = rm - dy * kw;
+                T wt = ks[dx] * ks[KSTR + dy] * ks[2 * KSTR + dz];
+                C<T> *p = tile + base + dz * txy + dy * g.tx + dx;
+                atomicAdd(&p->x, c.x * wt);
+                atomicAdd(&p->y, c.y * wt);
+            }
+            __syncwarp();
+        }
+        __syncthreads();
+        long long bxi = b % g.nbx, byi = (b / g.nbx) % g.nby, bzi = b / ((long long)g.nbx * g.nby);
+        int ox = (int)bxi * g.bx - g.hkw, oy = (int)byi * g.by - g.hkw;
+        int oz = g.zpad ? (int)bzi * g.bz - g.hkw : 0;
+        for (int row = warp; row < g.ty * g.tz; row += NWARPS) {
+            int y = row % g.ty, z = row / g.ty;
+            int gy = wrap3(oy + y, g.nf2);
+            int gz = g.zpad ? wrap3(oz + z, g.nf3) : z;
+            C<T> *grow = grid + ((long long)gz * g.nf2 + gy) * g.nf1;
+            const C<T> *trow = tile + row * g.tx;
+            for (int x = lane; x < g.tx; x += 32) {
+                C<T> v = trow[x];
+                if (v.x != (T)0 || v.y != (T)0) atomic_add_c(grow + wrap3(ox + x, g.nf1), v);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------ interpolator
+// One CTA per sub-problem: the bin's tile (with halo, wrapped) is staged in
+// shared memory with coalesced row loads; one warp per visibility gathers the
+// kw^3 taps and reduces with shuffles; results are written in bin order.
+template <typename T, int KW>
+__global__ void __launch_bounds__(NTHREADS)
+k_interp(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__ bin_count,
+         const int *__restrict__ sub_end, const R<T> *__restrict__ rec, const C<T> *__restrict__ grid,
+         C<T> *__restrict__ os, const double *__restrict__ wcoef) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int kw = KW > 0 ? KW : g.kw;
+    const int ntile = g.tx * g.ty * g.tz;
+    C<T> *tile = reinterpret_cast<C<T> *>(smem);
+    T *ksall = reinterpret_cast<T *>(tile + ntile);
+    T *coef = ksall + NWARPS * 3 * KSTR;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    T *ks = ksall + warp * 3 * KSTR;
+    if (g.wkind == 1)
+        for (int i = threadIdx.x; i < kw * (g.wdeg + 1); i += NTHREADS) coef[i] = (T)wcoef[i];
+    const int total = sub_end[g.nbins - 1];
+    const int kk = kw * kw, k3 = kk * kw;
+    const int txy = g.tx * g.ty;
+    for (int s = blockIdx.x; s < total; s += gridDim.x) {
+        long long b = find_bin(sub_end, g.nbins, s);
+        int cnt = bin_count[b];
+        int nsb = (cnt + g.sub - 1) / g.sub;
+        int chunk = s - (sub_end[b] - nsb);
+        int first = bin_start[b] + chunk * g.sub;
+        int last = min(first + g.sub, bin_start[b] + cnt);
+        long long bxi = b % g.nbx, byi = (b / g.nbx) % g.nby, bzi = b / ((long long)g.nbx * g.nby);
+        int ox = (int)bxi * g.bx - g.hkw, oy = (int)byi * g.by - g.hkw;
+        int oz = g.zpad ? (int)bzi * g.bz - g.hkw : 0;
+        for (int row = warp; row < g.ty * g.tz; row += NWARPS) {
+            int y = row % g.ty, z = row / g.ty;
+            int gy = wrap3(oy + y, g.nf2);
+            int gz = g.zpad ? wrap3(oz + z, g.nf3) : z;
+            const C<T> *grow = grid + ((long long)gz * g.nf2 + gy) * g.nf1;
+            C<T> *trow = tile + row * g.tx;
+            for (int x = lane; x < g.tx; x += 32) trow[x] = grow[wrap3(ox + x, g.nf1)];
+        }
+        __syncthreads();
+        for (int i = first + warp; i < last; i += NWARPS) {
+            R<T> r = rec[i];
+            warp_kernel_values<T>(g, coef, ks, r.x, r.y, r.z, kw, lane);
+            __syncwarp();
+            int cb = cell_bits(r.w);
+            int base = ((cb >> 20) & 0xfff) * txy + ((cb >> 10) & 0x3ff) * g.tx + (cb & 0x3ff);
+            T ar = 0, ai = 0;
+            for (int t = lane; t < k3; t += 32) {
+                int dz = t / kk;
+                int rm = t - dz * kk;
+                int dy = rm / kw;
+                int dx = rm - dy * kw;
+                T wt = ks[dx] * ks[KSTR + dy] * ks[2 * KSTR + dz];
+                C<T> v = tile[base + dz * txy + dy * g.tx + dx];
+                ar = fma(v.x, wt, ar);
+                ai = fma(v.y, wt, ai);
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                ar += __shfl_xor_sync(0xffffffffu, ar, o);
+                ai += __shfl_xor_sync(0xffffffffu, ai, o);
+            }
+            if (lane == 0) os[i] = C<T>{ar, ai};
+            __syncwarp();
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------ correction
+// Shared per-quarter-pixel factors: n, k' and psi3 depend on |l|, |m| only.
+struct QuarterPix {
+    double n, kp, psi3, ph;
+};
+
+__device__ __forceinline__ QuarterPix quarter(const DevCorr &cc, int r, int s) {
+    QuarterPix q;
+    double a = (double)r * cc.psx, b = (double)s * cc.psy;
+    q.n = sqrt(1.0 - a * a - b * b);                  // ra_exec.cu:31, precomp.cu:220
+    double k = q.n - 1;
+    q.kp = (k - cc.o_center) * cc.gamma * cc.h;       // cuft.cu:73
+    double ps = 0.0;
+    for (int i = 0; i < cc.nquad; ++i) ps += cc.qg[i] * cos(cc.qx[i] * q.kp);
+    q.psi3 = 2.0 * ps;                                // deconv.cu:45-57
+    q.ph = (k - cc.o_center) * cc.i_center;           // deconv.cu:390
+    return q;
+}
+
+// ms2dirty epilogue: w-screen sum over planes + all corrections, one pass.
+template <typename T>
+__global__ void k_correct_m2d(DevCorr cc, const C<T> *__restrict__ grid, C<T> *__restrict__ dirty) {
+    const int hx = cc.nx / 2, hy = cc.ny / 2;
+    const long long nq = (long long)(hx + 1) * (hy + 1);
+    const long long plane = (long long)cc.nf1 * cc.nf2;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nq;
+         q += (long long)gridDim.x * blockDim.x) {
+        int r = (int)(q / (hy + 1)), s = (int)(q - (long long)r * (hy + 1));
+        QuarterPix Q = quarter(cc, r, s);
+        double sc, cs;
+        sincos(Q.ph, &sc, &cs);
+        double den = cc.psi1[s] * cc.psi2[r] * Q.psi3 * Q.n;
+        double fr = cs / den, fi = sc / den;
+        int ixs[4], iys[4];
+        long long off[4];
+        int np = 0;
+        for (int sx = 0; sx < 2; ++sx) {
+            int ix = sx ? hx - r : hx + r;
+            if (ix < 0 || ix >= cc.nx || (sx && r == 0)) continue;
+            int w2 = sx ? cc.nf2 - r : r;
+            for (int sy = 0; sy < 2; ++sy) {
+                int iy = sy ? hy - s : hy + s;
+                if (iy < 0 || iy >= cc.ny || (sy && s == 0)) continue;
+                int w1 = sy ? cc.nf1 - s : s;
+                ixs[np] = ix;
+                iys[np] = iy;
+                off[np] = (long long)w2 * cc.nf1 + w1;
+                ++np;
+            }
+        }
+        double ar[4] = {0, 0, 0, 0}, ai[4] = {0, 0, 0, 0};
+        double es, ec, ss, scs;
+        sincos(Q.kp, &ss, &scs);                                   // step e^{i k'}
+        sincos(-Q.kp * (double)(cc.nf3 / 2), &es, &ec);            // e^{i k'(0 - nf3/2)}
+        for (int p = 0; p < cc.nf3; ++p) {
+            const C<T> *gp = grid + p * plane;
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                if (t < np) {
+                    C<T> v = gp[off[t]];
+                    ar[t] += (double)v.x * ec - (double)v.y * es;
+                    ai[t] += (double)v.x * es + (double)v.y * ec;
+                }
+            }
+            double nr = ec * scs - es * ss, ni = ec * ss + es * scs;
+            ec = nr;
+            es = ni;
+        }
+        for (int t = 0; t < np; ++t) {
+            C<T> o;
+            o.x = (T)(ar[t] * fr - ai[t] * fi);
+            o.y = (T)(ar[t] * fi + ai[t] * fr);
+            dirty[(long long)ixs[t] * cc.ny + iys[t]] = o;
+        }
+    }
+}
+
+// dirty2ms prologue: corrections + per-plane screen, written at the image cells
+// of every plane (the rest of the planes is zeroed by k_zero_pad).
+template <typename T>
+__global__ void k_correct_d2m(DevCorr cc, const C<T> *__restrict__ dirty, C<T> *__restrict__ grid) {
+    const int hx = cc.nx / 2, hy = cc.ny / 2;
+    const long long nq = (long long)(hx + 1) * (hy + 1);
+    const long long plane = (long long)cc.nf1 * cc.nf2;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nq;
+         q += (long long)gridDim.x * blockDim.x) {
+        int r = (int)(q / (hy + 1)), s = (int)(q - (long long)r * (hy + 1));
+        QuarterPix Q = quarter(cc, r, s);
+        double sc, cs;
+        sincos(-Q.ph, &sc, &cs);
+        double den = cc.psi1[s] * cc.psi2[r] * Q.psi3 * Q.n;
+        double fr = cs / den, fi = sc / den;
+        double vr[4], vi[4];
+        long long off[4];
+        int np = 0;
+        for (int sx = 0; sx < 2; ++sx) {
+            int ix = sx ? hx - r : hx + r;
+            if (ix < 0 || ix >= cc.nx || (sx && r == 0)) continue;
+            int w2 = sx ? cc.nf2 - r : r;
+            for (int sy = 0; sy < 2; ++sy) {
+                int iy = sy ? hy - s : hy + s;
+                if (iy < 0 || iy >= cc.ny || (sy && s == 0)) continue;
+                int w1 = sy ? cc.nf1 - s : s;
+                C<T> d = dirty[(long long)ix * cc.ny + iy];
+                vr[np] = (double)d.x * fr - (double)d.y * fi;
+                vi[np] = (double)d.x * fi + (double)d.y * fr;
+                off[np] = (long long)w2 * cc.nf1 + w1;
+                ++np;
+            }
+        }
+        double es, ec, ss, scs;
+        sincos(-Q.kp, &ss, &scs);                                  // step e^{-i k'}
+        sincos(Q.kp * (double)(cc.nf3 / 2), &es, &ec);             // e^{-i k'(0 - nf3/2)}
+        for (int p = 0; p < cc.nf3; ++p) {
+            C<T> *gp = grid + p * plane;
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                if (t < np) {
+                    C<T> o;
+                    o.x = (T)(vr[t] * ec - vi[t] * es);
+                    o.y = (T)(vr[t] * es + vi[t] * ec);
+                    gp[off[t]] = o;
+                }
+            }
+            double nr = ec * scs - es * ss, ni = ec * ss + es * scs;
+            ec = nr;
+            es = ni;
+        }
+    }
+}
+
+// Zero every cell of every plane that k_correct_d2m does not write.
+template <typename T>
+__global__ void k_zero_pad(int nx, int ny, int nf1, int nf2, int nf3, C<T> *__restrict__ grid) {
+    const long long rows = (long long)nf3 * nf2;
+    for (long long rr = blockIdx.x; rr < rows; rr += gridDim.x) {
+        int y = (int)(rr % nf2);
+        bool img = (y < nx - nx / 2) || (y >= nf2 - nx / 2);
+        int x0 = img ? ny - ny / 2 : 0, x1 = img ? nf1 - ny / 2 : nf1;
+        C<T> *row = grid + rr * nf1;
+        for (int x = x0 + threadIdx.x; x < x1; x += blockDim.x) row[x] = C<T>{0, 0};
+    }
+}
+
+// ------------------------------------------------------------------ launchers
+static int grid_for(long long n, int per = NTHREADS) {
+    long long b = (n + per - 1) / per;
+    if (b > 148LL * 32) b = 148LL * 32;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+void launch_wrange(const double *w, int stride, long long nrow, unsigned long long *keys, int *err,
+                   cudaStream_t st) {
+    k_wrange<<<grid_for(nrow), NTHREADS, 0, st>>>(w, stride, nrow, keys, err);
+}
+
+void launch_bin_count(const DevGeom &g, const double *u, const double *v, const double *w,
+                      const double *foc, int *bin_count, int *rank, int *err, cudaStream_t st) {
+    k_bin_count<<<grid_for(g.nrow * g.nchan), NTHREADS, 0, st>>>(g, u, v, w, foc, bin_count, rank, err);
+}
+
+void launch_nsub(const int *count, int *nsub, long long nb, int sub, cudaStream_t st) {
+    k_nsub<<<grid_for(nb), NTHREADS, 0, st>>>(count, nsub, nb, sub);
+}
+
+size_t scan_temp_bytes(long long n) {
+    size_t a = 0, b = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, a, (const int *)nullptr, (int *)nullptr, (int)n);
+    cub::DeviceScan::InclusiveSum(nullptr, b, (const int *)nullptr, (int *)nullptr, (int)n);
+    return a > b ? a : b;
+}
+
+int scan_exclusive(void *tmp, size_t tmpb, const int *in, int *out, long long n, cudaStream_t st) {
+    return cub::DeviceScan::ExclusiveSum(tmp, tmpb, in, out, (int)n, st) == cudaSuccess ? 0 : ERR_CUDA;
+}
+
+int scan_inclusive(void *tmp, size_t tmpb, const int *in, int *out, long long n, cudaStream_t st) {
+    return cub::DeviceScan::InclusiveSum(tmp, tmpb, in, out, (int)n, st) == cudaSuccess ? 0 : ERR_CUDA;
+}
+
+template <typename T>
+void launch_bin_scatter(const DevGeom &g, const double *u, const double *v, const double *w,
+                        const double *foc, const int *bin_start, const int *rank, void *rec, int *perm,
+                        cudaStream_t st) {
+    k_bin_scatter<T><<<grid_for(g.nrow * g.nchan), NTHREADS, 0, st>>>(
+        g, u, v, w, foc, bin_start, rank, reinterpret_cast<R<T> *>(rec), perm);
+}
+
+template <typename T>
+void launch_vis_prep(const DevGeom &g, const double *w, const double *foc, const void *vis,
+                     const void *wgt, const int *perm, void *cs, cudaStream_t st) {
+    k_vis_prep<T><<<grid_for(g.nrow * g.nchan), NTHREADS, 0, st>>>(
+        g, w, foc, reinterpret_cast<const C<T> *>(vis), reinterpret_cast<const T *>(wgt), perm,
+        reinterpret_cast<C<T> *>(cs));
+}
+
+template <typename T>
+void launch_vis_out(const DevGeom &g, const double *w, const double *foc, const void *os,
+                    const int *perm, const void *wgt, void *vis, cudaStream_t st) {
+    k_vis_out<T><<<grid_for(g.nrow * g.nchan), NTHREADS, 0, st>>>(
+        g, w, foc, reinterpret_cast<const C<T> *>(os), perm, reinterpret_cast<const T *>(wgt),
+        reinterpret_cast<C<T> *>(vis));
+}
+
+size_t tile_smem_bytes(const TileGeom &tg, int esize, int kw, int wdeg) {
+    size_t s = (size_t)tg.tx * tg.ty * tg.tz * 2 * esize;
+    s += (size_t)NWARPS * 3 * KSTR * esize;
+    s += (size_t)kw * (wdeg + 1) * esize;
+    return (s + 15) & ~(size_t)15;
+}
+
+template <typename T, int KW>
+static int launch_spread_kw(const DevGeom &g, size_t smem, const int *bs, const int *bc, const int *se,
+                            const void *rec, const void *cs, void *grid, const double *wc, int nsm,
+                            cudaStream_t st) {
+    auto kern = k_spread<T, KW>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return ERR_CUDA;
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, NTHREADS, smem);
+    if (occ < 1) return ERR_UNSUPPORTED;
+    kern<<<nsm * occ, NTHREADS, smem, st>>>(g, bs, bc, se, reinterpret_cast<const R<T> *>(rec),
+                                            reinterpret_cast<const C<T> *>(cs),
+                                            reinterpret_cast<C<T> *>(grid), wc);
+    return OK;
+}
+
+template <typename T, int KW>
+static int launch_interp_kw(const DevGeom &g, size_t smem, const int *bs, const int *bc, const int *se,
+                            const void *rec, const void *grid, void *os, const double *wc, int nsm,
+                            cudaStream_t st) {
+    auto kern = k_interp<T, KW>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return ERR_CUDA;
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, NTHREADS, smem);
+    if (occ < 1) return ERR_UNSUPPORTED;
+    kern<<<nsm * occ, NTHREADS, smem, st>>>(g, bs, bc, se, reinterpret_cast<const R<T> *>(rec),
+                                            reinterpret_cast<const C<T> *>(grid),
+                                            reinterpret_cast<C<T> *>(os), wc);
+    return OK;
+}
+
+#define CURIG_KW_SWITCH(F, ...)                                  \
+    switch (g.kw) {                                              \
+    case 2: return F<T, 2>(__VA_ARGS__);                         \
+    case 3: return F<T, 3>(__VA_ARGS__);                         \
+    case 4: return F<T, 4>(__VA_ARGS__);                         \
+    case 5: return F<T, 5>(__VA_ARGS__);                         \
+    case 6: return F<T, 6>(__VA_ARGS__);                         \
+    case 7: return F<T, 7>(__VA_ARGS__);                         \
+    case 8: return F<T, 8>(__VA_ARGS__);                         \
+    default: return F<T, 0>(__VA_ARGS__);                        \
+    }
+
+template <typename T>
+int launch_spread(const DevGeom &g, size_t smem, const int *bs, const int *bc, const int *se,
+                  const void *rec, const void *cs, void *grid, const double *wc, int nsm, cudaStream_t st) {
+    CURIG_KW_SWITCH(launch_spread_kw, g, smem, bs, bc, se, rec, cs, grid, wc, nsm, st)
+}
+
+template <typename T>
+int launch_interp(const DevGeom &g, size_t smem, const int *bs, const int *bc, const int *se,
+                  const void *rec, const void *grid, void *os, const double *wc, int nsm, cudaStream_t st) {
+    CURIG_KW_SWITCH(launch_interp_kw, g, smem, bs, bc, se, rec, grid, os, wc, nsm, st)
+}
+
+template <typename T>
+void launch_correct_m2d(const DevCorr &cc, const void *grid, void *dirty, cudaStream_t st) {
+    long long nq = (long long)(cc.nx / 2 + 1) * (cc.ny / 2 + 1);
+    k_correct_m2d<T><<<grid_for(nq, 128), 128, 0, st>>>(cc, reinterpret_cast<const C<T> *>(grid),
+                                                        reinterpret_cast<C<T> *>(dirty));
+}
+
+template <typename T>
+void launch_correct_d2m(const DevCorr &cc, const void *dirty, void *grid, cudaStream_t st) {
+    long long nq = (long long)(cc.nx / 2 + 1) * (cc.ny / 2 + 1);
+    k_correct_d2m<T><<<grid_for(nq, 128), 128, 0, st>>>(cc, reinterpret_cast<const C<T> *>(dirty),
+                                                        reinterpret_cast<C<T> *>(grid));
+}
+
+template <typename T>
+void launch_zero_pad(int nx, int ny, int nf1, int nf2, int nf3, void *grid, cudaStream_t st) {
+    long long rows = (long long)nf3 * nf2;
+    int blocks = rows > 148LL * 64 ? 148 * 64 : (int)rows;
+    k_zero_pad<T><<<blocks, 256, 0, st>>>(nx, ny, nf1, nf2, nf3, reinterpret_cast<C<T> *>(grid));
+}
+
+#define CURIG_INSTANTIATE(T)                                                                          \
+    template void launch_bin_scatter<T>(const DevGeom &, const double *, const double *,             \
+                                        const double *, const double *, const int *, const int *,     \
+                                        void *, int *, cudaStream_t);                                  \
+    template void launch_vis_prep<T>(const DevGeom &, const double *, const double *, const void *,   \
+                                     const void *, const int *, void *, cudaStream_t);                \
+    template void launch_vis_out<T>(const DevGeom &, const double *, const double *, const void *,    \
+                                    const int *, const void *, void *, cudaStream_t);                 \
+    template int launch_spread<T>(const DevGeom &, size_t, const int *, const int *, const int *,     \
+                                  const void *, const void *, void *, const double *, int,            \
+                                  cudaStream_t);                                                      \
+    template int launch_interp<T>(const DevGeom &, size_t, const int *, const int *, const int *,     \
+                                  const void *, const void *, void *, const double *, int,            \
+                                  cudaStream_t);                                                      \
+    template void launch_correct_m2d<T>(const DevCorr &, const void *, void *, cudaStream_t);         \
+    template void launch_correct_d2m<T>(const DevCorr &, const void *, void *, cudaStream_t);         \
+    template void launch_zero_pad<T>(int, int, int, int, int, void *, cudaStream_t);
+
+CURIG_INSTANTIATE(float)
+CURIG_INSTANTIATE(double)
+
+}  // namespace curig

@@ -1,0 +1,42 @@
+// Device kernels of the gridder (declarations shared by kernels.cu and plan.cu).
+#pragma once
+
+#include "curig_internal.h"
+
+namespace curig {
+
+template <typename T> struct cplx_t;
+template <> struct cplx_t<float> { using type = float2; };
+template <> struct cplx_t<double> { using type = double2; };
+
+// Everything a binning / spreading / interpolation launch needs, by value.
+struct DevGeom {
+    int nf1, nf2, nf3;
+    int kw, hkw;                   // kernel width, floor(kw/2)
+    int bx, by, bz, nbx, nby, nbz;
+    int tx, ty, tz, zpad;
+    int sub;                       // visibilities per sub-problem
+    long long nbins;
+    double beta, c;                // ES parameters
+    int wkind, wdeg;               // window kind (0 ES, 1 polynomial), degree
+    // visibility geometry
+    long long nrow;
+    int nchan;
+    int uvw_stride;                // 3 for [nrow][3], 1 for separate arrays
+    double psx, psy, i_center, gamma, o_center, sign;
+};
+
+// Quarter-pixel correction geometry (ms2dirty epilogue / dirty2ms prologue).
+struct DevCorr {
+    int nx, ny, nf1, nf2, nf3;
+    double psx, psy, o_center, i_center, gamma, h;
+    int nquad;
+    const double *qx;              // quadrature nodes (grid units)
+    const double *qg;              // quadrature weights * window
+    const double *psi1;            // [nf1/2+1]
+    const double *psi2;            // [nf2/2+1]
+};
+
+enum ErrFlag : int { EF_NONFINITE = 1, EF_RANGE = 2 };
+
+}  // namespace curig

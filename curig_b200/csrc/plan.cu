@@ -1,0 +1,433 @@
+// Host orchestration of one ms2dirty / dirty2ms plan: set points (w range,
+// sizing, tile binning), execute (spread -> cuFFT -> screen+correction, or the
+// adjoint chain), destroy.  Mirrors the reference's plan life cycle
+// (gridder_setting / gridder_execution / gridder_destroy, src/astro/cugridder.cu:105-328)
+// with device memory from the stream-ordered pool and no host synchronisation
+// inside execute.
+#include "plan.h"
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
+
+namespace curig {
+
+#define CU_TRY(x)                                   \
+    do {                                            \
+        cudaError_t e_ = (x);                       \
+        if (e_ != cudaSuccess) {                    \
+            p->last_error = cudaGetErrorString(e_); \
+            return e_ == cudaErrorMemoryAllocation ? ERR_NOMEM : ERR_CUDA; \
+        }                                           \
+    } while (0)
+
+template <typename X>
+static cudaError_t dalloc(X **ptr, size_t bytes, cudaStream_t st) {
+    *ptr = nullptr;
+    if (bytes == 0) bytes = 16;
+    return cudaMallocAsync((void **)ptr, bytes, st);
+}
+
+template <typename X>
+static void dfree(X *&ptr, cudaStream_t st) {
+    if (ptr) cudaFreeAsync((void *)ptr, st);
+    ptr = nullptr;
+}
+
+static void keep_pool_memory(int device) {
+    static bool done[64] = {false};
+    if (device < 0 || device >= 64 || done[device]) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        unsigned long long thr = ULLONG_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    done[device] = true;
+}
+
+// ------------------------------------------------------------------ cuFFT plan cache
+namespace {
+std::mutex g_fft_mu;
+std::map<std::tuple<int, int, int, int, int>, cufftHandle> g_fft;   // (dev, nf1, nf2, batch, prec)
+}
+
+static int fft_plan(int dev, int nf1, int nf2, int batch, int prec, cufftHandle &out) {
+    std::lock_guard<std::mutex> lk(g_fft_mu);
+    auto key = std::make_tuple(dev, nf1, nf2, batch, prec);
+    auto it = g_fft.find(key);
+    if (it != g_fft.end()) { out = it->second; return OK; }
+    cufftHandle h;
+    int n[2] = {nf2, nf1};
+    long long dist = (long long)nf1 * nf2;
+    if (cufftPlanMany(&h, 2, n, n, 1, (int)dist, n, 1, (int)dist, prec ? CUFFT_C2C : CUFFT_Z2Z, batch) !=
+        CUFFT_SUCCESS)
+        return ERR_CUFFT;
+    g_fft[key] = h;
+    out = h;
+    return OK;
+}
+
+// ------------------------------------------------------------------ learned-window registry
+namespace {
+std::mutex g_win_mu;
+std::vector<Window> g_windows;
+}
+
+int registry_set_window(int kw, int degree, const double *coef, double eps_reached) {
+    if (kw < 2 || kw > MAX_KW || degree < 1 || degree + 1 > MAX_POLY || !coef) return ERR_ARG;
+    Window w;
+    w.kind = 1;
+    w.kw = kw;
+    w.degree = degree;
+    w.coef.assign(coef, coef + (size_t)kw * (degree + 1));
+    w.eps_reached = eps_reached;
+    std::lock_guard<std::mutex> lk(g_win_mu);
+    for (auto &x : g_windows)
+        if (x.kw == kw) { x = w; return OK; }
+    g_windows.push_back(w);
+    return OK;
+}
+
+const Window *registry_pick_window(double eps) {
+    std::lock_guard<std::mutex> lk(g_win_mu);
+    const Window *best = nullptr;
+    for (auto &x : g_windows)
+        if (x.eps_reached <= eps && (!best || x.kw < best->kw)) best = &x;
+    return best;
+}
+
+const Window *registry_get_window(int kw) {
+    std::lock_guard<std::mutex> lk(g_win_mu);
+    for (auto &x : g_windows)
+        if (x.kw == kw) return &x;
+    return nullptr;
+}
+
+void registry_clear() {
+    std::lock_guard<std::mutex> lk(g_win_mu);
+    g_windows.clear();
+}
+
+// ------------------------------------------------------------------ plan
+int plan_create(int type, int nx, int ny, double psx, double psy, double eps, double sigma, int sign,
+                const Options &opt, Plan **out) {
+    *out = nullptr;
+    if ((type != 1 && type != 2) || nx <= 0 || ny <= 0 || nx > (1 << 24) || ny > (1 << 24))
+        return ERR_ARG;
+    if (opt.precision != 0 && opt.precision != 1) return ERR_ARG;
+    if (!std::isfinite(psx) || !std::isfinite(psy) || !(psx > 0) || !(psy > 0)) return ERR_ARG;
+    KernelParams kp;
+    int st = setup_kernel(eps, sigma, kp);
+    if (st != OK) return st;
+    Plan *p = new Plan();
+    p->type = type;
+    p->nx = nx;
+    p->ny = ny;
+    p->psx = psx;
+    p->psy = psy;
+    p->eps = eps;
+    p->sigma = sigma;
+    p->sign = sign >= 0 ? 1 : -1;
+    p->opt = opt;
+    p->st = opt.stream;
+    if (cudaGetDevice(&p->device) != cudaSuccess) { delete p; return ERR_CUDA; }
+    cudaDeviceGetAttribute(&p->nsm, cudaDevAttrMultiProcessorCount, p->device);
+    keep_pool_memory(p->device);
+    *out = p;
+    return OK;
+}
+
+void plan_release_points(Plan *p) {
+    cudaStream_t st = p->st;
+    dfree(p->d_foc, st); dfree(p->d_quad, st); dfree(p->d_psi1, st); dfree(p->d_psi2, st);
+    dfree(p->d_wcoef, st); dfree(p->d_bin_count, st); dfree(p->d_bin_start, st); dfree(p->d_nsub, st);
+    dfree(p->d_sub_end, st); dfree(p->d_rank, st); dfree(p->d_perm, st); dfree(p->d_err, st);
+    dfree(p->d_keys, st); dfree(p->d_rec, st); dfree(p->d_cs, st); dfree(p->d_grid, st);
+    dfree(p->d_scan_tmp, st);
+    p->ready = false;
+}
+
+int plan_destroy(Plan *p) {
+    if (!p) return OK;
+    plan_release_points(p);
+    cudaStreamSynchronize(p->st);
+    delete p;
+    return OK;
+}
+
+// Bin / tile geometry: the largest xy bin whose tile (bin + kw halo, all
+// w-planes when the w support never wraps, else 8-plane slabs) fits the
+// shared-memory budget.
+static int choose_tiles(Plan *p, int esize) {
+    const GridParams &gp = p->gp;
+    const int kw = gp.kp.kw;
+    TileGeom &t = p->tg;
+    size_t budget = p->opt.smem_budget ? p->opt.smem_budget : (esize == 4 ? 72 * 1024 : 100 * 1024);
+    int wdeg = p->win.kind ? p->win.degree : 0;
+    // does the w support stay inside [0, nf3)?  (z grows monotonically with w)
+    auto zstart = [&](double we) {
+        double wp = (we - gp.i_center) / gp.gamma;
+        double gz = (wp * INV_2PI + 0.5) * gp.nf3;
+        return std::ceil(gz - 0.5 * kw);
+    };
+    double z0 = zstart(p->wmin_eff), z1 = zstart(p->wmax_eff);
+    bool nowrap = z0 >= 1.0 && z1 + kw - 1 <= gp.nf3 - 2.0 && gp.nf3 <= 4000;
+    const int cand[] = {64, 48, 32, 24, 16, 12, 8, 6, 4, 2};
+    int bxy = 0;
+    auto fits = [&](int b, int tz) {
+        TileGeom q;
+        q.tx = b + kw; q.ty = b + kw; q.tz = tz;
+        return q.tx <= 1024 && tile_smem_bytes(q, esize, kw, wdeg) <= budget;
+    };
+    if (nowrap) {
+        for (int b : cand) {
+            if (p->opt.bin_xy && b != p->opt.bin_xy) continue;
+            if (b > gp.nf1 || b > gp.nf2) continue;
+            if (fits(b, gp.nf3)) { bxy = b; break; }
+        }
+    }
+    if (bxy) {
+        t.zpad = 0; t.bz = gp.nf3; t.tz = gp.nf3; t.nbz = 1;
+    } else {
+        t.zpad = 1;
+        int bz = std::min(8, gp.nf3);
+        for (int b : cand) {
+            if (p->opt.bin_xy && b != p->opt.bin_xy) continue;
+            if (b > gp.nf1 || b > gp.nf2) continue;
+            if (fits(b, bz + kw)) { bxy = b; break; }
+        }
+        if (!bxy) {
+            bz = 2;
+            for (int b : cand) {
+                if (b > gp.nf1 || b > gp.nf2) continue;
+                if (fits(b, bz + kw)) { bxy = b; break; }
+            }
+        }
+        if (!bxy) return ERR_UNSUPPORTED;
+        t.bz = bz; t.tz = bz + kw; t.nbz = (gp.nf3 + bz - 1) / bz;
+        if (t.tz > 4096) return ERR_UNSUPPORTED;
+    }
+    t.bx = t.by = bxy;
+    t.tx = bxy + kw; t.ty = bxy + kw;
+    t.nbx = (gp.nf1 + bxy - 1) / bxy;
+    t.nby = (gp.nf2 + bxy - 1) / bxy;
+    t.sub = p->opt.sub > 0 ? p->opt.sub : 2048;
+    t.smem_bytes = tile_smem_bytes(t, esize, kw, wdeg);
+    if (t.nbins() > INT_MAX / 2) return ERR_UNSUPPORTED;
+    return OK;
+}
+
+static double key_to_double(unsigned long long k) {
+    unsigned long long b = (k & 0x8000000000000000ULL) ? (k & 0x7fffffffffffffffULL) : ~k;
+    double d;
+    std::memcpy(&d, &b, 8);
+    return d;
+}
+
+int plan_setpts(Plan *p, long long nrow, int nchan, const double *du, const double *dv,
+                const double *dw, int stride, const double *h_freq) {
+    if (!p) return ERR_ARG;
+    if (nrow <= 0 || nchan <= 0 || !du || !dv || !dw || !h_freq || stride <= 0) return ERR_ARG;
+    if (nrow * (long long)nchan >= INT_MAX) return ERR_ARG;
+    for (int c = 0; c < nchan; ++c)
+        if (!std::isfinite(h_freq[c]) || !(h_freq[c] > 0)) return ERR_NONFINITE;
+    plan_release_points(p);
+    cudaStream_t st = p->st;
+    p->nrow = nrow;
+    p->nchan = nchan;
+    p->freq.assign(h_freq, h_freq + nchan);
+    p->du = du; p->dv = dv; p->dw = dw; p->stride = stride;
+    const int esize = p->opt.precision ? 4 : 8;
+    const long long M = nrow * nchan;
+
+    // 1. raw w range -> effective range over channels (precomp.cu:61-69, utils.cu:42-53)
+    CU_TRY(dalloc(&p->d_keys, 2 * sizeof(unsigned long long), st));
+    CU_TRY(dalloc(&p->d_err, sizeof(int), st));
+    unsigned long long hk[2] = {ULLONG_MAX, 0ULL};
+    CU_TRY(cudaMemcpyAsync(p->d_keys, hk, sizeof(hk), cudaMemcpyHostToDevice, st));
+    CU_TRY(cudaMemsetAsync(p->d_err, 0, sizeof(int), st));
+    launch_wrange(dw, stride, nrow, p->d_keys, p->d_err, st);
+    int herr = 0;
+    CU_TRY(cudaMemcpyAsync(hk, p->d_keys, sizeof(hk), cudaMemcpyDeviceToHost, st));
+    CU_TRY(cudaMemcpyAsync(&herr, p->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CU_TRY(cudaStreamSynchronize(st));
+    CU_TRY(cudaGetLastError());
+    if (herr & EF_NONFINITE) return ERR_NONFINITE;
+    double wmin = key_to_double(hk[0]), wmax = key_to_double(hk[1]);
+    double lo = INFINITY, hi = -INFINITY;
+    std::vector<double> foc(nchan);
+    for (int c = 0; c < nchan; ++c) {
+        foc[c] = h_freq[c] / SPEEDOFLIGHT;
+        double a = foc[c] * p->sign;
+        for (double w : {wmin, wmax}) {
+            double v = (w * a) * (2 * PI_D);
+            lo = std::min(lo, v);
+            hi = std::max(hi, v);
+        }
+    }
+    p->wmin_eff = lo;
+    p->wmax_eff = hi;
+
+    // 2. sizes (cugridder.cu:29-101, 180-186) and window
+    int kw_override = 0;
+    p->win = Window();
+    if (p->opt.window == 1) {
+        const Window *lw = registry_pick_window(p->eps);
+        if (!lw) return ERR_WINDOW;
+        p->win = *lw;
+        kw_override = lw->kw;
+    }
+    int s = grid_params(p->nx, p->ny, p->psx, p->psy, lo, hi, p->eps, p->sigma, p->sign, p->gp, kw_override);
+    if (s != OK) return s;
+    p->win.kw = p->gp.kp.kw;
+    s = choose_tiles(p, esize);
+    if (s != OK) return s;
+    const GridParams &gp = p->gp;
+    const TileGeom &tg = p->tg;
+    p->smem = tg.smem_bytes;
+
+    DevGeom &g = p->dg;
+    g = DevGeom{};
+    g.nf1 = gp.nf1; g.nf2 = gp.nf2; g.nf3 = gp.nf3;
+    g.kw = gp.kp.kw; g.hkw = gp.kp.kw / 2;
+    g.bx = tg.bx; g.by = tg.by; g.bz = tg.bz; g.nbx = tg.nbx; g.nby = tg.nby; g.nbz = tg.nbz;
+    g.tx = tg.tx; g.ty = tg.ty; g.tz = tg.tz; g.zpad = tg.zpad; g.sub = tg.sub;
+    g.nbins = tg.nbins();
+    g.beta = gp.kp.beta; g.c = gp.kp.c;
+    g.wkind = p->win.kind; g.wdeg = p->win.kind ? p->win.degree : 0;
+    g.nrow = nrow; g.nchan = nchan; g.uvw_stride = stride;
+    g.psx = gp.pixsize_x; g.psy = gp.pixsize_y; g.i_center = gp.i_center; g.gamma = gp.gamma;
+    g.o_center = gp.o_center; g.sign = (double)gp.sign;
+
+    // 3. correction tables (deconv.cu:60-197): psi1, psi2 on the grid, quadrature for psi3
+    std::vector<double> psi1, psi2;
+    psi_hat_grid(gp.nf1, gp.kp, p->win, psi1);
+    psi_hat_grid(gp.nf2, gp.kp, p->win, psi2);
+    double qx[MAX_QUAD], qg[MAX_QUAD];
+    int nq = quadrature_terms(gp.kp, p->win, qx, qg);
+    CU_TRY(dalloc(&p->d_foc, nchan * sizeof(double), st));
+    CU_TRY(dalloc(&p->d_quad, 2 * MAX_QUAD * sizeof(double), st));
+    CU_TRY(dalloc(&p->d_psi1, psi1.size() * sizeof(double), st));
+    CU_TRY(dalloc(&p->d_psi2, psi2.size() * sizeof(double), st));
+    CU_TRY(cudaMemcpyAsync(p->d_foc, foc.data(), nchan * sizeof(double), cudaMemcpyHostToDevice, st));
+    CU_TRY(cudaMemcpyAsync(p->d_quad, qx, nq * sizeof(double), cudaMemcpyHostToDevice, st));
+    CU_TRY(cudaMemcpyAsync(p->d_quad + MAX_QUAD, qg, nq * sizeof(double), cudaMemcpyHostToDevice, st));
+    CU_TRY(cudaMemcpyAsync(p->d_psi1, psi1.data(), psi1.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    CU_TRY(cudaMemcpyAsync(p->d_psi2, psi2.data(), psi2.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    if (p->win.kind == 1) {
+        CU_TRY(dalloc(&p->d_wcoef, p->win.coef.size() * sizeof(double), st));
+        CU_TRY(cudaMemcpyAsync(p->d_wcoef, p->win.coef.data(), p->win.coef.size() * sizeof(double),
+                               cudaMemcpyHostToDevice, st));
+    }
+    DevCorr &cc = p->dc;
+    cc.nx = p->nx; cc.ny = p->ny; cc.nf1 = gp.nf1; cc.nf2 = gp.nf2; cc.nf3 = gp.nf3;
+    cc.psx = gp.pixsize_x; cc.psy = gp.pixsize_y; cc.o_center = gp.o_center; cc.i_center = gp.i_center;
+    cc.gamma = gp.gamma; cc.h = gp.h; cc.nquad = nq;
+    cc.qx = p->d_quad; cc.qg = p->d_quad + MAX_QUAD; cc.psi1 = p->d_psi1; cc.psi2 = p->d_psi2;
+
+    // 4. binning: count, scan, scatter (replaces transpose + the unsorted point order)
+    const long long nb = g.nbins;
+    CU_TRY(dalloc(&p->d_bin_count, nb * sizeof(int), st));
+    CU_TRY(dalloc(&p->d_bin_start, nb * sizeof(int), st));
+    CU_TRY(dalloc(&p->d_nsub, nb * sizeof(int), st));
+    CU_TRY(dalloc(&p->d_sub_end, nb * sizeof(int), st));
+    CU_TRY(dalloc(&p->d_rank, M * sizeof(int), st));
+    CU_TRY(dalloc(&p->d_perm, M * sizeof(int), st));
+    CU_TRY(dalloc(&p->d_rec, M * 4 * (size_t)esize, st));
+    CU_TRY(dalloc(&p->d_cs, M * 2 * (size_t)esize, st));
+    p->scan_bytes = scan_temp_bytes(nb);
+    CU_TRY(dalloc(&p->d_scan_tmp, p->scan_bytes, st));
+    CU_TRY(cudaMemsetAsync(p->d_bin_count, 0, nb * sizeof(int), st));
+    launch_bin_count(g, du, dv, dw, p->d_foc, p->d_bin_count, p->d_rank, p->d_err, st);
+    launch_nsub(p->d_bin_count, p->d_nsub, nb, g.sub, st);
+    if (scan_exclusive(p->d_scan_tmp, p->scan_bytes, p->d_bin_count, p->d_bin_start, nb, st)) return ERR_CUDA;
+    if (scan_inclusive(p->d_scan_tmp, p->scan_bytes, p->d_nsub, p->d_sub_end, nb, st)) return ERR_CUDA;
+    if (p->opt.precision)
+        launch_bin_scatter<float>(g, du, dv, dw, p->d_foc, p->d_bin_start, p->d_rank, p->d_rec, p->d_perm, st);
+    else
+        launch_bin_scatter<double>(g, du, dv, dw, p->d_foc, p->d_bin_start, p->d_rank, p->d_rec, p->d_perm, st);
+    CU_TRY(cudaMemcpyAsync(&herr, p->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CU_TRY(cudaStreamSynchronize(st));
+    CU_TRY(cudaGetLastError());
+    if (herr & EF_NONFINITE) return ERR_NONFINITE;
+    if (herr & EF_RANGE) return ERR_GENERIC;
+    dfree(p->d_rank, st);
+
+    // 5. fine grid and FFT plans
+    size_t gbytes = (size_t)gp.nf1 * gp.nf2 * gp.nf3 * 2 * esize;
+    CU_TRY(dalloc(&p->d_grid, gbytes, st));
+    long long plane = (long long)gp.nf1 * gp.nf2;
+    int batch = (int)std::max(1LL, std::min((long long)gp.nf3, (1LL << 27) / plane));
+    p->fft_batch = batch;
+    p->fft_rest_batch = gp.nf3 % batch;
+    if (fft_plan(p->device, gp.nf1, gp.nf2, batch, p->opt.precision, p->fft_main)) return ERR_CUFFT;
+    if (p->fft_rest_batch &&
+        fft_plan(p->device, gp.nf1, gp.nf2, p->fft_rest_batch, p->opt.precision, p->fft_rest))
+        return ERR_CUFFT;
+    p->ready = true;
+    return OK;
+}
+
+static int run_fft(Plan *p, int dir) {
+    const GridParams &gp = p->gp;
+    long long plane = (long long)gp.nf1 * gp.nf2;
+    int done = 0;
+    while (done < gp.nf3) {
+        int b = (gp.nf3 - done >= p->fft_batch) ? p->fft_batch : p->fft_rest_batch;
+        cufftHandle h = (b == p->fft_batch) ? p->fft_main : p->fft_rest;
+        if (cufftSetStream(h, p->st) != CUFFT_SUCCESS) return ERR_CUFFT;
+        cufftResult r;
+        if (p->opt.precision) {
+            cufftComplex *d = reinterpret_cast<cufftComplex *>(p->d_grid) + done * plane;
+            r = cufftExecC2C(h, d, d, dir);
+        } else {
+            cufftDoubleComplex *d = reinterpret_cast<cufftDoubleComplex *>(p->d_grid) + done * plane;
+            r = cufftExecZ2Z(h, d, d, dir);
+        }
+        if (r != CUFFT_SUCCESS) return ERR_CUFFT;
+        done += b;
+    }
+    return OK;
+}
+
+template <typename T>
+static int execute_t(Plan *p, void *d_vis, const void *d_wgt, void *d_dirty) {
+    cudaStream_t st = p->st;
+    const DevGeom &g = p->dg;
+    const GridParams &gp = p->gp;
+    size_t gbytes = (size_t)gp.nf1 * gp.nf2 * gp.nf3 * 2 * sizeof(T);
+    int s;
+    if (p->type == 1) {
+        launch_vis_prep<T>(g, p->dw, p->d_foc, d_vis, d_wgt, p->d_perm, p->d_cs, st);
+        CU_TRY(cudaMemsetAsync(p->d_grid, 0, gbytes, st));
+        s = launch_spread<T>(g, p->smem, p->d_bin_start, p->d_bin_count, p->d_sub_end, p->d_rec, p->d_cs,
+                             p->d_grid, p->d_wcoef, p->nsm, st);
+        if (s) return s;
+        s = run_fft(p, CUFFT_INVERSE);           // +1, cuft.cu:127-143
+        if (s) return s;
+        launch_correct_m2d<T>(p->dc, p->d_grid, d_dirty, st);
+    } else {
+        launch_zero_pad<T>(p->nx, p->ny, gp.nf1, gp.nf2, gp.nf3, p->d_grid, st);
+        launch_correct_d2m<T>(p->dc, d_dirty, p->d_grid, st);
+        s = run_fft(p, CUFFT_FORWARD);           // -1
+        if (s) return s;
+        s = launch_interp<T>(g, p->smem, p->d_bin_start, p->d_bin_count, p->d_sub_end, p->d_rec, p->d_grid,
+                             p->d_cs, p->d_wcoef, p->nsm, st);
+        if (s) return s;
+        launch_vis_out<T>(g, p->dw, p->d_foc, p->d_cs, p->d_perm, d_wgt, d_vis, st);
+    }
+    CU_TRY(cudaGetLastError());
+    return OK;
+}
+
+int plan_execute(Plan *p, void *d_vis, const void *d_wgt, void *d_dirty) {
+    if (!p || !p->ready || !d_vis || !d_dirty) return ERR_ARG;
+    return p->opt.precision ? execute_t<float>(p, d_vis, d_wgt, d_dirty)
+                            : execute_t<double>(p, d_vis, d_wgt, d_dirty);
+}
+
+}  // namespace curig

@@ -1,0 +1,142 @@
+/*
+ * curig_b200 -- C ABI of the B200-native ms2dirty / dirty2ms gridder.
+ *
+ * Shared library: curig_b200/libcurafft.so (same file name as the reference's
+ * build product, Makefile:177-178 / setup.py:24).  All entry points are
+ * extern "C", take plain pointers and sizes, and return an int status:
+ *   0 ok, 1 generic error (the reference's code), 2 bad sigma, 3 bad argument,
+ *   4 CUDA error, 5 cuFFT error, 6 out of device memory, 7 NaN/Inf input,
+ *   8 unsupported option, 9 no learned window reaches the requested epsilon.
+ * No entry point calls exit(); errors are returned (the reference exits the
+ * process through checkCudaErrors, include/cuda_sample/helper_cuda.h:583-595).
+ *
+ * Conventions shared with the reference (include/cugridder.h:12-21,
+ * src/astro/cugridder.cu:330-612):
+ *   uvw    [nrow][3] float64, metres (u, v, w per row)
+ *   vis    [nrow] (reference ABI) or [nrow][nchan] complex
+ *   wgt    same shape as vis, real, may be NULL; it multiplies in both
+ *          directions (src/astro/ra_exec.cu:103, ra_exec.cu:81 -> utils.cu:189)
+ *   dirty  [nxdirty][nydirty] complex, row-major; pixel (ix, iy) is at
+ *          l = (ix - nxdirty/2) * pixsize_x, m = (iy - nydirty/2) * pixsize_y
+ *   sign   sign of the w term: phase = f/c (u l + v m + sign w (n - 1))
+ *   ms2dirty: dirty = sum wgt vis e^{+2 pi i phase} / n
+ *   dirty2ms: vis   = wgt sum_pix dirty / n e^{-2 pi i phase}
+ */
+#ifndef CURIG_H
+#define CURIG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+#include <complex>
+typedef std::complex<double> curig_cdouble;
+extern "C" {
+#else
+#include <complex.h>
+typedef double _Complex curig_cdouble;
+#endif
+
+/* ---------------------------------------------------------------- reference ABI
+ * Single channel (freq), FP64, host buffers; the library allocates, copies and
+ * frees all device memory inside the call.  fov in degrees; pixel sizes are
+ * fov/180*pi/nxdirty and fov/180*pi/nydirty (src/astro/cugridder.cu:48-49).
+ */
+/* replaces ms2dirty_1, include/cugridder.h:15-16 (src/astro/cugridder.cu:594-599) */
+int ms2dirty_1(int nrow, int nxdirty, int nydirty, double fov, double freq, double *uvw,
+               curig_cdouble *vis, curig_cdouble *dirty, double epsilon, double sigma, int sign);
+/* replaces ms2dirty_2, include/cugridder.h:13-14 (src/astro/cugridder.cu:587-592) */
+int ms2dirty_2(int nrow, int nxdirty, int nydirty, double fov, double freq, double *uvw,
+               curig_cdouble *vis, double *wgt, curig_cdouble *dirty, double epsilon, double sigma,
+               int sign);
+/* replaces dirty2ms_1, include/cugridder.h:17-18 (src/astro/cugridder.cu:601-606); vis is the output */
+int dirty2ms_1(int nrow, int nxdirty, int nydirty, double fov, double freq, double *uvw,
+               curig_cdouble *vis, curig_cdouble *dirty, double epsilon, double sigma, int sign);
+/* replaces dirty2ms_2, include/cugridder.h:19-20 (src/astro/cugridder.cu:608-612) */
+int dirty2ms_2(int nrow, int nxdirty, int nydirty, double fov, double freq, double *uvw,
+               curig_cdouble *vis, double *wgt, curig_cdouble *dirty, double epsilon, double sigma,
+               int sign);
+
+/* ---------------------------------------------------------------- options */
+typedef struct curig_opts {
+    int precision;        /* 0: FP64 (default), 1: FP32 gridding (FP64 w-phase and correction) */
+    int window;           /* 0: ES kernel (default), 1: learned window (curig_set_window) */
+    int bin_xy;           /* bin edge in cells, 0 = automatic */
+    int sub;              /* visibilities per sub-problem, 0 = automatic */
+    int64_t smem_budget;  /* shared-memory bytes per tile CTA, 0 = automatic */
+    void *stream;         /* cudaStream_t for the device-pointer API, NULL = legacy stream */
+} curig_opts;
+
+void curig_default_opts(curig_opts *opts);
+
+/* ---------------------------------------------------------------- one-shot, host buffers
+ * Multi-channel generalisation of the reference ABI (which uses freq[0] only,
+ * python/curagridder/curagridder.py:92): all nchan channels are folded into one
+ * transform and the dirty image is their sum.  vis/wgt/dirty element type
+ * follows opts->precision (complex128/float64 or complex64/float32).  pixsize
+ * in radians.  Replaces per-channel loops over ms2dirty_2 / dirty2ms_2.
+ */
+int curig_ms2dirty(int64_t nrow, int nchan, int nxdirty, int nydirty, double pixsize_x,
+                   double pixsize_y, const double *freq, const double *uvw, const void *vis,
+                   const void *wgt, void *dirty, double epsilon, double sigma, int sign,
+                   const curig_opts *opts);
+int curig_dirty2ms(int64_t nrow, int nchan, int nxdirty, int nydirty, double pixsize_x,
+                   double pixsize_y, const double *freq, const double *uvw, void *vis,
+                   const void *wgt, const void *dirty, double epsilon, double sigma, int sign,
+                   const curig_opts *opts);
+
+/* ---------------------------------------------------------------- plan API, device pointers
+ * C counterpart of gridder_setting / gridder_execution / gridder_destroy
+ * (include/cugridder.h:8-11): create once, set points once (device uvw,
+ * host frequencies), execute many times on new visibilities / images.
+ * type 1: ms2dirty (vis -> dirty), type 2: dirty2ms (dirty -> vis).
+ * The uvw buffer must stay valid while the plan executes.
+ */
+typedef struct curig_plan_s *curig_plan;
+int curig_makeplan(int type, int nxdirty, int nydirty, double pixsize_x, double pixsize_y,
+                   double epsilon, double sigma, int sign, const curig_opts *opts,
+                   curig_plan *plan);
+int curig_setpts(curig_plan plan, int64_t nrow, int nchan, const double *d_uvw,
+                 const double *h_freq);
+/* separate u, v, w device arrays with an element stride (1: SoA, 3: AoS) */
+int curig_setpts_uvw(curig_plan plan, int64_t nrow, int nchan, const double *d_u,
+                     const double *d_v, const double *d_w, int stride, const double *h_freq);
+int curig_execute(curig_plan plan, void *d_vis, const void *d_wgt, void *d_dirty);
+int curig_destroy(curig_plan plan);
+/* info[0..7] = nf1, nf2, nf3, kw, bin_xy, bin_z, n_bins, window kind;
+ * dinfo[0..5] = beta, gamma, h, w centre, w half width, n-1 centre */
+int curig_plan_info(curig_plan plan, int *info, double *dinfo);
+
+/* ---------------------------------------------------------------- learned window
+ * Register a piecewise-polynomial window for support width kw: coef is
+ * [kw][degree+1], interval d covers t in [d - kw/2, d + 1 - kw/2], variable
+ * s = 2 (t - d + kw/2) - 1 in [-1, 1], highest power first.  eps_reached is
+ * the relative error the window reaches against the exact DFT; a plan with
+ * opts.window = 1 picks the narrowest registered window with
+ * eps_reached <= epsilon.  No counterpart in the reference (its kernel is the
+ * fixed ES function, src/fourier/conv.cu:17-25).
+ */
+int curig_set_window(int kw, int degree, const double *coef, double eps_reached);
+void curig_clear_windows(void);
+
+/* ---------------------------------------------------------------- host-only helpers
+ * Sizes and scalars a transform would use, computed on the host without a GPU:
+ * iout[0..3] = nf1, nf2, nf3, kw; dout[0..5] = beta, gamma, h, w centre,
+ * w half width, n-1 centre.  wmin/wmax are the effective (f/c * sign * 2 pi)
+ * w extremes.  Restates setup_conv_opts (src/fourier/conv_interp_invoker.cu:46-116),
+ * get_num_cells (conv_interp_invoker.cu:29-44), set_nhg_type3
+ * (contrib/common.cpp:161-195) and setup_gridder_plan (src/astro/cugridder.cu:29-101).
+ */
+int curig_grid_params(int nxdirty, int nydirty, double pixsize_x, double pixsize_y, double wmin,
+                      double wmax, double epsilon, double sigma, int *iout, double *dout);
+/* Kernel Fourier transform of the ES window on fine-grid indices 0..nf/2,
+ * including the (-1)^k half-grid factor; out has nf/2+1 entries and equals the
+ * reference's fwkerhalf (src/fourier/deconv.cu:13-24, 60-102) times e^-beta. */
+int curig_psi_hat(int nf, double epsilon, double sigma, double *out);
+
+/* Last error text of this thread (static storage, empty if none). */
+const char *curig_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CURIG_H */
