@@ -1,0 +1,370 @@
+#!/usr/bin/env python
+"""Benchmark: visibilities/s of ms2dirty + dirty2ms on one B200 (or N, weak scaling).
+
+Workload (the 4096^2 configuration): 1e7 rows x 16 channels (0.9-1.1 GHz)
+= 1.6e8 visibilities, 4096 x 4096 image, fov 3 deg, sigma 2, epsilon 1e-5,
+u,v from an isotropic Gaussian baseline density (sigma = 0.3 R, truncated at
+R, R * fov / lambda_min = 0.47 * 4096 pixels), w uniform in +-1000 m, complex
+normal visibilities, weights uniform in (0.5, 1]; seeded synthetic data
+generated on the device (no dataset exists for this configuration).
+
+One step = set points (w range, sizing, binning) + ms2dirty + dirty2ms over
+the whole visibility set, inputs resident in HBM (`value`); `e2e` is the same
+step through the C ABI one-shot calls (curig_ms2dirty / curig_dirty2ms) from
+pinned host buffers, host<->device copies inside the timed region.  For N > 1
+each rank grids its own 1.6e8 visibilities and the partial dirty images are
+summed with one NCCL all-reduce before the degridding (weak scaling).
+
+`--impl reference` times the reference's CPU path for this transform (its
+explicit FP64 DFT, python/curagridder/test_wst.py:15-32, restated in C/OpenMP
+in oracle/dft.c) on the host cores over a bounded sample, extrapolated to the
+full workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+C = 299792458.0
+METRIC = "vis/s ms2dirty & dirty2ms at eps=1e-5: learned-kernel vs ES, same B200"
+
+
+def args_():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="curig", choices=["curig", "reference"])
+    ap.add_argument("--nrow", type=int, default=10_000_000)
+    ap.add_argument("--nchan", type=int, default=16)
+    ap.add_argument("--npix", type=int, default=4096)
+    ap.add_argument("--fov", type=float, default=3.0)
+    ap.add_argument("--eps", type=float, default=1e-5)
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--window", default="auto", choices=["auto", "es", "learned"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--accumulate", type=int, default=0, help="FP32 tile accumulation: 0 int32 fixed point, 1 float atomics")
+    ap.add_argument("--bin", type=int, default=0, help="bin edge in cells (0 automatic)")
+    ap.add_argument("--smem", type=int, default=0, help="shared-memory budget per tile CTA (bytes)")
+    return ap.parse_args()
+
+
+def workload(torch, nrow, nchan, npix, fov, seed, device):
+    """Seeded synthetic visibilities on the device."""
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    freq = np.linspace(0.9e9, 1.1e9, nchan) if nchan > 1 else np.array([1.0e9])
+    lam_min = C / freq.max()
+    R = 0.47 * npix * lam_min / (fov * np.pi / 180)
+    s = 0.3 * R
+    uv = torch.randn((nrow, 2), generator=g, device=device, dtype=torch.float64) * s
+    for _ in range(64):                                  # truncate the Gaussian at R
+        bad = (uv * uv).sum(1) > R * R
+        nb = int(bad.sum())
+        if nb == 0:
+            break
+        uv[bad] = torch.randn((nb, 2), generator=g, device=device, dtype=torch.float64) * s
+    w = (torch.rand((nrow, 1), generator=g, device=device, dtype=torch.float64) * 2 - 1) * 1000.0
+    uvw = torch.cat([uv, w], 1).contiguous()
+    vis = torch.complex(torch.randn((nrow, nchan), generator=g, device=device),
+                        torch.randn((nrow, nchan), generator=g, device=device))
+    wgt = 1.0 - torch.rand((nrow, nchan), generator=g, device=device) * 0.5   # (0.5, 1]
+    return freq, uvw, vis.contiguous(), wgt.contiguous()
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region (recipe's clocks line)."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        self.p = None
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+            self.f.close()
+
+    def summary(self):
+        try:
+            rows = [l.split(",") for l in open(self.path).read().strip().splitlines() if l.strip()]
+        except Exception:
+            return None
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = max(float(r[2]) for r in rows)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip() == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def measured_peak():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"], "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def cpu_baseline(uvw_h, freq, vis_h, wgt_h, npix, fov, target_s):
+    """Reference CPU path (explicit FP64 DFT, oracle/dft.c port) on a bounded
+    sample: nv visibilities x np pixels, extrapolated to full-image vis/s."""
+    from oracle import dft
+    psx = fov * np.pi / 180 / npix
+    nchan = len(freq)
+    rng = np.random.default_rng(0)
+    nrow_s = max(1, 20000 // nchan)
+    u = uvw_h[:nrow_s]
+    v = vis_h[:nrow_s]
+    w = wgt_h[:nrow_s]
+    npx, t1 = 64, 0.0
+    while t1 < 0.5 and npx < npix * npix:                  # calibrate to ~target_s seconds
+        npx *= 4
+        t0 = time.perf_counter()
+        dft.ms2dirty_dft(u, freq, v, w, npix, npix, psx, psx, -1, pix=rng.integers(0, npix * npix, npx))
+        t1 = time.perf_counter() - t0
+    npx = int(min(npix * npix, max(64, npx * target_s / max(t1, 1e-3))))
+    pix = rng.integers(0, npix * npix, npx)
+    t0 = time.perf_counter()
+    dft.ms2dirty_dft(u, freq, v, w, npix, npix, psx, psx, -1, pix=pix)
+    t = time.perf_counter() - t0
+    rate = nrow_s * nchan * npx / t                          # pixel * vis / s
+    vis_per_s = rate / (2.0 * npix * npix)                   # ms2dirty + dirty2ms over the full image
+    return {"value": vis_per_s, "unit": "vis/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"{nrow_s * nchan} vis x {npx} pixels of the {npix}^2 image, FP64 DFT "
+                      f"(oracle/dft.c, OpenMP), {t:.1f} s; extrapolated to ms2dirty+dirty2ms over "
+                      f"all pixels", "pixel_vis_per_s": rate}
+
+
+def main():
+    a = args_()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        return reference_arm(a, rank, world)
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    import curig_b200 as CG
+    from curig_b200.plan import GridderPlan, launch_count, set_timing
+
+    freq, uvw, vis, wgt = workload(torch, a.nrow, a.nchan, a.npix, a.fov, a.seed + rank, dev)
+    M = a.nrow * a.nchan
+    psx = a.fov * np.pi / 180 / a.npix
+    cdt = torch.complex64 if a.precision == "fp32" else torch.complex128
+    rdt = torch.float32 if a.precision == "fp32" else torch.float64
+    vis = vis.to(cdt)
+    wgt = wgt.to(rdt)
+    window = "es" if a.window in ("auto", "es") else "learned"
+    if a.window in ("auto", "learned"):
+        try:
+            from curig_b200 import learned
+            if learned.load_default_windows() and a.window == "auto":
+                window = "learned"
+        except Exception:
+            window = "es" if a.window == "auto" else "learned"
+    stream = torch.cuda.current_stream()
+    plan = GridderPlan(1, a.npix, a.npix, psx, psx, a.eps, 2.0, -1, precision=a.precision,
+                       window=window, stream=stream, bin_xy=a.bin, smem_budget=a.smem,
+                       accumulate=a.accumulate)
+    dirty = torch.empty((a.npix, a.npix), dtype=cdt, device=dev)
+    vout = torch.empty_like(vis)
+
+    def step():
+        plan.setpts(uvw, freq)
+        plan.execute_dir(1, vis, wgt, dirty)
+        if world > 1:
+            torch.distributed.all_reduce(dirty)
+        plan.execute_dir(2, vout, wgt, dirty)
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+    set_timing(True)
+    stages = []
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    n0 = launch_count()
+    with Clocks(local) as clk:
+        ev0.record(stream)
+        for _ in range(a.steps):
+            step()
+            stages.append(plan.timings())
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    launches = launch_count() - n0
+    set_timing(False)
+    ms = ev0.elapsed_time(ev1) / a.steps
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    value = M * world / (ms / 1e3)
+    info = plan.info()
+    st = {k: float(np.mean([s[k] for s in stages])) for k in stages[0]}
+
+    # roofline of the dominant kernel (algorithmic bytes per launch, live event times)
+    c = 8 if a.precision == "fp32" else 16
+    r = c // 2
+    G = info["nf1"] * info["nf2"] * info["nf3"]
+    alg = {"spread": 24 * a.nrow + M * (c + r) + G * c,
+           "interp": G * c + 24 * a.nrow + M * (r + c)}
+    dom = "spread" if st["spread"] >= st["interp"] else "interp"
+    peak, peak_kind = measured_peak()
+    achieved = alg[dom] / (st[dom] / 1e3) / 1e9
+    traffic = None
+    try:
+        prof = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+        key = f"{dom}_{a.precision}_kw{info['kw']}"
+        if key in prof:
+            traffic = prof[key]["bytes_per_launch"]
+    except Exception:
+        pass
+    roof = {"bound": "hbm", "kernel": f"k_{dom}", "achieved": round(achieved, 1), "peak": peak,
+            "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+            "traffic": traffic, "algorithmic_bytes": alg[dom], "kernel_ms": round(st[dom], 3)}
+
+    # e2e through the C ABI with pinned host buffers
+    e2e = None
+    if not a.no_e2e:
+        import ctypes
+        from curig_b200 import _lib
+        h_uvw = uvw.cpu().pin_memory()
+        h_vis = vis.cpu().pin_memory()
+        h_wgt = wgt.cpu().pin_memory()
+        h_dirty = torch.empty((a.npix, a.npix), dtype=cdt).pin_memory()
+        h_vout = torch.empty_like(h_vis).pin_memory()
+        fr = np.ascontiguousarray(freq, dtype=np.float64)
+        opts = _lib.make_opts(1 if a.precision == "fp32" else 0, 1 if window == "learned" else 0,
+                              a.bin, 0, a.smem, stream.cuda_stream, a.accumulate)
+
+        def e2e_step():
+            s1 = _lib.lib.curig_ms2dirty(a.nrow, a.nchan, a.npix, a.npix, psx, psx, fr.ctypes.data,
+                                         h_uvw.data_ptr(), h_vis.data_ptr(), h_wgt.data_ptr(),
+                                         h_dirty.data_ptr(), a.eps, 2.0, -1, ctypes.byref(opts))
+            s2 = _lib.lib.curig_dirty2ms(a.nrow, a.nchan, a.npix, a.npix, psx, psx, fr.ctypes.data,
+                                         h_uvw.data_ptr(), h_vout.data_ptr(), h_wgt.data_ptr(),
+                                         h_dirty.data_ptr(), a.eps, 2.0, -1, ctypes.byref(opts))
+            _lib.check(s1, "curig_ms2dirty")
+            _lib.check(s2, "curig_dirty2ms")
+
+        for _ in range(min(a.warmup, 2)):
+            e2e_step()
+        ke = max(1, min(a.steps, 3))
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(ke):
+            e2e_step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ems = ev0.elapsed_time(ev1) / ke
+        bi = 2 * h_uvw.numel() * 8 + h_vis.numel() * h_vis.element_size() + \
+            2 * h_wgt.numel() * h_wgt.element_size() + h_dirty.numel() * h_dirty.element_size()
+        bo = h_dirty.numel() * h_dirty.element_size() + h_vout.numel() * h_vout.element_size()
+        e2e = {"value": M / (ems / 1e3), "unit": "vis/s", "h2d_bytes_per_step": int(bi),
+               "d2h_bytes_per_step": int(bo), "ms_per_step": round(ems, 3), "steps": ke,
+               "api": "curig_ms2dirty + curig_dirty2ms (C ABI, pinned host buffers)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu:
+        n = max(1, 20000 // a.nchan)
+        cpu = cpu_baseline(uvw[:n].cpu().numpy(), freq, vis[:n].cpu().numpy().astype(np.complex128),
+                           wgt[:n].cpu().numpy().astype(np.float64), a.npix, a.fov, a.cpu_seconds)
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": "vis/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if a.precision == "fp32" else "f64",
+            "data": "synthetic (seeded Gaussian uv density, uniform w, complex-normal vis; generated on device)",
+            "config": {"workload": f"ms2dirty+dirty2ms, {a.nrow} rows x {a.nchan} ch "
+                                   f"({a.nrow * a.nchan} vis), {a.npix}^2, fov {a.fov} deg, "
+                                   f"eps {a.eps}, sigma 2", "window": window,
+                       "precision": a.precision, "kw": info["kw"], "nf": [info["nf1"], info["nf2"], info["nf3"]],
+                       "bin_xy": info["bin_xy"], "accumulate": ["int32 fixed point" if a.precision == "fp32" else "float atomics", "float atomics"][a.accumulate],
+                       "l2": "inputs (>= 1.9 GB per step) larger than L2; no flush needed",
+                       "parallelism": f"dp{world} (visibility shards, all-reduce of dirty)" if world > 1 else "single GPU"},
+            "e2e": e2e, "gpu_launches": int(launches / a.steps), "clocks": clk.summary(),
+            "roofline": roof, "cpu_baseline": cpu,
+            "stages_ms": {k: round(v, 3) for k, v in st.items()},
+        }
+        print(json.dumps(out), flush=True)
+    plan.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def reference_arm(a, rank, world):
+    """CPU explicit DFT of the reference (oracle/dft.c port) on the host cores."""
+    if rank != 0:
+        return
+    rng = np.random.default_rng(a.seed)
+    nchan = a.nchan
+    freq = np.linspace(0.9e9, 1.1e9, nchan) if nchan > 1 else np.array([1.0e9])
+    R = 0.47 * a.npix * (C / freq.max()) / (a.fov * np.pi / 180)
+    nrow = max(1, 20000 // nchan)
+    uv = rng.standard_normal((nrow, 2)) * 0.3 * R
+    uv[np.sum(uv * uv, 1) > R * R] *= 0.5
+    uvw = np.concatenate([uv, rng.uniform(-1000, 1000, (nrow, 1))], 1)
+    vis = rng.standard_normal((nrow, nchan)) + 1j * rng.standard_normal((nrow, nchan))
+    wgt = 1.0 - 0.5 * rng.random((nrow, nchan))
+    per = max(2.0, min(a.cpu_seconds, 150.0 / max(1, a.steps + a.warmup)))
+    for _ in range(a.warmup):
+        cpu_baseline(uvw, freq, vis, wgt, a.npix, a.fov, per / 4)
+    vals = [cpu_baseline(uvw, freq, vis, wgt, a.npix, a.fov, per) for _ in range(a.steps)]
+    v = float(np.median([x["value"] for x in vals]))
+    cb = dict(vals[-1])
+    cb["value"] = v
+    out = {"impl": "reference", "metric": METRIC, "value": v, "unit": "vis/s", "n_gpus": world,
+           "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * (a.nrow * a.nchan) / v,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (seeded Gaussian uv density, uniform w, complex-normal vis)",
+           "config": {"workload": f"ms2dirty+dirty2ms, {a.nrow} rows x {a.nchan} ch, {a.npix}^2, "
+                                  f"fov {a.fov} deg, eps {a.eps}", "path": "explicit FP64 DFT on host cores"},
+           "cpu_baseline": cb,
+           "e2e": {"value": v, "unit": "vis/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

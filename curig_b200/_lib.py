@@ -46,12 +46,12 @@ dirty2ms_2.restype = c_int
 
 class CurigOpts(ctypes.Structure):
     _fields_ = [("precision", c_int), ("window", c_int), ("bin_xy", c_int), ("sub", c_int),
-                ("smem_budget", c_int64), ("stream", c_void_p)]
+                ("smem_budget", c_int64), ("stream", c_void_p), ("accumulate", c_int), ("reserved", c_int)]
 
 
 def make_opts(precision: int = 0, window: int = 0, bin_xy: int = 0, sub: int = 0,
-              smem_budget: int = 0, stream: int | None = None) -> CurigOpts:
-    return CurigOpts(precision, window, bin_xy, sub, smem_budget, stream or None)
+              smem_budget: int = 0, stream: int | None = None, accumulate: int = 0) -> CurigOpts:
+    return CurigOpts(precision, window, bin_xy, sub, smem_budget, stream or None, accumulate, 0)
 
 
 _P = c_void_p
@@ -69,6 +69,14 @@ lib.curig_setpts_uvw.argtypes = [c_void_p, c_int64, c_int, _P, _P, _P, c_int, _P
 lib.curig_setpts_uvw.restype = c_int
 lib.curig_execute.argtypes = [c_void_p, _P, _P, _P]
 lib.curig_execute.restype = c_int
+lib.curig_execute_dir.argtypes = [c_void_p, c_int, _P, _P, _P]
+lib.curig_execute_dir.restype = c_int
+lib.curig_set_timing.argtypes = [c_int]
+lib.curig_set_timing.restype = None
+lib.curig_plan_timings.argtypes = [c_void_p, ctypes.POINTER(c_double), c_int]
+lib.curig_plan_timings.restype = c_int
+lib.curig_launch_count.argtypes = []
+lib.curig_launch_count.restype = c_int64
 lib.curig_destroy.argtypes = [c_void_p]
 lib.curig_destroy.restype = c_int
 lib.curig_plan_info.argtypes = [c_void_p, ctypes.POINTER(c_int), ctypes.POINTER(c_double)]

@@ -29,6 +29,7 @@ static Options to_options(const curig_opts *o) {
         opt.sub = o->sub;
         opt.smem_budget = o->smem_budget > 0 ? (size_t)o->smem_budget : 0;
         opt.stream = (cudaStream_t)o->stream;
+        opt.smode = o->accumulate;
     }
     return opt;
 }
@@ -179,6 +180,22 @@ extern "C" int curig_execute(curig_plan h, void *d_vis, const void *d_wgt, void 
     if (s != OK) return fail(s, h->p->last_error.empty() ? "execute failed" : h->p->last_error);
     return OK;
 }
+
+extern "C" int curig_execute_dir(curig_plan h, int type, void *d_vis, const void *d_wgt, void *d_dirty) {
+    if (!h) return fail(ERR_ARG, "null plan");
+    int s = plan_execute(h->p, d_vis, d_wgt, d_dirty, type);
+    if (s != OK) return fail(s, h->p->last_error.empty() ? "execute failed" : h->p->last_error);
+    return OK;
+}
+
+extern "C" void curig_set_timing(int on) { set_timing(on != 0); }
+
+extern "C" int curig_plan_timings(curig_plan h, double *out, int n) {
+    if (!h || !out) return fail(ERR_ARG, "null argument");
+    return plan_timings(h->p, out, n);
+}
+
+extern "C" int64_t curig_launch_count(void) { return launch_count(); }
 
 extern "C" int curig_destroy(curig_plan h) {
     if (!h) return OK;

@@ -2,9 +2,9 @@
 //
 // Replaces, on the ms2dirty / dirty2ms path of the reference:
 //   get_effective_coordinate + rescaling + pre_stage_1/2 + transpose
-//       (precomp.cu:48-79, utils.cu:56-154, cuft.cu:19-92)  -> k_bin_count / k_bin_scatter / k_vis_prep
-//   conv_3d_nputsdriven (conv.cu:144-228)                  -> k_spread (tile-binned)
-//   interp_3d_nputsdriven (interp.cu:143-227)              -> k_interp (tile-staged)
+//       (precomp.cu:48-79, utils.cu:56-154, cuft.cu:19-92)  -> k_bin_keys + radix sort + k_records / k_vis_prep
+//   conv_3d_nputsdriven (conv.cu:144-228)                  -> k_spread_t / k_spread (tile-binned)
+//   interp_3d_nputsdriven (interp.cu:143-227)              -> k_interp_t / k_interp (tile-staged)
 //   w_term_dft + deconv_2d + w_term_deconv + div_n_lm
 //       (cuft.cu:520-572, deconv.cu:236-417, ra_exec.cu:22-52) -> k_correct_m2d (one pass)
 //   div_n_lm + w_term_deconv + deconv_2d + w_term_idft
@@ -12,6 +12,7 @@
 //   matrix_elementwise_multiply + shift_corr (utils.cu:156-192, ra_exec.cu:56-89) -> k_vis_out
 //   thrust min/max over w (utils.cu:42-53)                  -> k_wrange
 #include "kernels.cuh"
+#include "plan.h"
 
 #include <cub/cub.cuh>
 
@@ -145,9 +146,12 @@ __global__ void k_wrange(const double *__restrict__ w, int stride, long long nro
 }
 
 // ------------------------------------------------------------------ binning
-__global__ void k_bin_count(DevGeom g, const double *__restrict__ uu, const double *__restrict__ vv,
-                            const double *__restrict__ ww, const double *__restrict__ foc,
-                            int *__restrict__ bin_count, int *__restrict__ rank, int *err) {
+// Sort key of one visibility: bin id in the high bits, its start cell inside
+// the bin's tile in the low cbits (so threads of a warp touch neighbouring
+// cells); 0xffffffff marks a visibility that could not be placed.
+__global__ void k_bin_keys(DevGeom g, const double *__restrict__ uu, const double *__restrict__ vv,
+                           const double *__restrict__ ww, const double *__restrict__ foc,
+                           unsigned *__restrict__ keys, int *__restrict__ vals, int *err) {
     const long long M = g.nrow * g.nchan;
     for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < M;
          j += (long long)gridDim.x * blockDim.x) {
@@ -157,97 +161,94 @@ __global__ void k_bin_count(DevGeom g, const double *__restrict__ uu, const doub
         VisLoc L;
         int e = vis_grid(g, uu, vv, ww, row, foc[ch], gx, gy, gz) ? locate(g, gx, gy, gz, L)
                                                                   : EF_NONFINITE;
+        unsigned key = 0xffffffffu;
         if (e) {
             atomicOr(err, e);
-            rank[j] = -1;
-            continue;
+        } else {
+            unsigned cell = g.cbits ? (unsigned)((L.lz * (g.by + 1) + L.ly) * (g.bx + 1) + L.lx) : 0u;
+            key = ((unsigned)L.bin << g.cbits) | cell;
         }
-        rank[j] = atomicAdd(&bin_count[L.bin], 1);
+        keys[j] = key;
+        vals[j] = (int)j;
     }
 }
 
-__global__ void k_nsub(const int *__restrict__ count, int *__restrict__ nsub, long long nb, int sub) {
-    for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < nb;
-         b += (long long)gridDim.x * blockDim.x)
-        nsub[b] = (count[b] + sub - 1) / sub;
+// first / one-past-last sorted position of every non-empty bin
+__global__ void k_bin_bounds(const unsigned *__restrict__ keys, long long M, int cbits,
+                             int *__restrict__ first, int *__restrict__ last) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < M;
+         i += (long long)gridDim.x * blockDim.x) {
+        unsigned k = keys[i];
+        if (k == 0xffffffffu) continue;
+        unsigned b = k >> cbits;
+        if (i == 0 || (keys[i - 1] >> cbits) != b || keys[i - 1] == 0xffffffffu) first[b] = (int)i;
+        if (i == M - 1 || keys[i + 1] == 0xffffffffu || (keys[i + 1] >> cbits) != b) last[b] = (int)i + 1;
+    }
 }
 
+__global__ void k_nsub(const int *__restrict__ first, const int *__restrict__ last, int *__restrict__ count,
+                       int *__restrict__ nsub, long long nb, int sub) {
+    for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < nb;
+         b += (long long)gridDim.x * blockDim.x) {
+        int c = last[b] - first[b];
+        count[b] = c;
+        nsub[b] = (c + sub - 1) / sub;
+    }
+}
+
+// Per sorted visibility: fractional offsets + packed start cell, and the
+// w-shift phase e^{i o_c w} (cuft.cu:19-39), computed in FP64.
 template <typename T>
-__global__ void k_bin_scatter(DevGeom g, const double *__restrict__ uu, const double *__restrict__ vv,
-                              const double *__restrict__ ww, const double *__restrict__ foc,
-                              const int *__restrict__ bin_start, const int *__restrict__ rank,
-                              R<T> *__restrict__ rec, int *__restrict__ perm) {
-    const long long M = g.nrow * g.nchan;
-    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < M;
-         j += (long long)gridDim.x * blockDim.x) {
-        int rk = rank[j];
-        if (rk < 0) { perm[j] = -1; continue; }
-        long long row = j / g.nchan;
-        int ch = (int)(j - row * g.nchan);
+__global__ void k_records(DevGeom g, const double *__restrict__ uu, const double *__restrict__ vv,
+                          const double *__restrict__ ww, const double *__restrict__ foc,
+                          const int *__restrict__ idx, long long M, R<T> *__restrict__ rec,
+                          C<T> *__restrict__ ph) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < M;
+         i += (long long)gridDim.x * blockDim.x) {
+        int j = idx[i];
+        int row = j / g.nchan;
+        int ch = j - row * g.nchan;
         double gx, gy, gz;
         VisLoc L;
         vis_grid(g, uu, vv, ww, row, foc[ch], gx, gy, gz);
         locate(g, gx, gy, gz, L);
-        int pos = bin_start[L.bin] + rk;
         R<T> r;
         r.x = (T)L.ux;
         r.y = (T)L.uy;
         r.z = (T)L.uz;
         if constexpr (sizeof(T) == 4) r.w = pack_cell_f(L.lx, L.ly, L.lz);
         else r.w = pack_cell_d(L.lx, L.ly, L.lz);
-        rec[pos] = r;
-        perm[j] = pos;
+        rec[i] = r;
+        double s, c;
+        sincos(g.o_center * w_eff(g, ww, row, foc[ch]), &s, &c);
+        ph[i] = C<T>{(T)c, (T)s};
     }
 }
 
-// c = vis * wgt * e^{i o_c w} in bin order (ra_exec.cu:98-104, cuft.cu:19-39).
+// c = vis * wgt * e^{i o_c w} gathered into bin order (ra_exec.cu:98-104).
 template <typename T>
-__global__ void k_vis_prep(DevGeom g, const double *__restrict__ ww, const double *__restrict__ foc,
-                           const C<T> *__restrict__ vis, const T *__restrict__ wgt,
-                           const int *__restrict__ perm, C<T> *__restrict__ cs) {
-    const long long M = g.nrow * g.nchan;
-    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < M;
-         j += (long long)gridDim.x * blockDim.x) {
-        int p = perm[j];
-        if (p < 0) continue;
-        long long row = j / g.nchan;
-        int ch = (int)(j - row * g.nchan);
-        double ph = g.o_center * w_eff(g, ww, row, foc[ch]);
-        double s, c;
-        sincos(ph, &s, &c);
-        C<T> v = vis[j];
-        double wt = wgt ? (double)wgt[j] : 1.0;
-        double vr = (double)v.x * wt, vi = (double)v.y * wt;
-        C<T> o;
-        o.x = (T)(vr * c - vi * s);
-        o.y = (T)(vr * s + vi * c);
-        cs[p] = o;
+__global__ void k_vis_prep(long long M, const int *__restrict__ idx, const C<T> *__restrict__ ph,
+                           const C<T> *__restrict__ vis, const T *__restrict__ wgt, C<T> *__restrict__ cs) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < M;
+         i += (long long)gridDim.x * blockDim.x) {
+        int j = idx[i];
+        C<T> v = vis[j], e = ph[i];
+        T wt = wgt ? wgt[j] : (T)1;
+        cs[i] = C<T>{(v.x * e.x - v.y * e.y) * wt, (v.x * e.y + v.y * e.x) * wt};
     }
 }
 
-// vis = interp * wgt * e^{-i o_c w} in input order (ra_exec.cu:56-89; the
-// reference's weight "divide" invoker launches the multiply kernel, utils.cu:189).
+// vis = interp * wgt * e^{-i o_c w} scattered back to input order
+// (ra_exec.cu:56-89; the reference's weight "divide" invoker multiplies, utils.cu:189).
 template <typename T>
-__global__ void k_vis_out(DevGeom g, const double *__restrict__ ww, const double *__restrict__ foc,
-                          const C<T> *__restrict__ os, const int *__restrict__ perm,
-                          const T *__restrict__ wgt, C<T> *__restrict__ vis) {
-    const long long M = g.nrow * g.nchan;
-    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < M;
-         j += (long long)gridDim.x * blockDim.x) {
-        int p = perm[j];
-        C<T> o;
-        if (p < 0) { o.x = 0; o.y = 0; vis[j] = o; continue; }
-        long long row = j / g.nchan;
-        int ch = (int)(j - row * g.nchan);
-        double ph = -g.o_center * w_eff(g, ww, row, foc[ch]);
-        double s, c;
-        sincos(ph, &s, &c);
-        C<T> v = os[p];
-        double wt = wgt ? (double)wgt[j] : 1.0;
-        double vr = (double)v.x * wt, vi = (double)v.y * wt;
-        o.x = (T)(vr * c - vi * s);
-        o.y = (T)(vr * s + vi * c);
-        vis[j] = o;
+__global__ void k_vis_out(long long M, const int *__restrict__ idx, const C<T> *__restrict__ ph,
+                          const C<T> *__restrict__ os, const T *__restrict__ wgt, C<T> *__restrict__ vis) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < M;
+         i += (long long)gridDim.x * blockDim.x) {
+        int j = idx[i];
+        C<T> v = os[i], e = ph[i];
+        T wt = wgt ? wgt[j] : (T)1;
+        vis[j] = C<T>{(v.x * e.x + v.y * e.y) * wt, (v.y * e.x - v.x * e.y) * wt};
     }
 }
 
@@ -436,6 +437,278 @@ k_interp(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__ b
     }
 }
 
+// ------------------------------------------------------------------ thread-per-visibility
+// Same sub-problem / tile structure, one thread per visibility: the kernel
+// values along x and y live in registers (compile-time width), the taps are
+// fully unrolled with immediate offsets, the w-axis value is evaluated per
+// plane, and shared-memory accumulation uses the native reduction
+// (red.shared.add).  Visibilities are sorted by start cell inside a bin, so
+// the 32 lanes of a warp update / read neighbouring cells.
+
+__device__ __forceinline__ void red_shared(float *p, float v) {
+    unsigned a = (unsigned)__cvta_generic_to_shared(p);
+    asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
+}
+__device__ __forceinline__ void red_shared(double *p, double v) {
+    unsigned a = (unsigned)__cvta_generic_to_shared(p);
+    asm volatile("red.shared.add.f64 [%0], %1;" ::"r"(a), "d"(v) : "memory");
+}
+
+// Window value for tap d: ES (direct) or the Horner table in parameter space.
+template <typename T>
+__device__ __forceinline__ T win_tap(const DevGeom &g, const WinTab<T> &tab, T u, int d) {
+    if (g.wkind == 0) return win_eval<T>(g, nullptr, u, d);
+    T s = (T)2 * u - (T)1;
+    T v = tab.c[d][0];
+#pragma unroll
+    for (int i = 1; i < TAB_DEG; ++i) v = fma(v, s, tab.c[d][i]);
+    return v;
+}
+
+template <typename T>
+__device__ __forceinline__ void sub_range(const DevGeom &g, const int *bin_start, const int *bin_count,
+                                          const int *sub_end, int s, long long &b, int &first, int &last) {
+    b = find_bin(sub_end, g.nbins, s);
+    int cnt = bin_count[b];
+    int nsb = (cnt + g.sub - 1) / g.sub;
+    int chunk = s - (sub_end[b] - nsb);
+    first = bin_start[b] + chunk * g.sub;
+    last = min(first + g.sub, bin_start[b] + cnt);
+}
+
+// Exact fixed-point accumulation of the FP32 spreader.  Shared-memory float
+// atomics are a compare-and-swap loop on this part (about 9 updates / clock /
+// SM without conflicts), native 32-bit integer atomics run at about 28.  Each
+// term x (scaled by q = 2^(35 - e), 2^(e-1) <= max|c| < 2^e, so |x| < 2^35 for
+// window products <= 2) is split exactly as h * 2^18 + l with |l| <= 2^17
+// (rounding l to an integer: error <= 0.5 of 2^-35 max|c|), and h, l go to two
+// int32 accumulators per component.  With at most 4096 terms per cell
+// (sub <= 4096): |sum h| <= 2^12 * 2^18 = 2^30 and |sum l| <= 2^12 * 2^17 =
+// 2^29, so nothing overflows; the sums are exact and order-independent.
+constexpr int FIX_BITS = 35;   // the split point 2^18 is built into split_fix
+
+__device__ __forceinline__ void split_fix(float x, int &h, int &l) {
+    const float M = 12582912.0f;                       // 1.5 * 2^23: rounds to integers below 2^22
+    float t = fmaf(x, 3.814697265625e-06f, M);         // x * 2^-18, rounded to an integer
+    h = __float_as_int(t) - 0x4B400000;
+    float hf = t - M;
+    float lf = fmaf(hf, -262144.0f, x);                // x - h * 2^18, exact
+    l = __float_as_int(lf + M) - 0x4B400000;
+}
+
+template <typename T>
+__device__ __forceinline__ T block_absmax(const C<T> *__restrict__ cs, int first, int last, T *red) {
+    T m = 0;
+    for (int i = first + threadIdx.x; i < last; i += NTHREADS) {
+        C<T> c = cs[i];
+        m = fmax(m, fmax(fabs(c.x), fabs(c.y)));
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    T r = 0;
+#pragma unroll
+    for (int w = 0; w < NWARPS; ++w) r = fmax(r, red[w]);
+    return r;
+}
+
+template <typename T, int KW>
+__global__ void __launch_bounds__(NTHREADS)
+k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__ bin_count,
+           const int *__restrict__ sub_end, const R<T> *__restrict__ rec, const C<T> *__restrict__ cs,
+           C<T> *__restrict__ grid, const WinTab<T> tab) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ T redbuf[NWARPS];
+    const int ntile = g.tx * g.ty * g.tz;
+    const bool fix = sizeof(T) == 4 && g.smode == 0;   // FP32: exact int32 fixed point
+    const int csz = fix ? 16 : (int)sizeof(C<T>);      // bytes per complex cell
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int total = sub_end[g.nbins - 1];
+    const int tx = g.tx, txy = g.tx * g.ty;
+    const int nvec = (ntile * csz) / 16;
+    int *fhr = reinterpret_cast<int *>(smem);          // SoA planes: re-high, re-low, im-high, im-low
+    int *flr = fhr + ntile, *fhi = flr + ntile, *fli = fhi + ntile;
+    for (int s = blockIdx.x; s < total; s += gridDim.x) {
+        long long b;
+        int first, last;
+        sub_range<T>(g, bin_start, bin_count, sub_end, s, b, first, last);
+        float4 *tv = reinterpret_cast<float4 *>(smem);
+        for (int e = threadIdx.x; e < nvec; e += NTHREADS) tv[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (!fix)
+            for (int e = nvec * 16 / csz + threadIdx.x; e < ntile; e += NTHREADS)
+                reinterpret_cast<C<T> *>(smem)[e] = C<T>{0, 0};
+        T q = 1;
+        double qinv = 1;
+        if (fix) {
+            T m = block_absmax<T>(cs, first, last, redbuf);
+            int e = m > (T)0 ? ilogb(m) + 1 : 0;       // 2^(e-1) <= m < 2^e
+            q = (T)ldexp(1.0, FIX_BITS - e);
+            qinv = ldexp(1.0, e - FIX_BITS);
+        }
+        __syncthreads();
+        for (int i = first + threadIdx.x; i < last; i += NTHREADS) {
+            R<T> r = rec[i];
+            C<T> c = cs[i];
+            T kx[KW], ky[KW];
+#pragma unroll
+            for (int d = 0; d < KW; ++d) {
+                kx[d] = win_tap<T>(g, tab, r.x, d);
+                ky[d] = win_tap<T>(g, tab, r.y, d);
+            }
+            int cb = cell_bits(r.w);
+            int cell = ((cb >> 20) & 0xfff) * txy + ((cb >> 10) & 0x3ff) * tx + (cb & 0x3ff);
+            c.x *= q;
+            c.y *= q;
+#pragma unroll 1
+            for (int dz = 0; dz < KW; ++dz) {
+                T kz = win_tap<T>(g, tab, r.z, dz);
+                T cr = c.x * kz, ci = c.y * kz;
+                int pz = cell + dz * txy;
+#pragma unroll
+                for (int dy = 0; dy < KW; ++dy) {
+                    T ar = cr * ky[dy], ai = ci * ky[dy];
+                    int prow = pz + dy * tx;
+                    if constexpr (sizeof(T) == 4) {
+                        if (fix) {
+#pragma unroll
+                            for (int dx = 0; dx < KW; ++dx) {
+                                int h, l;
+                                split_fix(ar * kx[dx], h, l);
+                                atomicAdd(fhr + prow + dx, h);
+                                atomicAdd(flr + prow + dx, l);
+                                split_fix(ai * kx[dx], h, l);
+                                atomicAdd(fhi + prow + dx, h);
+                                atomicAdd(fli + prow + dx, l);
+                            }
+                            continue;
+                        }
+                    }
+                    T *row = reinterpret_cast<T *>(smem) + 2 * prow;
+#pragma unroll
+                    for (int dx = 0; dx < KW; ++dx) {
+                        atomicAdd(row + 2 * dx, ar * kx[dx]);
+                        atomicAdd(row + 2 * dx + 1, ai * kx[dx]);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        long long bxi = b % g.nbx, byi = (b / g.nbx) % g.nby, bzi = b / ((long long)g.nbx * g.nby);
+        int ox = (int)bxi * g.bx - g.hkw, oy = (int)byi * g.by - g.hkw;
+        int oz = g.zpad ? (int)bzi * g.bz - g.hkw : 0;
+        for (int row = warp, y = warp % g.ty, z = warp / g.ty; row < g.ty * g.tz; row += NWARPS) {
+            int gy = wrap3(oy + y, g.nf2);
+            int gz = g.zpad ? wrap3(oz + z, g.nf3) : z;
+            y += NWARPS;
+            while (y >= g.ty) { y -= g.ty; ++z; }
+            C<T> *grow = grid + ((long long)gz * g.nf2 + gy) * g.nf1;
+            for (int x = lane; x < g.tx; x += 32) {
+                int e = row * g.tx + x;
+                C<T> v;
+                if (fix) {
+                    v = C<T>{(T)(((double)fhr[e] * 262144.0 + (double)flr[e]) * qinv),
+                             (T)(((double)fhi[e] * 262144.0 + (double)fli[e]) * qinv)};
+                } else {
+                    v = reinterpret_cast<const C<T> *>(smem)[e];
+                }
+                if (v.x != (T)0 || v.y != (T)0) atomic_add_c(grow + wrap3(ox + x, g.nf1), v);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Stage the tile (wrapped rows of all its planes): rows are walked without
+// divisions and eight rows are in flight per warp before the shared stores.
+template <typename T>
+__device__ __forceinline__ void load_tile(const DevGeom &g, const C<T> *__restrict__ grid, C<T> *tile,
+                                          long long b, int warp, int lane) {
+    long long bxi = b % g.nbx, byi = (b / g.nbx) % g.nby, bzi = b / ((long long)g.nbx * g.nby);
+    int ox = (int)bxi * g.bx - g.hkw, oy = (int)byi * g.by - g.hkw;
+    int oz = g.zpad ? (int)bzi * g.bz - g.hkw : 0;
+    const int nrows = g.ty * g.tz;
+    constexpr int RB = 8;
+    for (int x0 = 0; x0 < g.tx; x0 += 32) {
+        const int x = x0 + lane;
+        const bool xin = x < g.tx;
+        const int gx = wrap3(ox + x, g.nf1);
+        int row = warp, y = warp % g.ty, z = warp / g.ty;
+        while (row < nrows) {
+            C<T> v[RB];
+            int rr[RB];
+#pragma unroll
+            for (int k = 0; k < RB; ++k) {
+                rr[k] = row;
+                if (xin && row < nrows) {
+                    int gy = wrap3(oy + y, g.nf2);
+                    int gz = g.zpad ? wrap3(oz + z, g.nf3) : z;
+                    v[k] = grid[((long long)gz * g.nf2 + gy) * g.nf1 + gx];
+                }
+                row += NWARPS;
+                y += NWARPS;
+                while (y >= g.ty) { y -= g.ty; ++z; }
+            }
+#pragma unroll
+            for (int k = 0; k < RB; ++k)
+                if (xin && rr[k] < nrows) tile[rr[k] * g.tx + x] = v[k];
+        }
+    }
+}
+
+template <typename T, int KW>
+__global__ void __launch_bounds__(NTHREADS)
+k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__ bin_count,
+           const int *__restrict__ sub_end, const R<T> *__restrict__ rec, const C<T> *__restrict__ grid,
+           C<T> *__restrict__ os, const WinTab<T> tab) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    C<T> *tile = reinterpret_cast<C<T> *>(smem);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int total = sub_end[g.nbins - 1];
+    const int tx = g.tx, txy = g.tx * g.ty;
+    for (int s = blockIdx.x; s < total; s += gridDim.x) {
+        long long b;
+        int first, last;
+        sub_range<T>(g, bin_start, bin_count, sub_end, s, b, first, last);
+        load_tile<T>(g, grid, tile, b, warp, lane);
+        __syncthreads();
+        for (int i = first + threadIdx.x; i < last; i += NTHREADS) {
+            R<T> r = rec[i];
+            T kx[KW], ky[KW];
+#pragma unroll
+            for (int d = 0; d < KW; ++d) {
+                kx[d] = win_tap<T>(g, tab, r.x, d);
+                ky[d] = win_tap<T>(g, tab, r.y, d);
+            }
+            int cb = cell_bits(r.w);
+            const C<T> *base = tile + ((cb >> 20) & 0xfff) * txy + ((cb >> 10) & 0x3ff) * tx + (cb & 0x3ff);
+            T ar = 0, ai = 0;
+#pragma unroll 1
+            for (int dz = 0; dz < KW; ++dz) {
+                T kz = win_tap<T>(g, tab, r.z, dz);
+                const C<T> *pz = base + dz * txy;
+                T sr = 0, si = 0;
+#pragma unroll
+                for (int dy = 0; dy < KW; ++dy) {
+                    const C<T> *row = pz + dy * tx;
+                    T rr = 0, ri = 0;
+#pragma unroll
+                    for (int dx = 0; dx < KW; ++dx) {
+                        C<T> v = row[dx];
+                        rr = fma(v.x, kx[dx], rr);
+                        ri = fma(v.y, kx[dx], ri);
+                    }
+                    sr = fma(rr, ky[dy], sr);
+                    si = fma(ri, ky[dy], si);
+                }
+                ar = fma(sr, kz, ar);
+                ai = fma(si, kz, ai);
+            }
+            os[i] = C<T>{ar, ai};
+        }
+        __syncthreads();
+    }
+}
+
 // ------------------------------------------------------------------ correction
 // Shared per-quarter-pixel factors: n, k' and psi3 depend on |l|, |m| only.
 struct QuarterPix {
@@ -590,93 +863,146 @@ static int grid_for(long long n, int per = NTHREADS) {
 
 void launch_wrange(const double *w, int stride, long long nrow, unsigned long long *keys, int *err,
                    cudaStream_t st) {
+    count_launch();
     k_wrange<<<grid_for(nrow), NTHREADS, 0, st>>>(w, stride, nrow, keys, err);
 }
 
-void launch_bin_count(const DevGeom &g, const double *u, const double *v, const double *w,
-                      const double *foc, int *bin_count, int *rank, int *err, cudaStream_t st) {
-    k_bin_count<<<grid_for(g.nrow * g.nchan), NTHREADS, 0, st>>>(g, u, v, w, foc, bin_count, rank, err);
+void launch_bin_keys(const DevGeom &g, const double *u, const double *v, const double *w, const double *foc,
+                     unsigned *keys, int *vals, int *err, cudaStream_t st) {
+    count_launch();
+    k_bin_keys<<<grid_for(g.nrow * g.nchan), NTHREADS, 0, st>>>(g, u, v, w, foc, keys, vals, err);
 }
 
-void launch_nsub(const int *count, int *nsub, long long nb, int sub, cudaStream_t st) {
-    k_nsub<<<grid_for(nb), NTHREADS, 0, st>>>(count, nsub, nb, sub);
+size_t sort_temp_bytes(long long M, int end_bit) {
+    size_t b = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, b, (const unsigned *)nullptr, (unsigned *)nullptr,
+                                    (const int *)nullptr, (int *)nullptr, (int)M, 0, end_bit);
+    return b;
+}
+
+int sort_pairs(void *tmp, size_t tmpb, const unsigned *kin, unsigned *kout, const int *vin, int *vout,
+               long long M, int end_bit, cudaStream_t st) {
+    count_launch(2 * ((end_bit + 7) / 8) + 1);      // upsweep/histogram + one pass per digit (approx.)
+    return cub::DeviceRadixSort::SortPairs(tmp, tmpb, kin, kout, vin, vout, (int)M, 0, end_bit, st) ==
+                   cudaSuccess ? 0 : ERR_CUDA;
+}
+
+void launch_bin_bounds(const unsigned *keys, long long M, int cbits, int *first, int *last, cudaStream_t st) {
+    count_launch();
+    k_bin_bounds<<<grid_for(M), NTHREADS, 0, st>>>(keys, M, cbits, first, last);
+}
+
+void launch_nsub(const int *first, const int *last, int *count, int *nsub, long long nb, int sub,
+                 cudaStream_t st) {
+    count_launch();
+    k_nsub<<<grid_for(nb), NTHREADS, 0, st>>>(first, last, count, nsub, nb, sub);
 }
 
 size_t scan_temp_bytes(long long n) {
-    size_t a = 0, b = 0;
-    cub::DeviceScan::ExclusiveSum(nullptr, a, (const int *)nullptr, (int *)nullptr, (int)n);
+    size_t b = 0;
     cub::DeviceScan::InclusiveSum(nullptr, b, (const int *)nullptr, (int *)nullptr, (int)n);
-    return a > b ? a : b;
-}
-
-int scan_exclusive(void *tmp, size_t tmpb, const int *in, int *out, long long n, cudaStream_t st) {
-    return cub::DeviceScan::ExclusiveSum(tmp, tmpb, in, out, (int)n, st) == cudaSuccess ? 0 : ERR_CUDA;
+    return b;
 }
 
 int scan_inclusive(void *tmp, size_t tmpb, const int *in, int *out, long long n, cudaStream_t st) {
+    count_launch(2);   // CUB scan: init + scan kernels
     return cub::DeviceScan::InclusiveSum(tmp, tmpb, in, out, (int)n, st) == cudaSuccess ? 0 : ERR_CUDA;
 }
 
 template <typename T>
-void launch_bin_scatter(const DevGeom &g, const double *u, const double *v, const double *w,
-                        const double *foc, const int *bin_start, const int *rank, void *rec, int *perm,
-                        cudaStream_t st) {
-    k_bin_scatter<T><<<grid_for(g.nrow * g.nchan), NTHREADS, 0, st>>>(
-        g, u, v, w, foc, bin_start, rank, reinterpret_cast<R<T> *>(rec), perm);
+void launch_records(const DevGeom &g, const double *u, const double *v, const double *w, const double *foc,
+                    const int *idx, long long M, void *rec, void *ph, cudaStream_t st) {
+    count_launch();
+    k_records<T><<<grid_for(M), NTHREADS, 0, st>>>(g, u, v, w, foc, idx, M, reinterpret_cast<R<T> *>(rec),
+                                                   reinterpret_cast<C<T> *>(ph));
 }
 
 template <typename T>
-void launch_vis_prep(const DevGeom &g, const double *w, const double *foc, const void *vis,
-                     const void *wgt, const int *perm, void *cs, cudaStream_t st) {
-    k_vis_prep<T><<<grid_for(g.nrow * g.nchan), NTHREADS, 0, st>>>(
-        g, w, foc, reinterpret_cast<const C<T> *>(vis), reinterpret_cast<const T *>(wgt), perm,
-        reinterpret_cast<C<T> *>(cs));
+void launch_vis_prep(long long M, const int *idx, const void *ph, const void *vis, const void *wgt, void *cs,
+                     cudaStream_t st) {
+    count_launch();
+    k_vis_prep<T><<<grid_for(M), NTHREADS, 0, st>>>(M, idx, reinterpret_cast<const C<T> *>(ph),
+                                                    reinterpret_cast<const C<T> *>(vis),
+                                                    reinterpret_cast<const T *>(wgt), reinterpret_cast<C<T> *>(cs));
 }
 
 template <typename T>
-void launch_vis_out(const DevGeom &g, const double *w, const double *foc, const void *os,
-                    const int *perm, const void *wgt, void *vis, cudaStream_t st) {
-    k_vis_out<T><<<grid_for(g.nrow * g.nchan), NTHREADS, 0, st>>>(
-        g, w, foc, reinterpret_cast<const C<T> *>(os), perm, reinterpret_cast<const T *>(wgt),
-        reinterpret_cast<C<T> *>(vis));
+void launch_vis_out(long long M, const int *idx, const void *ph, const void *os, const void *wgt, void *vis,
+                    cudaStream_t st) {
+    count_launch();
+    k_vis_out<T><<<grid_for(M), NTHREADS, 0, st>>>(M, idx, reinterpret_cast<const C<T> *>(ph),
+                                                   reinterpret_cast<const C<T> *>(os),
+                                                   reinterpret_cast<const T *>(wgt), reinterpret_cast<C<T> *>(vis));
 }
 
 size_t tile_smem_bytes(const TileGeom &tg, int esize, int kw, int wdeg) {
-    size_t s = (size_t)tg.tx * tg.ty * tg.tz * 2 * esize;
+    size_t s = (size_t)tg.tx * tg.ty * tg.tz * 2 * (tg.fix ? 8 : esize);   // fixed point: 4 int32 per cell
     s += (size_t)NWARPS * 3 * KSTR * esize;
     s += (size_t)kw * (wdeg + 1) * esize;
     return (s + 15) & ~(size_t)15;
 }
 
-template <typename T, int KW>
-static int launch_spread_kw(const DevGeom &g, size_t smem, const int *bs, const int *bc, const int *se,
-                            const void *rec, const void *cs, void *grid, const double *wc, int nsm,
-                            cudaStream_t st) {
-    auto kern = k_spread<T, KW>;
+template <typename K>
+static int launch_persistent(K kern, size_t smem, int nsm, int &blocks) {
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return ERR_CUDA;
     int occ = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, NTHREADS, smem);
     if (occ < 1) return ERR_UNSUPPORTED;
-    kern<<<nsm * occ, NTHREADS, smem, st>>>(g, bs, bc, se, reinterpret_cast<const R<T> *>(rec),
-                                            reinterpret_cast<const C<T> *>(cs),
-                                            reinterpret_cast<C<T> *>(grid), wc);
+    blocks = nsm * occ;
+    return OK;
+}
+
+template <typename T>
+static WinTab<T> make_tab(const DevGeom &g, const double *ht) {
+    WinTab<T> t{};
+    if (g.wkind == 1 && ht)                         // host copy: [kw][TAB_DEG], highest power first
+        for (int d = 0; d < g.kw && d < TAB_KW; ++d)
+            for (int i = 0; i < TAB_DEG; ++i) t.c[d][i] = (T)ht[d * TAB_DEG + i];
+    return t;
+}
+
+template <typename T, int KW>
+static int launch_spread_kw(const DevGeom &g, size_t smem, const int *bs, const int *bc, const int *se,
+                            const void *rec, const void *cs, void *grid, const double *wc, const double *ht,
+                            int nsm, cudaStream_t st) {
+    int blocks = 0, s;
+    if constexpr (KW > 0) {
+        auto kern = k_spread_t<T, KW>;
+        if ((s = launch_persistent(kern, smem, nsm, blocks))) return s;
+        count_launch();
+        kern<<<blocks, NTHREADS, smem, st>>>(g, bs, bc, se, reinterpret_cast<const R<T> *>(rec),
+                                             reinterpret_cast<const C<T> *>(cs), reinterpret_cast<C<T> *>(grid),
+                                             make_tab<T>(g, ht));
+    } else {
+        auto kern = k_spread<T, 0>;
+        if ((s = launch_persistent(kern, smem, nsm, blocks))) return s;
+        count_launch();
+        kern<<<blocks, NTHREADS, smem, st>>>(g, bs, bc, se, reinterpret_cast<const R<T> *>(rec),
+                                             reinterpret_cast<const C<T> *>(cs), reinterpret_cast<C<T> *>(grid), wc);
+    }
     return OK;
 }
 
 template <typename T, int KW>
 static int launch_interp_kw(const DevGeom &g, size_t smem, const int *bs, const int *bc, const int *se,
-                            const void *rec, const void *grid, void *os, const double *wc, int nsm,
-                            cudaStream_t st) {
-    auto kern = k_interp<T, KW>;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-        return ERR_CUDA;
-    int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, NTHREADS, smem);
-    if (occ < 1) return ERR_UNSUPPORTED;
-    kern<<<nsm * occ, NTHREADS, smem, st>>>(g, bs, bc, se, reinterpret_cast<const R<T> *>(rec),
-                                            reinterpret_cast<const C<T> *>(grid),
-                                            reinterpret_cast<C<T> *>(os), wc);
+                            const void *rec, const void *grid, void *os, const double *wc, const double *ht,
+                            int nsm, cudaStream_t st) {
+    int blocks = 0, s;
+    if constexpr (KW > 0) {
+        auto kern = k_interp_t<T, KW>;
+        if ((s = launch_persistent(kern, smem, nsm, blocks))) return s;
+        count_launch();
+        kern<<<blocks, NTHREADS, smem, st>>>(g, bs, bc, se, reinterpret_cast<const R<T> *>(rec),
+                                             reinterpret_cast<const C<T> *>(grid), reinterpret_cast<C<T> *>(os),
+                                             make_tab<T>(g, ht));
+    } else {
+        auto kern = k_interp<T, 0>;
+        if ((s = launch_persistent(kern, smem, nsm, blocks))) return s;
+        count_launch();
+        kern<<<blocks, NTHREADS, smem, st>>>(g, bs, bc, se, reinterpret_cast<const R<T> *>(rec),
+                                             reinterpret_cast<const C<T> *>(grid), reinterpret_cast<C<T> *>(os), wc);
+    }
     return OK;
 }
 
@@ -689,24 +1015,31 @@ static int launch_interp_kw(const DevGeom &g, size_t smem, const int *bs, const 
     case 6: return F<T, 6>(__VA_ARGS__);                         \
     case 7: return F<T, 7>(__VA_ARGS__);                         \
     case 8: return F<T, 8>(__VA_ARGS__);                         \
+    case 9: return F<T, 9>(__VA_ARGS__);                         \
+    case 10: return F<T, 10>(__VA_ARGS__);                       \
+    case 11: return F<T, 11>(__VA_ARGS__);                       \
+    case 12: return F<T, 12>(__VA_ARGS__);                       \
     default: return F<T, 0>(__VA_ARGS__);                        \
     }
 
 template <typename T>
 int launch_spread(const DevGeom &g, size_t smem, const int *bs, const int *bc, const int *se,
-                  const void *rec, const void *cs, void *grid, const double *wc, int nsm, cudaStream_t st) {
-    CURIG_KW_SWITCH(launch_spread_kw, g, smem, bs, bc, se, rec, cs, grid, wc, nsm, st)
+                  const void *rec, const void *cs, void *grid, const double *wc, const double *ht, int nsm,
+                  cudaStream_t st) {
+    CURIG_KW_SWITCH(launch_spread_kw, g, smem, bs, bc, se, rec, cs, grid, wc, ht, nsm, st)
 }
 
 template <typename T>
 int launch_interp(const DevGeom &g, size_t smem, const int *bs, const int *bc, const int *se,
-                  const void *rec, const void *grid, void *os, const double *wc, int nsm, cudaStream_t st) {
-    CURIG_KW_SWITCH(launch_interp_kw, g, smem, bs, bc, se, rec, grid, os, wc, nsm, st)
+                  const void *rec, const void *grid, void *os, const double *wc, const double *ht, int nsm,
+                  cudaStream_t st) {
+    CURIG_KW_SWITCH(launch_interp_kw, g, smem, bs, bc, se, rec, grid, os, wc, ht, nsm, st)
 }
 
 template <typename T>
 void launch_correct_m2d(const DevCorr &cc, const void *grid, void *dirty, cudaStream_t st) {
     long long nq = (long long)(cc.nx / 2 + 1) * (cc.ny / 2 + 1);
+    count_launch();
     k_correct_m2d<T><<<grid_for(nq, 128), 128, 0, st>>>(cc, reinterpret_cast<const C<T> *>(grid),
                                                         reinterpret_cast<C<T> *>(dirty));
 }
@@ -714,6 +1047,7 @@ void launch_correct_m2d(const DevCorr &cc, const void *grid, void *dirty, cudaSt
 template <typename T>
 void launch_correct_d2m(const DevCorr &cc, const void *dirty, void *grid, cudaStream_t st) {
     long long nq = (long long)(cc.nx / 2 + 1) * (cc.ny / 2 + 1);
+    count_launch();
     k_correct_d2m<T><<<grid_for(nq, 128), 128, 0, st>>>(cc, reinterpret_cast<const C<T> *>(dirty),
                                                         reinterpret_cast<C<T> *>(grid));
 }
@@ -722,23 +1056,24 @@ template <typename T>
 void launch_zero_pad(int nx, int ny, int nf1, int nf2, int nf3, void *grid, cudaStream_t st) {
     long long rows = (long long)nf3 * nf2;
     int blocks = rows > 148LL * 64 ? 148 * 64 : (int)rows;
+    count_launch();
     k_zero_pad<T><<<blocks, 256, 0, st>>>(nx, ny, nf1, nf2, nf3, reinterpret_cast<C<T> *>(grid));
 }
 
 #define CURIG_INSTANTIATE(T)                                                                          \
-    template void launch_bin_scatter<T>(const DevGeom &, const double *, const double *,             \
-                                        const double *, const double *, const int *, const int *,     \
-                                        void *, int *, cudaStream_t);                                  \
-    template void launch_vis_prep<T>(const DevGeom &, const double *, const double *, const void *,   \
-                                     const void *, const int *, void *, cudaStream_t);                \
-    template void launch_vis_out<T>(const DevGeom &, const double *, const double *, const void *,    \
-                                    const int *, const void *, void *, cudaStream_t);                 \
+    template void launch_records<T>(const DevGeom &, const double *, const double *, const double *,  \
+                                    const double *, const int *, long long, void *, void *,           \
+                                    cudaStream_t);                                                    \
+    template void launch_vis_prep<T>(long long, const int *, const void *, const void *, const void *,\
+                                     void *, cudaStream_t);                                           \
+    template void launch_vis_out<T>(long long, const int *, const void *, const void *, const void *, \
+                                    void *, cudaStream_t);                                            \
     template int launch_spread<T>(const DevGeom &, size_t, const int *, const int *, const int *,     \
-                                  const void *, const void *, void *, const double *, int,            \
-                                  cudaStream_t);                                                      \
+                                  const void *, const void *, void *, const double *, const double *, \
+                                  int, cudaStream_t);                                                 \
     template int launch_interp<T>(const DevGeom &, size_t, const int *, const int *, const int *,     \
-                                  const void *, const void *, void *, const double *, int,            \
-                                  cudaStream_t);                                                      \
+                                  const void *, const void *, void *, const double *, const double *, \
+                                  int, cudaStream_t);                                                 \
     template void launch_correct_m2d<T>(const DevCorr &, const void *, void *, cudaStream_t);         \
     template void launch_correct_d2m<T>(const DevCorr &, const void *, void *, cudaStream_t);         \
     template void launch_zero_pad<T>(int, int, int, int, int, void *, cudaStream_t);

@@ -16,6 +16,8 @@ struct DevGeom {
     int bx, by, bz, nbx, nby, nbz;
     int tx, ty, tz, zpad;
     int sub;                       // visibilities per sub-problem
+    int cbits;                     // bits of the in-tile start cell in the sort key (0: bin only)
+    int smode;                     // FP32 tile accumulation: 0 exact int32 fixed point, 1 float atomics
     long long nbins;
     double beta, c;                // ES parameters
     int wkind, wdeg;               // window kind (0 ES, 1 polynomial), degree
@@ -38,5 +40,13 @@ struct DevCorr {
 };
 
 enum ErrFlag : int { EF_NONFINITE = 1, EF_RANGE = 2 };
+
+// Piecewise-polynomial window passed by value (kernel-parameter space, so the
+// Horner coefficients are uniform constant operands): c[d][i], interval d,
+// highest power first.  Used by the thread-per-visibility kernels (kw <= 12).
+constexpr int TAB_KW = 12, TAB_DEG = 12;   // degree 11
+template <typename T> struct WinTab {
+    T c[TAB_KW][TAB_DEG];
+};
 
 }  // namespace curig

@@ -7,6 +7,7 @@
 #include "plan.h"
 
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <cmath>
 #include <cstring>
@@ -112,6 +113,41 @@ void registry_clear() {
     g_windows.clear();
 }
 
+// ------------------------------------------------------------------ instrumentation
+namespace {
+std::atomic<long long> g_launches{0};
+std::atomic<bool> g_timing{false};
+}
+
+void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+long long launch_count() { return g_launches.load(); }
+void set_timing(bool on) { g_timing.store(on); }
+
+static void mark(Plan *p, int slot) {
+    if (!g_timing.load()) return;
+    if (!p->ev[slot]) cudaEventCreate(&p->ev[slot]);
+    cudaEventRecord(p->ev[slot], p->st);
+    p->ev_recorded[slot] = true;
+}
+
+int plan_timings(Plan *p, double *out, int n) {
+    static const int pairs[11][2] = {{EV_SET_BEGIN, EV_SET_END}, {EV_SET_WRANGE, EV_SET_END},
+                                     {EV_M2D_BEGIN, EV_M2D_PREP}, {EV_M2D_PREP, EV_M2D_ZERO},
+                                     {EV_M2D_ZERO, EV_M2D_SPREAD}, {EV_M2D_SPREAD, EV_M2D_FFT},
+                                     {EV_M2D_FFT, EV_M2D_END}, {EV_D2M_BEGIN, EV_D2M_CORRECT},
+                                     {EV_D2M_CORRECT, EV_D2M_FFT}, {EV_D2M_FFT, EV_D2M_INTERP},
+                                     {EV_D2M_INTERP, EV_D2M_END}};
+    if (cudaStreamSynchronize(p->st) != cudaSuccess) return ERR_CUDA;
+    for (int i = 0; i < n && i < 11; ++i) {
+        out[i] = -1.0;
+        int a = pairs[i][0], b = pairs[i][1];
+        float ms = 0;
+        if (p->ev_recorded[a] && p->ev_recorded[b] && cudaEventElapsedTime(&ms, p->ev[a], p->ev[b]) == cudaSuccess)
+            out[i] = ms;
+    }
+    return OK;
+}
+
 // ------------------------------------------------------------------ plan
 int plan_create(int type, int nx, int ny, double psx, double psy, double eps, double sigma, int sign,
                 const Options &opt, Plan **out) {
@@ -144,10 +180,10 @@ int plan_create(int type, int nx, int ny, double psx, double psy, double eps, do
 void plan_release_points(Plan *p) {
     cudaStream_t st = p->st;
     dfree(p->d_foc, st); dfree(p->d_quad, st); dfree(p->d_psi1, st); dfree(p->d_psi2, st);
-    dfree(p->d_wcoef, st); dfree(p->d_bin_count, st); dfree(p->d_bin_start, st); dfree(p->d_nsub, st);
-    dfree(p->d_sub_end, st); dfree(p->d_rank, st); dfree(p->d_perm, st); dfree(p->d_err, st);
-    dfree(p->d_keys, st); dfree(p->d_rec, st); dfree(p->d_cs, st); dfree(p->d_grid, st);
-    dfree(p->d_scan_tmp, st);
+    dfree(p->d_wcoef, st); dfree(p->d_bin_count, st); dfree(p->d_bin_start, st); dfree(p->d_bin_last, st);
+    dfree(p->d_nsub, st); dfree(p->d_sub_end, st); dfree(p->d_key_a, st); dfree(p->d_key_b, st);
+    dfree(p->d_val_a, st); dfree(p->d_idx, st); dfree(p->d_err, st); dfree(p->d_keys, st);
+    dfree(p->d_rec, st); dfree(p->d_ph, st); dfree(p->d_cs, st); dfree(p->d_grid, st); dfree(p->d_tmp, st);
     p->ready = false;
 }
 
@@ -155,6 +191,8 @@ int plan_destroy(Plan *p) {
     if (!p) return OK;
     plan_release_points(p);
     cudaStreamSynchronize(p->st);
+    for (auto &e : p->ev)
+        if (e) cudaEventDestroy(e);
     delete p;
     return OK;
 }
@@ -162,60 +200,52 @@ int plan_destroy(Plan *p) {
 // Bin / tile geometry: the largest xy bin whose tile (bin + kw halo, all
 // w-planes when the w support never wraps, else 8-plane slabs) fits the
 // shared-memory budget.
-static int choose_tiles(Plan *p, int esize) {
+// Bin / tile geometry: among the xy bin sizes whose tile (bin + kw halo, all
+// w-planes when the w support never wraps, else 8- or 4-plane slabs) fits the
+// shared-memory budget, the one with the smallest tile/core cell ratio (the
+// halo overhead of zeroing, staging and flushing a tile).
+static int choose_tiles(Plan *p, int esize, bool force_slabs) {
     const GridParams &gp = p->gp;
     const int kw = gp.kp.kw;
     TileGeom &t = p->tg;
-    size_t budget = p->opt.smem_budget ? p->opt.smem_budget : (esize == 4 ? 72 * 1024 : 100 * 1024);
+    t.fix = p->opt.smode == 0 && esize == 4 && kw <= TAB_KW;   // FP32 spreader: int32 fixed point
+    size_t budget = p->opt.smem_budget ? p->opt.smem_budget : (t.fix ? 112 * 1024 : esize == 4 ? 72 * 1024 : 100 * 1024);
     int wdeg = p->win.kind ? p->win.degree : 0;
-    // does the w support stay inside [0, nf3)?  (z grows monotonically with w)
+    // does the w support stay inside [0, nf3)?  (z grows monotonically with w;
+    // same arithmetic as the binning kernel, which rejects any start outside)
     auto zstart = [&](double we) {
         double wp = (we - gp.i_center) / gp.gamma;
         double gz = (wp * INV_2PI + 0.5) * gp.nf3;
         return std::ceil(gz - 0.5 * kw);
     };
     double z0 = zstart(p->wmin_eff), z1 = zstart(p->wmax_eff);
-    bool nowrap = z0 >= 1.0 && z1 + kw - 1 <= gp.nf3 - 2.0 && gp.nf3 <= 4000;
-    const int cand[] = {64, 48, 32, 24, 16, 12, 8, 6, 4, 2};
-    int bxy = 0;
-    auto fits = [&](int b, int tz) {
+    bool nowrap = !force_slabs && z0 >= 0.0 && z1 <= gp.nf3 - kw && gp.nf3 <= 4000;
+    const int cand[] = {64, 48, 32, 24, 20, 16, 12, 10, 8, 6, 4, 2};
+    double best = 1e30;
+    int bb = 0, bz_best = 0;
+    auto consider = [&](int b, int bz, int tz) {
+        if ((p->opt.bin_xy && b != p->opt.bin_xy) || b > gp.nf1 || b > gp.nf2) return;
         TileGeom q;
-        q.tx = b + kw; q.ty = b + kw; q.tz = tz;
-        return q.tx <= 1024 && tile_smem_bytes(q, esize, kw, wdeg) <= budget;
+        q.tx = b + kw; q.ty = b + kw; q.tz = tz; q.fix = t.fix;
+        if (q.tx > 1024 || tz > 4096 || tile_smem_bytes(q, esize, kw, wdeg) > budget) return;
+        double ratio = (double)q.tx * q.ty * tz / ((double)b * b * bz);
+        if (ratio < best - 1e-9) { best = ratio; bb = b; bz_best = bz; }
     };
-    if (nowrap) {
-        for (int b : cand) {
-            if (p->opt.bin_xy && b != p->opt.bin_xy) continue;
-            if (b > gp.nf1 || b > gp.nf2) continue;
-            if (fits(b, gp.nf3)) { bxy = b; break; }
-        }
+    for (int b : cand) {
+        if (nowrap) consider(b, gp.nf3, gp.nf3);
+        for (int bz : {8, 4, 2}) if (bz < gp.nf3) consider(b, bz, bz + kw);
     }
-    if (bxy) {
+    if (!bb) return ERR_UNSUPPORTED;
+    if (nowrap && bz_best == gp.nf3) {
         t.zpad = 0; t.bz = gp.nf3; t.tz = gp.nf3; t.nbz = 1;
     } else {
-        t.zpad = 1;
-        int bz = std::min(8, gp.nf3);
-        for (int b : cand) {
-            if (p->opt.bin_xy && b != p->opt.bin_xy) continue;
-            if (b > gp.nf1 || b > gp.nf2) continue;
-            if (fits(b, bz + kw)) { bxy = b; break; }
-        }
-        if (!bxy) {
-            bz = 2;
-            for (int b : cand) {
-                if (b > gp.nf1 || b > gp.nf2) continue;
-                if (fits(b, bz + kw)) { bxy = b; break; }
-            }
-        }
-        if (!bxy) return ERR_UNSUPPORTED;
-        t.bz = bz; t.tz = bz + kw; t.nbz = (gp.nf3 + bz - 1) / bz;
-        if (t.tz > 4096) return ERR_UNSUPPORTED;
+        t.zpad = 1; t.bz = bz_best; t.tz = bz_best + kw; t.nbz = (gp.nf3 + bz_best - 1) / bz_best;
     }
-    t.bx = t.by = bxy;
-    t.tx = bxy + kw; t.ty = bxy + kw;
-    t.nbx = (gp.nf1 + bxy - 1) / bxy;
-    t.nby = (gp.nf2 + bxy - 1) / bxy;
-    t.sub = p->opt.sub > 0 ? p->opt.sub : 2048;
+    t.bx = t.by = bb;
+    t.tx = bb + kw; t.ty = bb + kw;
+    t.nbx = (gp.nf1 + bb - 1) / bb;
+    t.nby = (gp.nf2 + bb - 1) / bb;
+    t.sub = std::min(p->opt.sub > 0 ? p->opt.sub : 4096, 4096);   // fixed-point headroom assumes <= 4096
     t.smem_bytes = tile_smem_bytes(t, esize, kw, wdeg);
     if (t.nbins() > INT_MAX / 2) return ERR_UNSUPPORTED;
     return OK;
@@ -245,6 +275,7 @@ int plan_setpts(Plan *p, long long nrow, int nchan, const double *du, const doub
     const long long M = nrow * nchan;
 
     // 1. raw w range -> effective range over channels (precomp.cu:61-69, utils.cu:42-53)
+    mark(p, EV_SET_BEGIN);
     CU_TRY(dalloc(&p->d_keys, 2 * sizeof(unsigned long long), st));
     CU_TRY(dalloc(&p->d_err, sizeof(int), st));
     unsigned long long hk[2] = {ULLONG_MAX, 0ULL};
@@ -284,11 +315,18 @@ int plan_setpts(Plan *p, long long nrow, int nchan, const double *du, const doub
     int s = grid_params(p->nx, p->ny, p->psx, p->psy, lo, hi, p->eps, p->sigma, p->sign, p->gp, kw_override);
     if (s != OK) return s;
     p->win.kw = p->gp.kp.kw;
-    s = choose_tiles(p, esize);
+    bool force_slabs = false;
+retry_tiles:
+    s = choose_tiles(p, esize, force_slabs);
     if (s != OK) return s;
     const GridParams &gp = p->gp;
     const TileGeom &tg = p->tg;
     p->smem = tg.smem_bytes;
+    {
+        TileGeom ti = tg;
+        ti.fix = 0;
+        p->smem_interp = tile_smem_bytes(ti, esize, gp.kp.kw, p->win.kind ? p->win.degree : 0);
+    }
 
     DevGeom &g = p->dg;
     g = DevGeom{};
@@ -299,6 +337,21 @@ int plan_setpts(Plan *p, long long nrow, int nchan, const double *du, const doub
     g.nbins = tg.nbins();
     g.beta = gp.kp.beta; g.c = gp.kp.c;
     g.wkind = p->win.kind; g.wdeg = p->win.kind ? p->win.degree : 0;
+    g.smode = p->opt.smode;
+    // window table for the thread-per-visibility kernels: the learned window, or
+    // in FP32 the ES window as degree-(TAB_DEG-1) Horner polynomials
+    p->htab.clear();
+    if (g.kw <= TAB_KW && (p->win.kind == 1 || p->opt.precision == 1)) {
+        Window src = p->win;
+        if (src.kind == 0) es_horner_window(gp.kp, TAB_DEG - 1, src);
+        if (src.degree <= TAB_DEG - 1) {
+            p->htab.assign((size_t)g.kw * TAB_DEG, 0.0);
+            for (int d = 0; d < g.kw; ++d)
+                for (int i = 0; i <= src.degree; ++i)
+                    p->htab[d * TAB_DEG + (TAB_DEG - 1 - src.degree) + i] = src.coef[(size_t)d * (src.degree + 1) + i];
+            g.wkind = 1;
+        }
+    }
     g.nrow = nrow; g.nchan = nchan; g.uvw_stride = stride;
     g.psx = gp.pixsize_x; g.psy = gp.pixsize_y; g.i_center = gp.i_center; g.gamma = gp.gamma;
     g.o_center = gp.o_center; g.sign = (double)gp.sign;
@@ -329,33 +382,68 @@ int plan_setpts(Plan *p, long long nrow, int nchan, const double *du, const doub
     cc.gamma = gp.gamma; cc.h = gp.h; cc.nquad = nq;
     cc.qx = p->d_quad; cc.qg = p->d_quad + MAX_QUAD; cc.psi1 = p->d_psi1; cc.psi2 = p->d_psi2;
 
-    // 4. binning: count, scan, scatter (replaces transpose + the unsorted point order)
+    // 4. binning: key per visibility (bin, start cell), radix sort, bin bounds,
+    //    sub-problem scan, records in bin order (replaces the transpose and the
+    //    unsorted point order of the reference)
     const long long nb = g.nbins;
-    CU_TRY(dalloc(&p->d_bin_count, nb * sizeof(int), st));
+    mark(p, EV_SET_WRANGE);
+    int binbits = 1;
+    while ((1LL << binbits) < nb) ++binbits;
+    long long cells = (long long)(tg.tz - g.kw + 1) * (tg.by + 1) * (tg.bx + 1);
+    int cbits = 0;
+    while ((1LL << cbits) < cells) ++cbits;
+    if (binbits + cbits > 31) cbits = 0;                 // bin-only keys for very large grids
+    if (binbits > 31) return ERR_UNSUPPORTED;
+    g.cbits = cbits;
+    const int end_bit = binbits + cbits;
+    CU_TRY(dalloc(&p->d_key_a, M * sizeof(unsigned), st));
+    CU_TRY(dalloc(&p->d_key_b, M * sizeof(unsigned), st));
+    CU_TRY(dalloc(&p->d_val_a, M * sizeof(int), st));
+    CU_TRY(dalloc(&p->d_idx, M * sizeof(int), st));
     CU_TRY(dalloc(&p->d_bin_start, nb * sizeof(int), st));
+    CU_TRY(dalloc(&p->d_bin_last, nb * sizeof(int), st));
+    CU_TRY(dalloc(&p->d_bin_count, nb * sizeof(int), st));
     CU_TRY(dalloc(&p->d_nsub, nb * sizeof(int), st));
     CU_TRY(dalloc(&p->d_sub_end, nb * sizeof(int), st));
-    CU_TRY(dalloc(&p->d_rank, M * sizeof(int), st));
-    CU_TRY(dalloc(&p->d_perm, M * sizeof(int), st));
-    CU_TRY(dalloc(&p->d_rec, M * 4 * (size_t)esize, st));
-    CU_TRY(dalloc(&p->d_cs, M * 2 * (size_t)esize, st));
-    p->scan_bytes = scan_temp_bytes(nb);
-    CU_TRY(dalloc(&p->d_scan_tmp, p->scan_bytes, st));
-    CU_TRY(cudaMemsetAsync(p->d_bin_count, 0, nb * sizeof(int), st));
-    launch_bin_count(g, du, dv, dw, p->d_foc, p->d_bin_count, p->d_rank, p->d_err, st);
-    launch_nsub(p->d_bin_count, p->d_nsub, nb, g.sub, st);
-    if (scan_exclusive(p->d_scan_tmp, p->scan_bytes, p->d_bin_count, p->d_bin_start, nb, st)) return ERR_CUDA;
-    if (scan_inclusive(p->d_scan_tmp, p->scan_bytes, p->d_nsub, p->d_sub_end, nb, st)) return ERR_CUDA;
-    if (p->opt.precision)
-        launch_bin_scatter<float>(g, du, dv, dw, p->d_foc, p->d_bin_start, p->d_rank, p->d_rec, p->d_perm, st);
-    else
-        launch_bin_scatter<double>(g, du, dv, dw, p->d_foc, p->d_bin_start, p->d_rank, p->d_rec, p->d_perm, st);
+    p->tmp_bytes = std::max(sort_temp_bytes(M, end_bit), scan_temp_bytes(nb));
+    CU_TRY(dalloc(&p->d_tmp, p->tmp_bytes, st));
+    launch_bin_keys(g, du, dv, dw, p->d_foc, p->d_key_a, p->d_val_a, p->d_err, st);
+    if (sort_pairs(p->d_tmp, p->tmp_bytes, p->d_key_a, p->d_key_b, p->d_val_a, p->d_idx, M, end_bit, st))
+        return ERR_CUDA;
+    CU_TRY(cudaMemsetAsync(p->d_bin_start, 0, nb * sizeof(int), st));
+    CU_TRY(cudaMemsetAsync(p->d_bin_last, 0, nb * sizeof(int), st));
+    launch_bin_bounds(p->d_key_b, M, cbits, p->d_bin_start, p->d_bin_last, st);
+    launch_nsub(p->d_bin_start, p->d_bin_last, p->d_bin_count, p->d_nsub, nb, g.sub, st);
+    if (scan_inclusive(p->d_tmp, p->tmp_bytes, p->d_nsub, p->d_sub_end, nb, st)) return ERR_CUDA;
     CU_TRY(cudaMemcpyAsync(&herr, p->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     CU_TRY(cudaStreamSynchronize(st));
     CU_TRY(cudaGetLastError());
     if (herr & EF_NONFINITE) return ERR_NONFINITE;
-    if (herr & EF_RANGE) return ERR_GENERIC;
-    dfree(p->d_rank, st);
+    if (herr & EF_RANGE) {
+        if (p->tg.zpad == 0 && !force_slabs) {          // a w support reached the grid edge: use z slabs
+            force_slabs = true;
+            herr = 0;
+            CU_TRY(cudaMemsetAsync(p->d_err, 0, sizeof(int), st));
+            dfree(p->d_key_a, st); dfree(p->d_key_b, st); dfree(p->d_val_a, st); dfree(p->d_idx, st);
+            dfree(p->d_bin_start, st); dfree(p->d_bin_last, st); dfree(p->d_bin_count, st);
+            dfree(p->d_nsub, st); dfree(p->d_sub_end, st); dfree(p->d_tmp, st);
+            dfree(p->d_foc, st); dfree(p->d_quad, st); dfree(p->d_psi1, st); dfree(p->d_psi2, st);
+            dfree(p->d_wcoef, st);
+            goto retry_tiles;
+        }
+        return ERR_GENERIC;
+    }
+    CU_TRY(dalloc(&p->d_rec, M * 4 * (size_t)esize, st));
+    CU_TRY(dalloc(&p->d_ph, M * 2 * (size_t)esize, st));
+    CU_TRY(dalloc(&p->d_cs, M * 2 * (size_t)esize, st));
+    if (p->opt.precision)
+        launch_records<float>(g, du, dv, dw, p->d_foc, p->d_idx, M, p->d_rec, p->d_ph, st);
+    else
+        launch_records<double>(g, du, dv, dw, p->d_foc, p->d_idx, M, p->d_rec, p->d_ph, st);
+    dfree(p->d_key_a, st);
+    dfree(p->d_key_b, st);
+    dfree(p->d_val_a, st);
+    dfree(p->d_bin_last, st);
 
     // 5. fine grid and FFT plans
     size_t gbytes = (size_t)gp.nf1 * gp.nf2 * gp.nf3 * 2 * esize;
@@ -368,6 +456,7 @@ int plan_setpts(Plan *p, long long nrow, int nchan, const double *du, const doub
     if (p->fft_rest_batch &&
         fft_plan(p->device, gp.nf1, gp.nf2, p->fft_rest_batch, p->opt.precision, p->fft_rest))
         return ERR_CUFFT;
+    mark(p, EV_SET_END);
     p->ready = true;
     return OK;
 }
@@ -395,39 +484,53 @@ static int run_fft(Plan *p, int dir) {
 }
 
 template <typename T>
-static int execute_t(Plan *p, void *d_vis, const void *d_wgt, void *d_dirty) {
+static int execute_t(Plan *p, int type, void *d_vis, const void *d_wgt, void *d_dirty) {
     cudaStream_t st = p->st;
     const DevGeom &g = p->dg;
     const GridParams &gp = p->gp;
     size_t gbytes = (size_t)gp.nf1 * gp.nf2 * gp.nf3 * 2 * sizeof(T);
+    const long long M = p->nrow * p->nchan;
     int s;
-    if (p->type == 1) {
-        launch_vis_prep<T>(g, p->dw, p->d_foc, d_vis, d_wgt, p->d_perm, p->d_cs, st);
+    if (type == 1) {
+        mark(p, EV_M2D_BEGIN);
+        launch_vis_prep<T>(M, p->d_idx, p->d_ph, d_vis, d_wgt, p->d_cs, st);
+        mark(p, EV_M2D_PREP);
         CU_TRY(cudaMemsetAsync(p->d_grid, 0, gbytes, st));
+        mark(p, EV_M2D_ZERO);
         s = launch_spread<T>(g, p->smem, p->d_bin_start, p->d_bin_count, p->d_sub_end, p->d_rec, p->d_cs,
-                             p->d_grid, p->d_wcoef, p->nsm, st);
+                             p->d_grid, p->d_wcoef, p->htab.empty() ? nullptr : p->htab.data(), p->nsm, st);
         if (s) return s;
+        mark(p, EV_M2D_SPREAD);
         s = run_fft(p, CUFFT_INVERSE);           // +1, cuft.cu:127-143
         if (s) return s;
+        mark(p, EV_M2D_FFT);
         launch_correct_m2d<T>(p->dc, p->d_grid, d_dirty, st);
+        mark(p, EV_M2D_END);
     } else {
+        mark(p, EV_D2M_BEGIN);
         launch_zero_pad<T>(p->nx, p->ny, gp.nf1, gp.nf2, gp.nf3, p->d_grid, st);
         launch_correct_d2m<T>(p->dc, d_dirty, p->d_grid, st);
+        mark(p, EV_D2M_CORRECT);
         s = run_fft(p, CUFFT_FORWARD);           // -1
         if (s) return s;
-        s = launch_interp<T>(g, p->smem, p->d_bin_start, p->d_bin_count, p->d_sub_end, p->d_rec, p->d_grid,
-                             p->d_cs, p->d_wcoef, p->nsm, st);
+        mark(p, EV_D2M_FFT);
+        s = launch_interp<T>(g, p->smem_interp, p->d_bin_start, p->d_bin_count, p->d_sub_end, p->d_rec, p->d_grid,
+                             p->d_cs, p->d_wcoef, p->htab.empty() ? nullptr : p->htab.data(), p->nsm, st);
         if (s) return s;
-        launch_vis_out<T>(g, p->dw, p->d_foc, p->d_cs, p->d_perm, d_wgt, d_vis, st);
+        mark(p, EV_D2M_INTERP);
+        launch_vis_out<T>(M, p->d_idx, p->d_ph, p->d_cs, d_wgt, d_vis, st);
+        mark(p, EV_D2M_END);
     }
     CU_TRY(cudaGetLastError());
     return OK;
 }
 
-int plan_execute(Plan *p, void *d_vis, const void *d_wgt, void *d_dirty) {
+int plan_execute(Plan *p, void *d_vis, const void *d_wgt, void *d_dirty, int type) {
     if (!p || !p->ready || !d_vis || !d_dirty) return ERR_ARG;
-    return p->opt.precision ? execute_t<float>(p, d_vis, d_wgt, d_dirty)
-                            : execute_t<double>(p, d_vis, d_wgt, d_dirty);
+    if (type == 0) type = p->type;
+    if (type != 1 && type != 2) return ERR_ARG;
+    return p->opt.precision ? execute_t<float>(p, type, d_vis, d_wgt, d_dirty)
+                            : execute_t<double>(p, type, d_vis, d_wgt, d_dirty);
 }
 
 }  // namespace curig

@@ -13,6 +13,7 @@ struct Options {
     int window = 0;           // 0: ES kernel, 1: learned window table (see set_window)
     int bin_xy = 0;           // bin edge in cells (0: chosen from the shared-memory budget)
     int sub = 0;              // visibilities per sub-problem (0: default)
+    int smode = 0;            // FP32 tile accumulation: 0 exact int32 fixed point, 1 float atomics
     size_t smem_budget = 0;   // bytes of shared memory per CTA for tiles (0: default)
     cudaStream_t stream = nullptr;
 };
@@ -38,16 +39,20 @@ struct Plan {
     DevGeom dg{};
     DevCorr dc{};
     Window win;
-    size_t smem = 0;
+    size_t smem = 0, smem_interp = 0;
     double wmin_eff = 0, wmax_eff = 0;
+    std::vector<double> htab;   // window table [kw][TAB_DEG] for the thread-per-visibility kernels
 
     // device buffers owned by the plan
     double *d_foc = nullptr, *d_quad = nullptr, *d_psi1 = nullptr, *d_psi2 = nullptr, *d_wcoef = nullptr;
-    int *d_bin_count = nullptr, *d_bin_start = nullptr, *d_nsub = nullptr, *d_sub_end = nullptr;
-    int *d_rank = nullptr, *d_perm = nullptr, *d_err = nullptr;
+    int *d_bin_count = nullptr, *d_bin_start = nullptr, *d_bin_last = nullptr, *d_nsub = nullptr,
+        *d_sub_end = nullptr;
+    unsigned *d_key_a = nullptr, *d_key_b = nullptr;   // sort keys (unsorted / sorted)
+    int *d_val_a = nullptr, *d_idx = nullptr;           // input index (unsorted / sorted = bin order)
+    int *d_err = nullptr;
     unsigned long long *d_keys = nullptr;
-    void *d_rec = nullptr, *d_cs = nullptr, *d_grid = nullptr, *d_scan_tmp = nullptr;
-    size_t scan_bytes = 0;
+    void *d_rec = nullptr, *d_ph = nullptr, *d_cs = nullptr, *d_grid = nullptr, *d_tmp = nullptr;
+    size_t tmp_bytes = 0;
 
     cufftHandle fft_main = 0, fft_rest = 0;
     int fft_batch = 0, fft_rest_batch = 0;
@@ -55,42 +60,65 @@ struct Plan {
     // learned-window tables per width (coefficients [kw][deg+1]); empty -> ES only
     std::vector<Window> learned;
     std::string last_error;
+
+    // optional per-stage CUDA events (enabled by set_timing), see STAGE_* below
+    cudaEvent_t ev[16] = {};
+    bool ev_recorded[16] = {};
 };
+
+// event slots: setpts 0..2, ms2dirty 3..8, dirty2ms 9..13
+enum Stage : int {
+    EV_SET_BEGIN = 0, EV_SET_WRANGE = 1, EV_SET_END = 2,
+    EV_M2D_BEGIN = 3, EV_M2D_PREP = 4, EV_M2D_ZERO = 5, EV_M2D_SPREAD = 6, EV_M2D_FFT = 7, EV_M2D_END = 8,
+    EV_D2M_BEGIN = 9, EV_D2M_CORRECT = 10, EV_D2M_FFT = 11, EV_D2M_INTERP = 12, EV_D2M_END = 13,
+};
+void set_timing(bool on);
+// durations (ms) of the last setpts / executes: [0] setpts, [1] binning part of setpts,
+// [2] vis prep, [3] grid zero, [4] spread, [5] FFT (m2d), [6] correct (m2d),
+// [7] correct+zero (d2m), [8] FFT (d2m), [9] interp, [10] vis out; -1 when not recorded
+int plan_timings(Plan *p, double *out, int n);
+long long launch_count();
+void count_launch(int n = 1);
 
 int plan_create(int type, int nx, int ny, double psx, double psy, double eps, double sigma, int sign,
                 const Options &opt, Plan **out);
 int plan_setpts(Plan *p, long long nrow, int nchan, const double *du, const double *dv,
                 const double *dw, int stride, const double *h_freq);
-int plan_execute(Plan *p, void *d_vis, const void *d_wgt, void *d_dirty);
+int plan_execute(Plan *p, void *d_vis, const void *d_wgt, void *d_dirty, int type = 0);
 int plan_destroy(Plan *p);
 void plan_release_points(Plan *p);
 
 // launchers (kernels.cu)
 void launch_wrange(const double *w, int stride, long long nrow, unsigned long long *keys, int *err,
                    cudaStream_t st);
-void launch_bin_count(const DevGeom &g, const double *u, const double *v, const double *w,
-                      const double *foc, int *bin_count, int *rank, int *err, cudaStream_t st);
-void launch_nsub(const int *count, int *nsub, long long nb, int sub, cudaStream_t st);
+void launch_bin_keys(const DevGeom &g, const double *u, const double *v, const double *w, const double *foc,
+                     unsigned *keys, int *vals, int *err, cudaStream_t st);
+size_t sort_temp_bytes(long long M, int end_bit);
+int sort_pairs(void *tmp, size_t tmpb, const unsigned *kin, unsigned *kout, const int *vin, int *vout,
+               long long M, int end_bit, cudaStream_t st);
+void launch_bin_bounds(const unsigned *keys, long long M, int cbits, int *first, int *last, cudaStream_t st);
+void launch_nsub(const int *first, const int *last, int *count, int *nsub, long long nb, int sub,
+                 cudaStream_t st);
 size_t scan_temp_bytes(long long n);
-int scan_exclusive(void *tmp, size_t tmpb, const int *in, int *out, long long n, cudaStream_t st);
 int scan_inclusive(void *tmp, size_t tmpb, const int *in, int *out, long long n, cudaStream_t st);
 size_t tile_smem_bytes(const TileGeom &tg, int esize, int kw, int wdeg);
 template <typename T>
-void launch_bin_scatter(const DevGeom &g, const double *u, const double *v, const double *w,
-                        const double *foc, const int *bin_start, const int *rank, void *rec, int *perm,
-                        cudaStream_t st);
+void launch_records(const DevGeom &g, const double *u, const double *v, const double *w, const double *foc,
+                    const int *idx, long long M, void *rec, void *ph, cudaStream_t st);
 template <typename T>
-void launch_vis_prep(const DevGeom &g, const double *w, const double *foc, const void *vis,
-                     const void *wgt, const int *perm, void *cs, cudaStream_t st);
+void launch_vis_prep(long long M, const int *idx, const void *ph, const void *vis, const void *wgt, void *cs,
+                     cudaStream_t st);
 template <typename T>
-void launch_vis_out(const DevGeom &g, const double *w, const double *foc, const void *os,
-                    const int *perm, const void *wgt, void *vis, cudaStream_t st);
+void launch_vis_out(long long M, const int *idx, const void *ph, const void *os, const void *wgt, void *vis,
+                    cudaStream_t st);
 template <typename T>
 int launch_spread(const DevGeom &g, size_t smem, const int *bs, const int *bc, const int *se,
-                  const void *rec, const void *cs, void *grid, const double *wc, int nsm, cudaStream_t st);
+                  const void *rec, const void *cs, void *grid, const double *wc, const double *ht, int nsm,
+                  cudaStream_t st);
 template <typename T>
 int launch_interp(const DevGeom &g, size_t smem, const int *bs, const int *bc, const int *se,
-                  const void *rec, const void *grid, void *os, const double *wc, int nsm, cudaStream_t st);
+                  const void *rec, const void *grid, void *os, const double *wc, const double *ht, int nsm,
+                  cudaStream_t st);
 template <typename T>
 void launch_correct_m2d(const DevCorr &cc, const void *grid, void *dirty, cudaStream_t st);
 template <typename T>

@@ -31,18 +31,30 @@ def _stream_handle(stream):
     return getattr(stream, "cuda_stream", stream)
 
 
+def set_timing(on: bool) -> None:
+    """Record per-stage CUDA events in every plan (off by default)."""
+    _lib.lib.curig_set_timing(1 if on else 0)
+
+
+def launch_count() -> int:
+    """Kernels launched by libcurafft.so in this process."""
+    return int(_lib.lib.curig_launch_count())
+
+
 class GridderPlan:
     """One ms2dirty (kind=1) or dirty2ms (kind=2) transform with fixed image
     geometry; set points once, execute many times."""
 
     def __init__(self, kind, nxdirty, nydirty, pixsize_x, pixsize_y, epsilon, sigma=2.0, sign=-1,
-                 precision="fp64", window="es", stream=None, bin_xy=0, sub=0, smem_budget=0):
+                 precision="fp64", window="es", stream=None, bin_xy=0, sub=0, smem_budget=0,
+                 accumulate=0):
         self.kind = kind
         self.nxdirty, self.nydirty = int(nxdirty), int(nydirty)
         self.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
         self.window = WINDOWS[window] if isinstance(window, str) else int(window)
         self._stream = _stream_handle(stream)
-        self._opts = _lib.make_opts(self.precision, self.window, bin_xy, sub, smem_budget, self._stream)
+        self._opts = _lib.make_opts(self.precision, self.window, bin_xy, sub, smem_budget, self._stream,
+                                    accumulate)
         h = ctypes.c_void_p()
         _lib.check(_lib.lib.curig_makeplan(kind, self.nxdirty, self.nydirty, float(pixsize_x),
                                            float(pixsize_y), float(epsilon), float(sigma), int(sign),
@@ -68,6 +80,19 @@ class GridderPlan:
         dirty2ms: reads dirty, writes vis.  Device tensors or pointers."""
         _lib.check(_lib.lib.curig_execute(self._h, _lib.ptr(vis), _lib.ptr(wgt), _lib.ptr(dirty)),
                    "execute")
+
+    def execute_dir(self, kind, vis, wgt, dirty):
+        """Execute in direction ``kind`` (1 ms2dirty, 2 dirty2ms) with the same points."""
+        _lib.check(_lib.lib.curig_execute_dir(self._h, int(kind), _lib.ptr(vis), _lib.ptr(wgt),
+                                              _lib.ptr(dirty)), "execute")
+
+    def timings(self) -> dict:
+        """Stage durations (ms) of the last setpts / executes (needs set_timing(True))."""
+        out = (ctypes.c_double * 11)()
+        _lib.check(_lib.lib.curig_plan_timings(self._h, out, 11), "plan_timings")
+        keys = ["setpts", "binning", "vis_prep", "grid_zero", "spread", "fft_m2d", "correct_m2d",
+                "correct_d2m", "fft_d2m", "interp", "vis_out"]
+        return {k: out[i] for i, k in enumerate(keys)}
 
     def info(self) -> dict:
         ii = (ctypes.c_int * 8)()

@@ -64,6 +64,8 @@ typedef struct curig_opts {
     int sub;              /* visibilities per sub-problem, 0 = automatic */
     int64_t smem_budget;  /* shared-memory bytes per tile CTA, 0 = automatic */
     void *stream;         /* cudaStream_t for the device-pointer API, NULL = legacy stream */
+    int accumulate;       /* FP32 tile accumulation: 0 exact int32 fixed point (default), 1 float atomics */
+    int reserved;
 } curig_opts;
 
 void curig_default_opts(curig_opts *opts);
@@ -101,6 +103,8 @@ int curig_setpts(curig_plan plan, int64_t nrow, int nchan, const double *d_uvw,
 int curig_setpts_uvw(curig_plan plan, int64_t nrow, int nchan, const double *d_u,
                      const double *d_v, const double *d_w, int stride, const double *h_freq);
 int curig_execute(curig_plan plan, void *d_vis, const void *d_wgt, void *d_dirty);
+/* execute in either direction with the same points: type 1 ms2dirty, 2 dirty2ms */
+int curig_execute_dir(curig_plan plan, int type, void *d_vis, const void *d_wgt, void *d_dirty);
 int curig_destroy(curig_plan plan);
 /* info[0..7] = nf1, nf2, nf3, kw, bin_xy, bin_z, n_bins, window kind;
  * dinfo[0..5] = beta, gamma, h, w centre, w half width, n-1 centre */
@@ -132,6 +136,19 @@ int curig_grid_params(int nxdirty, int nydirty, double pixsize_x, double pixsize
  * including the (-1)^k half-grid factor; out has nf/2+1 entries and equals the
  * reference's fwkerhalf (src/fourier/deconv.cu:13-24, 60-102) times e^-beta. */
 int curig_psi_hat(int nf, double epsilon, double sigma, double *out);
+
+/* ---------------------------------------------------------------- instrumentation
+ * Per-stage CUDA-event timing (the reference's -DTIME stage timers,
+ * src/astro/cugridder.cu:348-450, ra_exec.cu:163-307), off by default.
+ * curig_plan_timings synchronises the plan's stream and writes up to n
+ * durations in ms: [0] setpts, [1] binning part of setpts, [2] vis prep,
+ * [3] grid zero, [4] spread, [5] FFT (ms2dirty), [6] screen+correction,
+ * [7] correction+screen (dirty2ms), [8] FFT (dirty2ms), [9] interpolation,
+ * [10] vis output; -1 where a stage did not run.  curig_launch_count returns
+ * the number of kernels this library has launched in the process. */
+void curig_set_timing(int on);
+int curig_plan_timings(curig_plan plan, double *out, int n);
+int64_t curig_launch_count(void);
 
 /* Last error text of this thread (static storage, empty if none). */
 const char *curig_last_error(void);

@@ -119,12 +119,13 @@ def test_disk2000_256_against_reference_truth(C):
 
 # ---------------------------------------------------------------- multi-channel, FP32, plan API
 def _plan_run(kind, nx, ny, psx, psy, eps, sign, uvw, freq, vis=None, wgt=None, dirty=None,
-              precision="fp64", window="es"):
+              precision="fp64", window="es", accumulate=0):
     import torch
     from curig_b200 import GridderPlan
     dt = torch.complex128 if precision == "fp64" else torch.complex64
     rt = torch.float64 if precision == "fp64" else torch.float32
-    p = GridderPlan(kind, nx, ny, psx, psy, eps, 2.0, sign, precision=precision, window=window)
+    p = GridderPlan(kind, nx, ny, psx, psy, eps, 2.0, sign, precision=precision, window=window,
+                    accumulate=accumulate)
     d_uvw = torch.from_numpy(np.ascontiguousarray(uvw)).cuda()
     p.setpts(d_uvw, freq)
     nrow, nchan = uvw.shape[0], len(freq)
@@ -146,12 +147,14 @@ def _plan_run(kind, nx, ny, psx, psy, eps, sign, uvw, freq, vis=None, wgt=None, 
     return out, info
 
 
+@pytest.mark.parametrize("accumulate", [0, 1])
 @pytest.mark.parametrize("precision,eps,tol", [("fp64", 1e-9, 1e-8), ("fp64", 1e-5, 1e-4),
                                                ("fp32", 1e-5, 2e-5), ("fp32", 1e-4, 2e-4)])
-def test_multichannel_plan_vs_dft(C, precision, eps, tol):
+def test_multichannel_plan_vs_dft(C, precision, eps, tol, accumulate):
     freq, uvw, ms, wgt = disk_inputs(3000, 4, 128, 2.0, f0=0.9e9, fmax=1.1e9, max_pix=60, wmax=300)
     psx = psy = 2.0 * np.pi / 180 / 128
-    d, info = _plan_run(1, 128, 128, psx, psy, eps, -1, uvw, freq, vis=ms, wgt=wgt, precision=precision)
+    d, info = _plan_run(1, 128, 128, psx, psy, eps, -1, uvw, freq, vis=ms, wgt=wgt, precision=precision,
+                        accumulate=accumulate)
     pix = np.random.default_rng(1).integers(0, 128 * 128, 600)
     ref = dft.ms2dirty_dft(uvw, freq, ms, wgt, 128, 128, psx, psy, -1, pix=pix)
     assert l2err(ref, d.ravel()[pix]) < tol
@@ -203,3 +206,16 @@ def test_bad_sigma_is_rejected(C):
     freq, uvw, ms, dirty, wgt = wst_inputs(20, 1, 16, 16, 2)
     out = np.zeros((16, 16), dtype=np.complex128)
     assert L.ms2dirty_1(20, 16, 16, 2.0, 1e9, uvw, ms, out, 1e-6, 1.0, 1) == 2
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_fixed_point_accumulation_matches_float(C, precision):
+    """Integer (fixed-point) tile accumulation against the floating-point one on
+    a dense case (many visibilities per cell)."""
+    freq, uvw, ms, wgt = disk_inputs(200000, 2, 64, 2.0, max_pix=24, wmax=300)
+    psx = 2.0 * np.pi / 180 / 64
+    d0, _ = _plan_run(1, 64, 64, psx, psx, 1e-6, 1, uvw, freq, vis=ms, wgt=wgt, precision=precision,
+                      accumulate=0)
+    d2, _ = _plan_run(1, 64, 64, psx, psx, 1e-6, 1, uvw, freq, vis=ms, wgt=wgt, precision=precision,
+                      accumulate=1)
+    assert l2err(d0, d2) < (2e-6 if precision == "fp32" else 1e-12)
