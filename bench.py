@@ -53,6 +53,7 @@ def args_():
     ap.add_argument("--window", default="auto", choices=["auto", "es", "learned"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-arms", action="store_true", help="skip the ES comparison arms")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--accumulate", type=int, default=0, help="FP32 tile accumulation: 0 int32 fixed point, 1 float atomics")
@@ -167,6 +168,43 @@ def cpu_baseline(uvw_h, freq, vis_h, wgt_h, npix, fov, target_s):
                       f"all pixels", "pixel_vis_per_s": rate}
 
 
+def es_width_for(eps):
+    """Smallest ES width whose measured error (shipped window study, 256^2 FP64
+    against the DFT) is <= eps, and an epsilon that makes the reference's width
+    rule pick it; falls back to the rule itself."""
+    try:
+        from curig_b200 import learned
+        data = json.load(open(learned.DEFAULT_FILE))
+        ok = sorted(e["W"] for e in data["windows"] if e["es_measured"] <= eps)
+        if ok:
+            return ok[0], 10.0 ** (1 - ok[0]), {e["W"]: e for e in data["windows"]}
+    except Exception:
+        pass
+    return None, eps, {}
+
+
+def accuracy_probe(torch, plan_kw, uvw, freq, vis, wgt, npix, fov, nrow_s=1250, npx=192):
+    """Relative l2 error of one ms2dirty on a visibility subset at the full image
+    geometry against the FP64 DFT (oracle/dft.c as the checker) on sampled pixels."""
+    from curig_b200.plan import GridderPlan
+    from oracle import dft
+    psx = fov * np.pi / 180 / npix
+    u = uvw[:nrow_s].contiguous()
+    v = vis[:nrow_s].contiguous()
+    w = wgt[:nrow_s].contiguous()
+    p = GridderPlan(1, npix, npix, psx, psx, **plan_kw)
+    p.setpts(u, freq)
+    d = torch.empty((npix, npix), dtype=v.dtype, device=v.device)
+    p.execute(v, w, d)
+    torch.cuda.synchronize()
+    p.close()
+    pix = np.random.default_rng(5).integers(0, npix * npix, npx)
+    got = d.reshape(-1)[torch.from_numpy(pix).to(d.device)].cpu().numpy()
+    ref = dft.ms2dirty_dft(u.cpu().numpy(), freq, v.cpu().numpy().astype(np.complex128),
+                           w.cpu().numpy().astype(np.float64), npix, npix, psx, psx, -1, pix=pix)
+    return float(np.sqrt(np.sum(np.abs(got - ref) ** 2) / np.sum(np.abs(ref) ** 2)))
+
+
 def main():
     a = args_()
     rank = int(os.environ.get("RANK", "0"))
@@ -181,7 +219,6 @@ def main():
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    import curig_b200 as CG
     from curig_b200.plan import GridderPlan, launch_count, set_timing
 
     freq, uvw, vis, wgt = workload(torch, a.nrow, a.nchan, a.npix, a.fov, a.seed + rank, dev)
@@ -191,57 +228,100 @@ def main():
     rdt = torch.float32 if a.precision == "fp32" else torch.float64
     vis = vis.to(cdt)
     wgt = wgt.to(rdt)
-    window = "es" if a.window in ("auto", "es") else "learned"
+    window = "es"
     if a.window in ("auto", "learned"):
-        try:
-            from curig_b200 import learned
-            if learned.load_default_windows() and a.window == "auto":
-                window = "learned"
-        except Exception:
-            window = "es" if a.window == "auto" else "learned"
+        from curig_b200 import learned
+        have = learned.load_default_windows()
+        if a.window == "learned" and not have:
+            raise RuntimeError("no trained windows found")
+        window = "learned" if have else "es"
     stream = torch.cuda.current_stream()
-    plan = GridderPlan(1, a.npix, a.npix, psx, psx, a.eps, 2.0, -1, precision=a.precision,
-                       window=window, stream=stream, bin_xy=a.bin, smem_budget=a.smem,
-                       accumulate=a.accumulate)
     dirty = torch.empty((a.npix, a.npix), dtype=cdt, device=dev)
     vout = torch.empty_like(vis)
-
-    def step():
-        plan.setpts(uvw, freq)
-        plan.execute_dir(1, vis, wgt, dirty)
-        if world > 1:
-            torch.distributed.all_reduce(dirty)
-        plan.execute_dir(2, vout, wgt, dirty)
-
-    for _ in range(a.warmup):
-        step()
-    torch.cuda.synchronize()
-    set_timing(True)
-    stages = []
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    if world > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
-    n0 = launch_count()
-    with Clocks(local) as clk:
+
+    def time_arm(win, eps, steps, warmup, with_clocks=False):
+        plan = GridderPlan(1, a.npix, a.npix, psx, psx, eps, 2.0, -1, precision=a.precision, window=win,
+                           stream=stream, bin_xy=a.bin, smem_budget=a.smem, accumulate=a.accumulate)
+
+        def step():
+            plan.setpts(uvw, freq)
+            plan.execute_dir(1, vis, wgt, dirty)
+            if world > 1:
+                torch.distributed.all_reduce(dirty)
+            plan.execute_dir(2, vout, wgt, dirty)
+
+        for _ in range(warmup):
+            step()
+        torch.cuda.synchronize()
+        set_timing(True)
+        stages = []
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        n0 = launch_count()
+        clk = Clocks(local) if with_clocks else None
+        if clk:
+            clk.__enter__()
         ev0.record(stream)
-        for _ in range(a.steps):
+        for _ in range(steps):
             step()
             stages.append(plan.timings())
         ev1.record(stream)
         torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
-    launches = launch_count() - n0
-    set_timing(False)
-    ms = ev0.elapsed_time(ev1) / a.steps
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-    value = M * world / (ms / 1e3)
-    info = plan.info()
-    st = {k: float(np.mean([s[k] for s in stages])) for k in stages[0]}
+        if clk:
+            clk.__exit__()
+        if world > 1:
+            torch.distributed.barrier()
+        launches = launch_count() - n0
+        set_timing(False)
+        ms = ev0.elapsed_time(ev1) / steps
+        if world > 1:
+            t = torch.tensor([ms], device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+        info = plan.info()
+        plan.close()
+        st = {k: float(np.mean([s[k] for s in stages])) for k in stages[0]}
+        return {"value": M * world / (ms / 1e3), "ms": ms, "stages": st, "info": info,
+                "launches": launches // steps, "clocks": clk.summary() if clk else None}
+
+    head = time_arm(window, a.eps, a.steps, a.warmup, with_clocks=True)
+    value, ms, st, info = head["value"], head["ms"], head["stages"], head["info"]
+
+    # ES arms beside the learned one (single process only, to keep N > 1 runs short)
+    arms = {}
+    if world == 1 and window == "learned" and not a.no_arms:
+        w_es, eps_es, table = es_width_for(a.eps)
+        ks = max(2, a.steps // 2)
+        if w_es is not None:
+            r = time_arm("es", eps_es, ks, 2)
+            arms["es_equal_error"] = {"value": r["value"], "ms_per_step": round(r["ms"], 3), "kw": r["info"]["kw"],
+                                      "measured_error_256": table[w_es]["es_measured"],
+                                      "rule": "smallest ES width whose measured error <= eps"}
+        r = time_arm("es", a.eps, ks, 2)
+        kw = r["info"]["kw"]
+        arms["es_reference_rule"] = {"value": r["value"], "ms_per_step": round(r["ms"], 3), "kw": kw,
+                                     "measured_error_256": table.get(kw, {}).get("es_measured"),
+                                     "rule": "kw = ceil(-log10(eps/10)) (conv_interp_invoker.cu:84)"}
+        if table:
+            arms["learned_measured_error_256"] = table[info["kw"]]["eps_reached"]
+
+    # accuracy at the full image geometry (visibility subset vs the FP64 DFT)
+    acc = None
+    if rank == 0 and not a.no_cpu:
+        try:
+            base = dict(sigma=2.0, sign=-1, precision=a.precision)
+            acc = {"headline": accuracy_probe(torch, dict(base, epsilon=a.eps, window=window), uvw, freq, vis,
+                                              wgt, a.npix, a.fov)}
+            if "es_equal_error" in arms:
+                acc["es_equal_error"] = accuracy_probe(torch, dict(base, epsilon=10.0 ** (1 - arms["es_equal_error"]["kw"]),
+                                                                   window="es"), uvw, freq, vis, wgt, a.npix, a.fov)
+            if "es_reference_rule" in arms:
+                acc["es_reference_rule"] = accuracy_probe(torch, dict(base, epsilon=a.eps, window="es"), uvw,
+                                                          freq, vis, wgt, a.npix, a.fov)
+        except Exception as exc:  # pragma: no cover
+            acc = {"error": str(exc)}
 
     # roofline of the dominant kernel (algorithmic bytes per launch, live event times)
     c = 8 if a.precision == "fp32" else 16
@@ -260,7 +340,7 @@ def main():
             traffic = prof[key]["bytes_per_launch"]
     except Exception:
         pass
-    roof = {"bound": "hbm", "kernel": f"k_{dom}", "achieved": round(achieved, 1), "peak": peak,
+    roof = {"bound": "hbm", "kernel": f"k_{dom}_t", "achieved": round(achieved, 1), "peak": peak,
             "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
             "traffic": traffic, "algorithmic_bytes": alg[dom], "kernel_ms": round(st[dom], 3)}
 
@@ -324,12 +404,11 @@ def main():
                        "bin_xy": info["bin_xy"], "accumulate": ["int32 fixed point" if a.precision == "fp32" else "float atomics", "float atomics"][a.accumulate],
                        "l2": "inputs (>= 1.9 GB per step) larger than L2; no flush needed",
                        "parallelism": f"dp{world} (visibility shards, all-reduce of dirty)" if world > 1 else "single GPU"},
-            "e2e": e2e, "gpu_launches": int(launches / a.steps), "clocks": clk.summary(),
-            "roofline": roof, "cpu_baseline": cpu,
+            "e2e": e2e, "gpu_launches": int(head["launches"]), "clocks": head["clocks"],
+            "roofline": roof, "cpu_baseline": cpu, "arms": arms, "accuracy_vs_dft": acc,
             "stages_ms": {k: round(v, 3) for k, v in st.items()},
         }
         print(json.dumps(out), flush=True)
-    plan.close()
     if world > 1:
         torch.distributed.destroy_process_group()
 

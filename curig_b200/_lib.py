@@ -92,6 +92,14 @@ lib.curig_grid_params.argtypes = [c_int, c_int, c_double, c_double, c_double, c_
 lib.curig_grid_params.restype = c_int
 lib.curig_psi_hat.argtypes = [c_int, c_double, c_double, ctypes.POINTER(c_double)]
 lib.curig_psi_hat.restype = c_int
+lib.curig_window_nparams.argtypes = []
+lib.curig_window_nparams.restype = c_int
+lib.curig_train_window.argtypes = [c_int, c_double, c_int, c_double, _P, _P]
+lib.curig_train_window.restype = c_int
+lib.curig_window_loss_grad.argtypes = [c_int, c_double, _P, _P, _P]
+lib.curig_window_loss_grad.restype = c_int
+lib.curig_window_table.argtypes = [c_int, c_double, _P, c_int, _P]
+lib.curig_window_table.restype = c_int
 lib.curig_default_opts.argtypes = [ctypes.POINTER(CurigOpts)]
 lib.curig_default_opts.restype = None
 

@@ -122,6 +122,22 @@ int curig_plan_info(curig_plan plan, int *info, double *dinfo);
 int curig_set_window(int kw, int degree, const double *coef, double eps_reached);
 void curig_clear_windows(void);
 
+/* Learned window: phi(t) = exp(beta (sqrt(1 - x^2) - 1) + g(x^2)), x = 2t/W, with
+ * g a 1-32-32-32-1 tanh MLP (FP32 parameters, curig_window_nparams() of them:
+ * W1[32] b1[32] W2[32][32] b2[32] W3[32][32] b3[32] Wo[32] bo).  The objective
+ * is log of the RMS error, over fractional offsets and the image band
+ * |xi| <= 1/(2 sigma), of gridding one visibility, transforming and correcting
+ * by the window's Fourier transform, against the exact DFT (per axis).
+ * curig_train_window runs `iters` Adam steps on the current GPU in place on
+ * params (loss_hist[iters] optional); curig_window_loss_grad evaluates the RMS
+ * error and the gradient of its log; curig_window_table tabulates the window
+ * (normalised to max 1) as [W][degree+1] Horner coefficients for
+ * curig_set_window.  No counterpart in the reference. */
+int curig_window_nparams(void);
+int curig_train_window(int W, double sigma, int iters, double lr, float *params, double *loss_hist);
+int curig_window_loss_grad(int W, double sigma, const float *params, double *loss, float *grad);
+int curig_window_table(int W, double sigma, const float *params, int degree, double *coef);
+
 /* ---------------------------------------------------------------- host-only helpers
  * Sizes and scalars a transform would use, computed on the host without a GPU:
  * iout[0..3] = nf1, nf2, nf3, kw; dout[0..5] = beta, gamma, h, w centre,
