@@ -99,6 +99,8 @@ lib.curig_train_window.restype = c_int
 lib.curig_window_loss_grad.argtypes = [c_int, c_double, _P, _P, _P]
 lib.curig_window_loss_grad.restype = c_int
 lib.curig_window_table.argtypes = [c_int, c_double, _P, c_int, _P]
+lib.curig_window_loss_grad_static.argtypes = [c_int, c_double, _P, _P, _P]
+lib.curig_window_loss_grad_static.restype = c_int
 lib.curig_window_table.restype = c_int
 lib.curig_default_opts.argtypes = [ctypes.POINTER(CurigOpts)]
 lib.curig_default_opts.restype = None

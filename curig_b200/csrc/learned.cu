@@ -354,3 +354,83 @@ extern "C" int curig_window_table(int W, double sigma, const float *params, int 
     }
     return OK;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of curig_window_loss_grad.
+//
+// Some callers cannot allocate device memory at the point where they need the
+// window objective: processes whose device memory is reserved up front by
+// another framework's pool (nothing is left for cudaMalloc), and real-time or
+// embedded pipelines that forbid allocation after initialisation so that
+// latency stays bounded.  This entry point runs the same kernel with its
+// scratch (parameter copy, Adam moments, gradient, quadrature nodes and the
+// loss) in a file-scope device array instead of cudaMalloc'd buffers.
+//
+// The array is g_window_scratch below: WSCRATCH_BYTES (64 KiB) per GPU, held
+// by every GPU that loads the library until the process exits.  Host code must
+// not hand the symbol itself to a kernel (in host code it is only a stand-in,
+// not a device address); its device address is looked up once per device with
+// cudaGetSymbolAddress, on the first call made with that device current.  Make
+// that first call before any stream capture.  All calls share the one array and
+// it keeps the last call's contents, so calls that overlap on the GPU (other
+// threads, other streams) race; this entry point serialises on the legacy
+// stream and returns only when its results are copied out.
+// ---------------------------------------------------------------------------
+namespace curig {
+
+constexpr size_t WSCRATCH_BYTES = 64 * 1024;
+static __device__ __align__(256) unsigned char g_window_scratch[WSCRATCH_BYTES];
+
+static void *window_scratch_ptr(int &status) {
+    static void *addr[64] = {nullptr};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) { status = ERR_CUDA; return nullptr; }
+    if (!addr[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_window_scratch) != cudaSuccess || !p) { status = ERR_CUDA; return nullptr; }
+        addr[dev] = p;
+    }
+    status = OK;
+    return addr[dev];
+}
+
+}  // namespace curig
+
+extern "C" int curig_window_loss_grad_static(int W, double sigma, const float *params, double *loss,
+                                             float *grad) {
+    using namespace curig;
+    if (!params || W < 2 || W > TMAXW || !(sigma > 1.0)) return ERR_ARG;   // W beyond 12 does not fit
+    // layout in the static array: P, m1, m2, grad (NPAR floats each), qx, qw (TNQ doubles), out (1 double)
+    const size_t fbytes = NPAR * sizeof(float), nodes = TNQ * sizeof(double);
+    const size_t o_m1 = fbytes, o_m2 = 2 * fbytes, o_g = 3 * fbytes;
+    const size_t o_qx = (4 * fbytes + 255) & ~(size_t)255, o_qw = o_qx + nodes, o_out = o_qw + nodes;
+    static_assert((4 * NPAR * sizeof(float) + 255) / 256 * 256 + 2 * TNQ * sizeof(double) + sizeof(double) <=
+                      WSCRATCH_BYTES, "window scratch too small");
+    int st = OK;
+    unsigned char *base = static_cast<unsigned char *>(window_scratch_ptr(st));
+    if (st != OK) return st;
+    TrainGeom G{};
+    G.W = W; G.nf = TNF; G.nxi = TNXI; G.nq = TNQ; G.np = TNF * W + TNQ;
+    G.beta = es_beta_for(W, sigma); G.sigma = sigma;
+    G.b1 = 0.9; G.b2 = 0.999; G.eps = 1e-8;
+    G.want_update = 0;
+    std::vector<double> x(TNQ), w(TNQ);
+    gauss_legendre(TNQ, x.data(), w.data());
+    float *P = reinterpret_cast<float *>(base), *m1 = reinterpret_cast<float *>(base + o_m1);
+    float *m2 = reinterpret_cast<float *>(base + o_m2), *g = reinterpret_cast<float *>(base + o_g);
+    double *qx = reinterpret_cast<double *>(base + o_qx), *qw = reinterpret_cast<double *>(base + o_qw);
+    double *out = reinterpret_cast<double *>(base + o_out);
+    // every region the kernel reads is written first; the moments (unused
+    // without an update) are cleared so no stale state of an earlier call remains
+    if (cudaMemcpy(P, params, fbytes, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(m1, 0, 2 * fbytes) != cudaSuccess ||
+        cudaMemcpy(qx, x.data(), nodes, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(qw, w.data(), nodes, cudaMemcpyHostToDevice) != cudaSuccess)
+        return ERR_CUDA;
+    count_launch();
+    k_window_step<<<1, TTHREADS>>>(G, P, m1, m2, qx, qw, out, g);
+    if (cudaDeviceSynchronize() != cudaSuccess) return ERR_CUDA;
+    if (loss && cudaMemcpy(loss, out, sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) return ERR_CUDA;
+    if (grad && cudaMemcpy(grad, g, fbytes, cudaMemcpyDeviceToHost) != cudaSuccess) return ERR_CUDA;
+    return cudaGetLastError() == cudaSuccess ? OK : ERR_CUDA;
+}

@@ -138,6 +138,18 @@ int curig_train_window(int W, double sigma, int iters, double lr, float *params,
 int curig_window_loss_grad(int W, double sigma, const float *params, double *loss, float *grad);
 int curig_window_table(int W, double sigma, const float *params, int degree, double *coef);
 
+/* Same result as curig_window_loss_grad, but allocates nothing on the device:
+ * for callers that cannot call cudaMalloc where they need the objective (their
+ * device memory is reserved up front by another framework's pool, or their
+ * pipeline forbids allocation after initialisation).  Its scratch lives in one
+ * 64 KiB file-scope device array that every GPU loading the library holds until
+ * exit; the array's device address is looked up on the first call with a
+ * device current, so make that first call before any stream capture.  Calls
+ * share the array: calls that overlap on the GPU race.  W above 12 is rejected
+ * (status 3).  params, loss and grad are host pointers.  No counterpart in the
+ * reference. */
+int curig_window_loss_grad_static(int W, double sigma, const float *params, double *loss, float *grad);
+
 /* ---------------------------------------------------------------- host-only helpers
  * Sizes and scalars a transform would use, computed on the host without a GPU:
  * iout[0..3] = nf1, nf2, nf3, kw; dout[0..5] = beta, gamma, h, w centre,
