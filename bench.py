@@ -56,9 +56,10 @@ def args_():
     ap.add_argument("--no-arms", action="store_true", help="skip the ES comparison arms")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--accumulate", type=int, default=0, help="FP32 tile accumulation: 0 int32 fixed point, 1 float atomics")
+    ap.add_argument("--accumulate", type=int, default=0, help="FP32 tile accumulation: 0 automatic, 1 float atomics, 2 one-word int32 fixed point, 3 two-word (exact)")
     ap.add_argument("--bin", type=int, default=0, help="bin edge in cells (0 automatic)")
     ap.add_argument("--smem", type=int, default=0, help="shared-memory budget per tile CTA (bytes)")
+    ap.add_argument("--sub", type=int, default=0, help="visibilities per tile chunk (0 automatic)")
     return ap.parse_args()
 
 
@@ -205,6 +206,23 @@ def accuracy_probe(torch, plan_kw, uvw, freq, vis, wgt, npix, fov, nrow_s=1250, 
     return float(np.sqrt(np.sum(np.abs(got - ref) ** 2) / np.sum(np.abs(ref) ** 2)))
 
 
+def accumulation_check(torch, plan_kw, accumulate, uvw, freq, vis, wgt, npix, fov):
+    """Relative l2 difference of one full-workload ms2dirty accumulated in the
+    given FP32 tile mode against the exact two-word fixed-point mode."""
+    from curig_b200.plan import GridderPlan
+    psx = fov * np.pi / 180 / npix
+    out = []
+    for acc in (accumulate, 3):
+        p = GridderPlan(1, npix, npix, psx, psx, accumulate=acc, **plan_kw)
+        p.setpts(uvw, freq)
+        d = torch.empty((npix, npix), dtype=vis.dtype, device=vis.device)
+        p.execute(vis, wgt, d)
+        torch.cuda.synchronize()
+        p.close()
+        out.append(d)
+    return float(torch.linalg.vector_norm(out[0] - out[1]) / torch.linalg.vector_norm(out[1]))
+
+
 def main():
     a = args_()
     rank = int(os.environ.get("RANK", "0"))
@@ -240,9 +258,12 @@ def main():
     vout = torch.empty_like(vis)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
+    # every arm accumulates like the headline (automatic mode resolved at its epsilon)
+    acc_mode = a.accumulate or (2 if a.eps >= 1e-5 else 3)
+
     def time_arm(win, eps, steps, warmup, with_clocks=False):
         plan = GridderPlan(1, a.npix, a.npix, psx, psx, eps, 2.0, -1, precision=a.precision, window=win,
-                           stream=stream, bin_xy=a.bin, smem_budget=a.smem, accumulate=a.accumulate)
+                           stream=stream, bin_xy=a.bin, sub=a.sub, smem_budget=a.smem, accumulate=acc_mode)
 
         def step():
             plan.setpts(uvw, freq)
@@ -311,9 +332,13 @@ def main():
     acc = None
     if rank == 0 and not a.no_cpu:
         try:
-            base = dict(sigma=2.0, sign=-1, precision=a.precision)
+            base = dict(sigma=2.0, sign=-1, precision=a.precision, accumulate=acc_mode, sub=a.sub)
             acc = {"headline": accuracy_probe(torch, dict(base, epsilon=a.eps, window=window), uvw, freq, vis,
                                               wgt, a.npix, a.fov)}
+            if a.precision == "fp32" and acc_mode != 3:
+                acc["accumulation_vs_exact"] = accumulation_check(
+                    torch, dict(sigma=2.0, sign=-1, precision=a.precision, epsilon=a.eps, window=window, sub=a.sub,
+                                bin_xy=a.bin), acc_mode, uvw, freq, vis, wgt, a.npix, a.fov)
             if "es_equal_error" in arms:
                 acc["es_equal_error"] = accuracy_probe(torch, dict(base, epsilon=10.0 ** (1 - arms["es_equal_error"]["kw"]),
                                                                    window="es"), uvw, freq, vis, wgt, a.npix, a.fov)
@@ -356,7 +381,7 @@ def main():
         h_vout = torch.empty_like(h_vis).pin_memory()
         fr = np.ascontiguousarray(freq, dtype=np.float64)
         opts = _lib.make_opts(1 if a.precision == "fp32" else 0, 1 if window == "learned" else 0,
-                              a.bin, 0, a.smem, stream.cuda_stream, a.accumulate)
+                              a.bin, a.sub, a.smem, stream.cuda_stream, a.accumulate)
 
         def e2e_step():
             s1 = _lib.lib.curig_ms2dirty(a.nrow, a.nchan, a.npix, a.npix, psx, psx, fr.ctypes.data,
@@ -401,7 +426,7 @@ def main():
                                    f"({a.nrow * a.nchan} vis), {a.npix}^2, fov {a.fov} deg, "
                                    f"eps {a.eps}, sigma 2", "window": window,
                        "precision": a.precision, "kw": info["kw"], "nf": [info["nf1"], info["nf2"], info["nf3"]],
-                       "bin_xy": info["bin_xy"], "accumulate": ["int32 fixed point" if a.precision == "fp32" else "float atomics", "float atomics"][a.accumulate],
+                       "bin_xy": info["bin_xy"], "accumulate": ({1: "float atomics", 2: "one-word int32 fixed point", 3: "two-word int32 fixed point (exact)"}[acc_mode] if a.precision == "fp32" else "float atomics"),
                        "l2": "inputs (>= 1.9 GB per step) larger than L2; no flush needed",
                        "parallelism": f"dp{world} (visibility shards, all-reduce of dirty)" if world > 1 else "single GPU"},
             "e2e": e2e, "gpu_launches": int(head["launches"]), "clocks": head["clocks"],

@@ -26,6 +26,10 @@ template <typename T> using R = typename rec_t<T>::type;
 
 constexpr int NTHREADS = 256;
 constexpr int NWARPS = NTHREADS / 32;
+// k_spread_t: 16 warps per CTA, two CTAs per SM at the shared-memory budget of
+// one fixed-point tile
+constexpr int TTHREADS = 512;
+constexpr int TWARPS = TTHREADS / 32;
 constexpr int KSTR = 32;                 // per-axis stride of the per-warp kernel-value scratch
 constexpr double TWO_PI = 2.0 * PI_D;
 
@@ -146,9 +150,10 @@ __global__ void k_wrange(const double *__restrict__ w, int stride, long long nro
 }
 
 // ------------------------------------------------------------------ binning
-// Sort key of one visibility: bin id in the high bits, its start cell inside
-// the bin's tile in the low cbits (so threads of a warp touch neighbouring
-// cells); 0xffffffff marks a visibility that could not be placed.
+// Sort key of one visibility: bin id in the high bits, then the residue mod 32
+// of its start cell's index in the tile (the shared-memory bank of its first
+// tap), then the start cell in the bin; 0xffffffff marks a visibility that
+// could not be placed.
 __global__ void k_bin_keys(DevGeom g, const double *__restrict__ uu, const double *__restrict__ vv,
                            const double *__restrict__ ww, const double *__restrict__ foc,
                            unsigned *__restrict__ keys, int *__restrict__ vals, int *err) {
@@ -165,7 +170,12 @@ __global__ void k_bin_keys(DevGeom g, const double *__restrict__ uu, const doubl
         if (e) {
             atomicOr(err, e);
         } else {
-            unsigned cell = g.cbits ? (unsigned)((L.lz * (g.by + 1) + L.ly) * (g.bx + 1) + L.lx) : 0u;
+            unsigned cell = 0u;
+            if (g.cbits) {
+                unsigned cb = (unsigned)((L.lz * (g.by + 1) + L.ly) * (g.bx + 1) + L.lx);
+                unsigned ct = (unsigned)((L.lz * g.ty + L.ly) * g.tx + L.lx);
+                cell = g.cbits >= 5 ? ((ct & 31u) << (g.cbits - 5)) | (cb >> 5) : cb;
+            }
             key = ((unsigned)L.bin << g.cbits) | cell;
         }
         keys[j] = key;
@@ -465,15 +475,19 @@ __device__ __forceinline__ T win_tap(const DevGeom &g, const WinTab<T> &tab, T u
     return v;
 }
 
-template <typename T>
+// Sub-problem s is chunk j of the nsb chunks of bin b: the bin's sorted
+// positions start + m * stride, m < n.  Chunks interleave, so each one samples
+// every start-cell residue of the bin.
 __device__ __forceinline__ void sub_range(const DevGeom &g, const int *bin_start, const int *bin_count,
-                                          const int *sub_end, int s, long long &b, int &first, int &last) {
+                                          const int *sub_end, int s, long long &b, int &start, int &stride,
+                                          int &n) {
     b = find_bin(sub_end, g.nbins, s);
     int cnt = bin_count[b];
     int nsb = (cnt + g.sub - 1) / g.sub;
-    int chunk = s - (sub_end[b] - nsb);
-    first = bin_start[b] + chunk * g.sub;
-    last = min(first + g.sub, bin_start[b] + cnt);
+    int j = s - (sub_end[b] - nsb);
+    start = bin_start[b] + j;
+    stride = nsb;
+    n = (cnt - j + nsb - 1) / nsb;
 }
 
 // Exact fixed-point accumulation of the FP32 spreader.  Shared-memory float
@@ -496,57 +510,136 @@ __device__ __forceinline__ void split_fix(float x, int &h, int &l) {
     l = __float_as_int(lf + M) - 0x4B400000;
 }
 
+// Largest component magnitude and sum of per-visibility largest component
+// magnitudes over the chunk's visibilities (block-wide; every thread gets both).
 template <typename T>
-__device__ __forceinline__ T block_absmax(const C<T> *__restrict__ cs, int first, int last, T *red) {
-    T m = 0;
-    for (int i = first + threadIdx.x; i < last; i += NTHREADS) {
-        C<T> c = cs[i];
-        m = fmax(m, fmax(fabs(c.x), fabs(c.y)));
+__device__ __forceinline__ void block_absmax_sum(const C<T> *__restrict__ cs, int start, int stride, int n,
+                                                 T *red, T &mx, T &sm) {
+    T m = 0, a = 0;
+    for (int k = threadIdx.x; k < n; k += TTHREADS) {
+        C<T> c = cs[start + k * stride];
+        T v = fmax(fabs(c.x), fabs(c.y));
+        m = fmax(m, v);
+        a += v;
     }
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    for (int o = 16; o > 0; o >>= 1) {
+        m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        red[threadIdx.x >> 5] = m;
+        red[TWARPS + (threadIdx.x >> 5)] = a;
+    }
     __syncthreads();
-    T r = 0;
+    mx = 0;
+    sm = 0;
 #pragma unroll
-    for (int w = 0; w < NWARPS; ++w) r = fmax(r, red[w]);
-    return r;
+    for (int w = 0; w < TWARPS; ++w) {
+        mx = fmax(mx, red[w]);
+        sm += red[TWARPS + w];
+    }
+}
+
+// One-word fixed point: each term x * q is rounded to an integer by one FMA
+// against 1.5 * 2^23 (valid for |x q| <= 2^22) and added with one int32 atomic
+// per component.  A cell (x, y, z) receives only from visibilities whose start
+// column lies in the kw x kw box ending at (x, y); B = max over cells of the
+// sum of max(|re c|, |im c|) over that box bounds every cell sum by B wmax3.
+// The chunk's scale q = 2^k takes the largest k with max|c| wmax3 q <= 2^22
+// and B wmax3 q <= 2^30, so no cell sum (at most B wmax3 q + n/2 < 2^31)
+// overflows; a term's rounding error is at most 2^-23 of max|c| wmax3, unless
+// the box bound binds (more than about 250 visibilities of the largest
+// magnitude in one box).
+__device__ __forceinline__ int round_fix(float a, float k) {
+    return __float_as_int(fmaf(a, k, 12582912.0f)) - 0x4B400000;
 }
 
 template <typename T, int KW>
-__global__ void __launch_bounds__(NTHREADS)
+__global__ void __launch_bounds__(TTHREADS, sizeof(T) == 4 ? 2 : 1)
 k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__ bin_count,
            const int *__restrict__ sub_end, const R<T> *__restrict__ rec, const C<T> *__restrict__ cs,
            C<T> *__restrict__ grid, const WinTab<T> tab) {
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ T redbuf[NWARPS];
+    __shared__ T redbuf[2 * TWARPS];
     const int ntile = g.tx * g.ty * g.tz;
-    const bool fix = sizeof(T) == 4 && g.smode == 0;   // FP32: exact int32 fixed point
-    const int csz = fix ? 16 : (int)sizeof(C<T>);      // bytes per complex cell
+    const bool fix = sizeof(T) == 4 && g.smode == 0;    // FP32: exact two-word int32 fixed point
+    const bool fix1 = sizeof(T) == 4 && g.smode == 2;   // FP32: one-word int32 fixed point
+    const int csz = fix ? 16 : (int)sizeof(C<T>);       // bytes per complex cell
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int total = sub_end[g.nbins - 1];
     const int tx = g.tx, txy = g.tx * g.ty;
     const int nvec = (ntile * csz) / 16;
-    int *fhr = reinterpret_cast<int *>(smem);          // SoA planes: re-high, re-low, im-high, im-low
+    int *fhr = reinterpret_cast<int *>(smem);          // two-word planes: re-high, re-low, im-high, im-low
     int *flr = fhr + ntile, *fhi = flr + ntile, *fli = fhi + ntile;
+    int *fre = fhr, *fim = flr;                        // one-word planes: re, im
+    float *colsum = reinterpret_cast<float *>(fhr + 2 * ntile);   // one-word: per start column sum|c|
     for (int s = blockIdx.x; s < total; s += gridDim.x) {
         long long b;
-        int first, last;
-        sub_range<T>(g, bin_start, bin_count, sub_end, s, b, first, last);
+        int start, stride, n;
+        sub_range(g, bin_start, bin_count, sub_end, s, b, start, stride, n);
         float4 *tv = reinterpret_cast<float4 *>(smem);
-        for (int e = threadIdx.x; e < nvec; e += NTHREADS) tv[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int e = threadIdx.x; e < nvec; e += TTHREADS) tv[e] = make_float4(0.f, 0.f, 0.f, 0.f);
         if (!fix)
-            for (int e = nvec * 16 / csz + threadIdx.x; e < ntile; e += NTHREADS)
+            for (int e = nvec * 16 / csz + threadIdx.x; e < ntile; e += TTHREADS)
                 reinterpret_cast<C<T> *>(smem)[e] = C<T>{0, 0};
+        if (fix1)
+            for (int e = threadIdx.x; e < txy; e += TTHREADS) colsum[e] = 0.f;
         T q = 1;
         double qinv = 1;
-        if (fix) {
-            T m = block_absmax<T>(cs, first, last, redbuf);
-            int e = m > (T)0 ? ilogb(m) + 1 : 0;       // 2^(e-1) <= m < 2^e
-            q = (T)ldexp(1.0, FIX_BITS - e);
-            qinv = ldexp(1.0, e - FIX_BITS);
+        if (fix || fix1) {
+            T m, sm;
+            block_absmax_sum<T>(cs, start, stride, n, redbuf, m, sm);
+            int k;
+            if (fix) {
+                int e = m > (T)0 ? ilogb(m) + 1 : 0;       // 2^(e-1) <= m < 2^e
+                k = FIX_BITS - e;
+            } else {
+                // start-column histogram of max(|re c|, |im c|), then its kw x kw box sums
+                for (int j = threadIdx.x; j < n; j += TTHREADS) {
+                    int cb = cell_bits(rec[start + j * stride].w);
+                    C<T> c = cs[start + j * stride];
+                    atomicAdd(colsum + ((cb >> 10) & 0x3ff) * tx + (cb & 0x3ff), (float)fmax(fabs(c.x), fabs(c.y)));
+                }
+                __syncthreads();
+                float bmax = 0.f;
+                for (int e = threadIdx.x; e < txy; e += TTHREADS) {
+                    const int x = e % tx, y = e / tx;
+                    float a = 0.f;
+                    for (int yy = max(0, y - KW + 1); yy <= y; ++yy)
+                        for (int xx = max(0, x - KW + 1); xx <= x; ++xx) a += colsum[yy * tx + xx];
+                    bmax = fmaxf(bmax, a);
+                }
+                for (int o = 16; o > 0; o >>= 1) bmax = fmaxf(bmax, __shfl_xor_sync(0xffffffffu, bmax, o));
+                __syncthreads();                                  // redbuf reads of block_absmax_sum done
+                if (lane == 0) redbuf[warp] = (T)bmax;
+                __syncthreads();
+                T bb = 0;
+#pragma unroll
+                for (int w = 0; w < TWARPS; ++w) bb = fmax(bb, redbuf[w]);
+                // float sums of <= 4096 terms: relative error < 2^-12, inside the bound's factor-2 margin
+                int em = m > (T)0 ? ilogb(m * g.wmax3) + 1 : 0;
+                int es = bb > (T)0 ? ilogb(bb * g.wmax3) + 1 : 0;
+                k = min(22 - em, 30 - es);
+            }
+            k = min(k, 120);                             // chunks of near-zero values
+            q = (T)ldexp(1.0, k);
+            qinv = ldexp(1.0, -k);
         }
         __syncthreads();
-        for (int i = first + threadIdx.x; i < last; i += NTHREADS) {
+        // Lane l of a warp takes row l of the 32 x L matrix of the chunk's
+        // positions (sorted by start-cell residue mod 32), warps walk its
+        // columns: the lanes' cells are distinct mod 32 wherever the residues
+        // are balanced, and every tap then hits 32 distinct banks.  A chunk of
+        // fewer than TWARPS columns splits each visibility's w-planes into S
+        // parts (one warp per column and part) so that all warps have work.
+        const int L = (n + 31) >> 5;
+        const int S = max(1, min(KW, TWARPS / max(L, 1)));
+        for (int u = warp; u < L * S; u += TWARPS) {
+            const int k = u / S, part = u - k * S;
+            const int m = lane * L + k;
+            if (m >= n) continue;
+            const int i = start + m * stride;
+            const int dz0 = part * KW / S, dz1 = (part + 1) * KW / S;
             R<T> r = rec[i];
             C<T> c = cs[i];
             T kx[KW], ky[KW];
@@ -560,7 +653,7 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
             c.x *= q;
             c.y *= q;
 #pragma unroll 1
-            for (int dz = 0; dz < KW; ++dz) {
+            for (int dz = dz0; dz < dz1; ++dz) {
                 T kz = win_tap<T>(g, tab, r.z, dz);
                 T cr = c.x * kz, ci = c.y * kz;
                 int pz = cell + dz * txy;
@@ -569,6 +662,14 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
                     T ar = cr * ky[dy], ai = ci * ky[dy];
                     int prow = pz + dy * tx;
                     if constexpr (sizeof(T) == 4) {
+                        if (fix1) {
+#pragma unroll
+                            for (int dx = 0; dx < KW; ++dx) {
+                                atomicAdd(fre + prow + dx, round_fix(ar, kx[dx]));
+                                atomicAdd(fim + prow + dx, round_fix(ai, kx[dx]));
+                            }
+                            continue;
+                        }
                         if (fix) {
 #pragma unroll
                             for (int dx = 0; dx < KW; ++dx) {
@@ -596,22 +697,36 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
         long long bxi = b % g.nbx, byi = (b / g.nbx) % g.nby, bzi = b / ((long long)g.nbx * g.nby);
         int ox = (int)bxi * g.bx - g.hkw, oy = (int)byi * g.by - g.hkw;
         int oz = g.zpad ? (int)bzi * g.bz - g.hkw : 0;
-        for (int row = warp, y = warp % g.ty, z = warp / g.ty; row < g.ty * g.tz; row += NWARPS) {
-            int gy = wrap3(oy + y, g.nf2);
-            int gz = g.zpad ? wrap3(oz + z, g.nf3) : z;
-            y += NWARPS;
-            while (y >= g.ty) { y -= g.ty; ++z; }
-            C<T> *grow = grid + ((long long)gz * g.nf2 + gy) * g.nf1;
-            for (int x = lane; x < g.tx; x += 32) {
-                int e = row * g.tx + x;
+        // Flush: thread t walks cells t, t + TTHREADS, ... of the tile in
+        // memory order with (x, y, z) advanced incrementally; fixed-point
+        // cells convert in FP32 (one rounding of each word, then one FMA).
+        {
+            const float qf = (float)qinv, qf18 = (float)(qinv * 262144.0);
+            const int ty = g.ty, q0 = TTHREADS / tx;
+            const int sx = TTHREADS - q0 * tx, sy = q0 % ty, sz = q0 / ty;
+            int x = threadIdx.x % tx, yz = threadIdx.x / tx;
+            int y = yz % ty, z = yz / ty;
+            for (int e = threadIdx.x; e < ntile; e += TTHREADS) {
                 C<T> v;
                 if (fix) {
-                    v = C<T>{(T)(((double)fhr[e] * 262144.0 + (double)flr[e]) * qinv),
-                             (T)(((double)fhi[e] * 262144.0 + (double)fli[e]) * qinv)};
+                    v.x = (T)fmaf(__int2float_rn(fhr[e]), qf18, __int2float_rn(flr[e]) * qf);
+                    v.y = (T)fmaf(__int2float_rn(fhi[e]), qf18, __int2float_rn(fli[e]) * qf);
+                } else if (fix1) {
+                    v.x = (T)(__int2float_rn(fre[e]) * qf);
+                    v.y = (T)(__int2float_rn(fim[e]) * qf);
                 } else {
                     v = reinterpret_cast<const C<T> *>(smem)[e];
                 }
-                if (v.x != (T)0 || v.y != (T)0) atomic_add_c(grow + wrap3(ox + x, g.nf1), v);
+                if (v.x != (T)0 || v.y != (T)0) {
+                    int gx = wrap3(ox + x, g.nf1), gy = wrap3(oy + y, g.nf2);
+                    int gz = g.zpad ? wrap3(oz + z, g.nf3) : z;
+                    atomic_add_c(grid + ((long long)gz * g.nf2 + gy) * g.nf1 + gx, v);
+                }
+                x += sx;
+                if (x >= tx) { x -= tx; ++y; }
+                y += sy;
+                z += sz;
+                if (y >= ty) { y -= ty; ++z; }
             }
         }
         __syncthreads();
@@ -656,22 +771,31 @@ __device__ __forceinline__ void load_tile(const DevGeom &g, const C<T> *__restri
 }
 
 template <typename T, int KW>
-__global__ void __launch_bounds__(NTHREADS)
+__global__ void __launch_bounds__(NTHREADS, sizeof(T) == 4 ? 3 : 2)
 k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__ bin_count,
            const int *__restrict__ sub_end, const R<T> *__restrict__ rec, const C<T> *__restrict__ grid,
            C<T> *__restrict__ os, const WinTab<T> tab) {
     extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ C<T> partial[NTHREADS];      // per (column, part, lane) sums of split visibilities
     C<T> *tile = reinterpret_cast<C<T> *>(smem);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int total = sub_end[g.nbins - 1];
     const int tx = g.tx, txy = g.tx * g.ty;
     for (int s = blockIdx.x; s < total; s += gridDim.x) {
         long long b;
-        int first, last;
-        sub_range<T>(g, bin_start, bin_count, sub_end, s, b, first, last);
+        int start, stride, n;
+        sub_range(g, bin_start, bin_count, sub_end, s, b, start, stride, n);
         load_tile<T>(g, grid, tile, b, warp, lane);
         __syncthreads();
-        for (int i = first + threadIdx.x; i < last; i += NTHREADS) {
+        // same lane / position map and w-plane split as k_spread_t
+        const int L = (n + 31) >> 5;
+        const int S = max(1, min(KW, NWARPS / max(L, 1)));
+        for (int u = warp; u < L * S; u += NWARPS) {
+            const int k = u / S, part = u - k * S;
+            const int m = lane * L + k;
+            if (m >= n) continue;
+            const int i = start + m * stride;
+            const int dz0 = part * KW / S, dz1 = (part + 1) * KW / S;
             R<T> r = rec[i];
             T kx[KW], ky[KW];
 #pragma unroll
@@ -683,7 +807,7 @@ k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
             const C<T> *base = tile + ((cb >> 20) & 0xfff) * txy + ((cb >> 10) & 0x3ff) * tx + (cb & 0x3ff);
             T ar = 0, ai = 0;
 #pragma unroll 1
-            for (int dz = 0; dz < KW; ++dz) {
+            for (int dz = dz0; dz < dz1; ++dz) {
                 T kz = win_tap<T>(g, tab, r.z, dz);
                 const C<T> *pz = base + dz * txy;
                 T sr = 0, si = 0;
@@ -703,7 +827,21 @@ k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
                 ar = fma(sr, kz, ar);
                 ai = fma(si, kz, ai);
             }
-            os[i] = C<T>{ar, ai};
+            if (S == 1) os[i] = C<T>{ar, ai};
+            else partial[u * 32 + lane] = C<T>{ar, ai};
+        }
+        if (S > 1) {                                   // L * S <= NWARPS: one pass
+            __syncthreads();
+            for (int m = threadIdx.x; m < n; m += NTHREADS) {
+                const int ln = m / L, k = m - ln * L;
+                C<T> v = partial[(k * S) * 32 + ln];
+                for (int p = 1; p < S; ++p) {
+                    C<T> w = partial[(k * S + p) * 32 + ln];
+                    v.x += w.x;
+                    v.y += w.y;
+                }
+                os[start + m * stride] = v;
+            }
         }
         __syncthreads();
     }
@@ -936,18 +1074,19 @@ void launch_vis_out(long long M, const int *idx, const void *ph, const void *os,
 }
 
 size_t tile_smem_bytes(const TileGeom &tg, int esize, int kw, int wdeg) {
-    size_t s = (size_t)tg.tx * tg.ty * tg.tz * 2 * (tg.fix ? 8 : esize);   // fixed point: 4 int32 per cell
+    size_t s = (size_t)tg.tx * tg.ty * tg.tz * 2 * (tg.fix == 1 ? 8 : esize);   // two-word: 4 int32 per cell
+    if (tg.fix == 2) s += (size_t)tg.tx * tg.ty * 4;                           // one-word: column load histogram
     s += (size_t)NWARPS * 3 * KSTR * esize;
     s += (size_t)kw * (wdeg + 1) * esize;
     return (s + 15) & ~(size_t)15;
 }
 
 template <typename K>
-static int launch_persistent(K kern, size_t smem, int nsm, int &blocks) {
+static int launch_persistent(K kern, size_t smem, int nsm, int &blocks, int threads = NTHREADS) {
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return ERR_CUDA;
     int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, NTHREADS, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, smem);
     if (occ < 1) return ERR_UNSUPPORTED;
     blocks = nsm * occ;
     return OK;
@@ -969,9 +1108,9 @@ static int launch_spread_kw(const DevGeom &g, size_t smem, const int *bs, const 
     int blocks = 0, s;
     if constexpr (KW > 0) {
         auto kern = k_spread_t<T, KW>;
-        if ((s = launch_persistent(kern, smem, nsm, blocks))) return s;
+        if ((s = launch_persistent(kern, smem, nsm, blocks, TTHREADS))) return s;
         count_launch();
-        kern<<<blocks, NTHREADS, smem, st>>>(g, bs, bc, se, reinterpret_cast<const R<T> *>(rec),
+        kern<<<blocks, TTHREADS, smem, st>>>(g, bs, bc, se, reinterpret_cast<const R<T> *>(rec),
                                              reinterpret_cast<const C<T> *>(cs), reinterpret_cast<C<T> *>(grid),
                                              make_tab<T>(g, ht));
     } else {

@@ -17,7 +17,8 @@ struct DevGeom {
     int tx, ty, tz, zpad;
     int sub;                       // visibilities per sub-problem
     int cbits;                     // bits of the in-tile start cell in the sort key (0: bin only)
-    int smode;                     // FP32 tile accumulation: 0 exact int32 fixed point, 1 float atomics
+    int smode;                     // FP32 tile accumulation: 0 two-word int32, 1 float atomics, 2 one-word int32
+    float wmax3;                   // bound on |kx ky kz| of the tabulated window
     long long nbins;
     double beta, c;                // ES parameters
     int wkind, wdeg;               // window kind (0 ES, 1 polynomial), degree

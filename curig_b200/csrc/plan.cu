@@ -155,6 +155,7 @@ int plan_create(int type, int nx, int ny, double psx, double psy, double eps, do
     if ((type != 1 && type != 2) || nx <= 0 || ny <= 0 || nx > (1 << 24) || ny > (1 << 24))
         return ERR_ARG;
     if (opt.precision != 0 && opt.precision != 1) return ERR_ARG;
+    if (opt.smode < 0 || opt.smode > 3) return ERR_ARG;
     if (!std::isfinite(psx) || !std::isfinite(psy) || !(psx > 0) || !(psy > 0)) return ERR_ARG;
     KernelParams kp;
     int st = setup_kernel(eps, sigma, kp);
@@ -197,18 +198,30 @@ int plan_destroy(Plan *p) {
     return OK;
 }
 
-// Bin / tile geometry: the largest xy bin whose tile (bin + kw halo, all
-// w-planes when the w support never wraps, else 8-plane slabs) fits the
-// shared-memory budget.
 // Bin / tile geometry: among the xy bin sizes whose tile (bin + kw halo, all
 // w-planes when the w support never wraps, else 8- or 4-plane slabs) fits the
 // shared-memory budget, the one with the smallest tile/core cell ratio (the
 // halo overhead of zeroing, staging and flushing a tile).
+// FP32 tile accumulation of the spreader (kernel numbering: 0 two-word int32,
+// 1 float atomics, 2 one-word int32).  Automatic: one word when the requested
+// epsilon is at least 1e-5 (its rounding, about 1.5e-6 relative, stays well
+// inside the error budget), else the exact two-word form.
+static int tile_mode(const Plan *p) {
+    switch (p->opt.smode) {
+    case 1: return 1;
+    case 2: return 2;
+    case 3: return 0;
+    default: return p->eps >= 1e-5 ? 2 : 0;
+    }
+}
+
 static int choose_tiles(Plan *p, int esize, bool force_slabs) {
     const GridParams &gp = p->gp;
     const int kw = gp.kp.kw;
     TileGeom &t = p->tg;
-    t.fix = p->opt.smode == 0 && esize == 4 && kw <= TAB_KW;   // FP32 spreader: int32 fixed point
+    // FP32 spreader: int32 fixed point, two words (exact) or one word per component
+    const int mode = tile_mode(p);
+    t.fix = (esize == 4 && kw <= TAB_KW) ? (mode == 0 ? 1 : mode == 2 ? 2 : 0) : 0;
     size_t budget = p->opt.smem_budget ? p->opt.smem_budget : (t.fix ? 112 * 1024 : esize == 4 ? 72 * 1024 : 100 * 1024);
     int wdeg = p->win.kind ? p->win.degree : 0;
     // does the w support stay inside [0, nf3)?  (z grows monotonically with w;
@@ -245,7 +258,7 @@ static int choose_tiles(Plan *p, int esize, bool force_slabs) {
     t.tx = bb + kw; t.ty = bb + kw;
     t.nbx = (gp.nf1 + bb - 1) / bb;
     t.nby = (gp.nf2 + bb - 1) / bb;
-    t.sub = std::min(p->opt.sub > 0 ? p->opt.sub : 4096, 4096);   // fixed-point headroom assumes <= 4096
+    t.sub = std::min(p->opt.sub > 0 ? p->opt.sub : 4096, 4096);   // two-word headroom assumes <= 4096
     t.smem_bytes = tile_smem_bytes(t, esize, kw, wdeg);
     if (t.nbins() > INT_MAX / 2) return ERR_UNSUPPORTED;
     return OK;
@@ -337,7 +350,7 @@ retry_tiles:
     g.nbins = tg.nbins();
     g.beta = gp.kp.beta; g.c = gp.kp.c;
     g.wkind = p->win.kind; g.wdeg = p->win.kind ? p->win.degree : 0;
-    g.smode = p->opt.smode;
+    g.smode = tile_mode(p);
     // window table for the thread-per-visibility kernels: the learned window, or
     // in FP32 the ES window as degree-(TAB_DEG-1) Horner polynomials
     p->htab.clear();
@@ -351,6 +364,19 @@ retry_tiles:
                     p->htab[d * TAB_DEG + (TAB_DEG - 1 - src.degree) + i] = src.coef[(size_t)d * (src.degree + 1) + i];
             g.wkind = 1;
         }
+    }
+    // bound on one tap's window product (sampled table maximum, 1% margin):
+    // sets the scale of the one-word fixed-point spreader
+    g.wmax3 = 8.0f;
+    if (!p->htab.empty()) {
+        double wm = 0.0;
+        for (int d = 0; d < g.kw; ++d)
+            for (int k = 0; k <= 1024; ++k) {
+                double x = 2.0 * k / 1024.0 - 1.0, v = 0.0;
+                for (int i = 0; i < TAB_DEG; ++i) v = v * x + p->htab[(size_t)d * TAB_DEG + i];
+                wm = std::max(wm, std::fabs(v));
+            }
+        g.wmax3 = (float)(wm * wm * wm * 1.01);
     }
     g.nrow = nrow; g.nchan = nchan; g.uvw_stride = stride;
     g.psx = gp.pixsize_x; g.psy = gp.pixsize_y; g.i_center = gp.i_center; g.gamma = gp.gamma;

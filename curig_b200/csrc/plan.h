@@ -13,7 +13,8 @@ struct Options {
     int window = 0;           // 0: ES kernel, 1: learned window table (see set_window)
     int bin_xy = 0;           // bin edge in cells (0: chosen from the shared-memory budget)
     int sub = 0;              // visibilities per sub-problem (0: default)
-    int smode = 0;            // FP32 tile accumulation: 0 exact int32 fixed point, 1 float atomics
+    int smode = 0;            // FP32 tile accumulation: 0 automatic, 1 float atomics,
+                              // 2 one-word int32 fixed point, 3 exact two-word int32 fixed point
     size_t smem_budget = 0;   // bytes of shared memory per CTA for tiles (0: default)
     cudaStream_t stream = nullptr;
 };

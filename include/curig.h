@@ -64,7 +64,10 @@ typedef struct curig_opts {
     int sub;              /* visibilities per sub-problem, 0 = automatic */
     int64_t smem_budget;  /* shared-memory bytes per tile CTA, 0 = automatic */
     void *stream;         /* cudaStream_t for the device-pointer API, NULL = legacy stream */
-    int accumulate;       /* FP32 tile accumulation: 0 exact int32 fixed point (default), 1 float atomics */
+    int accumulate;       /* FP32 tile accumulation: 0 automatic (default: one-word when
+                             epsilon >= 1e-5, else two-word), 1 float atomics, 2 one-word
+                             int32 fixed point (22-bit terms, deterministic), 3 two-word
+                             int32 fixed point (exact sums, deterministic) */
     int reserved;
 } curig_opts;
 

@@ -119,13 +119,13 @@ def test_disk2000_256_against_reference_truth(C):
 
 # ---------------------------------------------------------------- multi-channel, FP32, plan API
 def _plan_run(kind, nx, ny, psx, psy, eps, sign, uvw, freq, vis=None, wgt=None, dirty=None,
-              precision="fp64", window="es", accumulate=0):
+              precision="fp64", window="es", accumulate=0, sub=0):
     import torch
     from curig_b200 import GridderPlan
     dt = torch.complex128 if precision == "fp64" else torch.complex64
     rt = torch.float64 if precision == "fp64" else torch.float32
     p = GridderPlan(kind, nx, ny, psx, psy, eps, 2.0, sign, precision=precision, window=window,
-                    accumulate=accumulate)
+                    accumulate=accumulate, sub=sub)
     d_uvw = torch.from_numpy(np.ascontiguousarray(uvw)).cuda()
     p.setpts(d_uvw, freq)
     nrow, nchan = uvw.shape[0], len(freq)
@@ -147,7 +147,7 @@ def _plan_run(kind, nx, ny, psx, psy, eps, sign, uvw, freq, vis=None, wgt=None, 
     return out, info
 
 
-@pytest.mark.parametrize("accumulate", [0, 1])
+@pytest.mark.parametrize("accumulate", [0, 1, 2, 3])
 @pytest.mark.parametrize("precision,eps,tol", [("fp64", 1e-9, 1e-8), ("fp64", 1e-5, 1e-4),
                                                ("fp32", 1e-5, 2e-5), ("fp32", 1e-4, 2e-4)])
 def test_multichannel_plan_vs_dft(C, precision, eps, tol, accumulate):
@@ -215,7 +215,43 @@ def test_fixed_point_accumulation_matches_float(C, precision):
     freq, uvw, ms, wgt = disk_inputs(200000, 2, 64, 2.0, max_pix=24, wmax=300)
     psx = 2.0 * np.pi / 180 / 64
     d0, _ = _plan_run(1, 64, 64, psx, psx, 1e-6, 1, uvw, freq, vis=ms, wgt=wgt, precision=precision,
-                      accumulate=0)
+                      accumulate=3)
     d2, _ = _plan_run(1, 64, 64, psx, psx, 1e-6, 1, uvw, freq, vis=ms, wgt=wgt, precision=precision,
                       accumulate=1)
     assert l2err(d0, d2) < (2e-6 if precision == "fp32" else 1e-12)
+
+
+@pytest.mark.parametrize("sub,tol", [(0, 3e-6), (4096, 3e-6), (256, 3e-6)])
+def test_one_word_fixed_point_matches_exact(C, sub, tol):
+    """One-word int32 tile accumulation (22-bit terms) against the exact two-word
+    one on a dense case (up to 4096 visibilities per chunk in a few cells):
+    nothing may overflow and the error stays at the 22-bit rounding level."""
+    freq, uvw, ms, wgt = disk_inputs(200000, 2, 64, 2.0, max_pix=24, wmax=300)
+    psx = 2.0 * np.pi / 180 / 64
+    d0, _ = _plan_run(1, 64, 64, psx, psx, 1e-6, 1, uvw, freq, vis=ms, wgt=wgt, precision="fp32",
+                      accumulate=3)
+    d1, _ = _plan_run(1, 64, 64, psx, psx, 1e-6, 1, uvw, freq, vis=ms, wgt=wgt, precision="fp32",
+                      accumulate=2, sub=sub)
+    assert l2err(d0, d1) < tol
+
+
+def test_one_word_fixed_point_all_in_one_cell(C):
+    """Every visibility of a 4096-visibility chunk at the same uv point: the box
+    bound must scale the chunk so that no int32 cell sum overflows."""
+    rng = np.random.default_rng(7)
+    n = 4000
+    uvw = np.tile(np.array([[120.0, -80.0, 15.0]]), (n, 1))
+    freq = np.array([1.0e9])
+    ms = (rng.standard_normal((n, 1)) + 1j * rng.standard_normal((n, 1))).astype(np.complex128)
+    wgt = np.ones((n, 1))
+    psx = 1.0 * np.pi / 180 / 64
+    d3, _ = _plan_run(1, 64, 64, psx, psx, 1e-5, -1, uvw, freq, vis=ms, wgt=wgt, precision="fp32", accumulate=3)
+    d2, _ = _plan_run(1, 64, 64, psx, psx, 1e-5, -1, uvw, freq, vis=ms, wgt=wgt, precision="fp32", accumulate=2)
+    assert l2err(d3, d2) < 1e-5
+
+
+def test_bad_accumulate_option_is_rejected(C):
+    from curig_b200 import GridderPlan
+    from curig_b200._lib import CurigError
+    with pytest.raises(CurigError):
+        GridderPlan(1, 32, 32, 1e-4, 1e-4, 1e-5, precision="fp32", accumulate=4)
