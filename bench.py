@@ -223,6 +223,54 @@ def accumulation_check(torch, plan_kw, accumulate, uvw, freq, vis, wgt, npix, fo
     return float(torch.linalg.vector_norm(out[0] - out[1]) / torch.linalg.vector_norm(out[1]))
 
 
+def batch8_autograd(torch, dev, steps, warmup, seed, window):
+    """8 independent problems, 1e6 visibilities each (1 channel at 1 GHz),
+    1024^2, fov 2 deg, FP32, eps 1e-5: one step = differentiable ms2dirty of
+    all 8 + backward of ||dirty - d||^2 to the visibilities and weights.
+    Points are set once (outside the timed region); inputs on the device."""
+    from curig_b200.autograd import BatchGridder
+    B, nrow, npix, fov = 8, 1_000_000, 1024, 2.0
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed + 1000)
+    lam = C / 1.0e9
+    R = 0.47 * npix * lam / (fov * np.pi / 180)
+    uvws = []
+    for _ in range(B):
+        r = R * torch.sqrt(torch.rand(nrow, generator=g, device=dev, dtype=torch.float64))
+        th = 2 * np.pi * torch.rand(nrow, generator=g, device=dev, dtype=torch.float64)
+        w = (torch.rand(nrow, generator=g, device=dev, dtype=torch.float64) * 2 - 1) * 200.0
+        uvws.append(torch.stack([r * torch.cos(th), r * torch.sin(th), w], 1).contiguous())
+    vis = torch.complex(torch.randn((B, nrow, 1), generator=g, device=dev),
+                        torch.randn((B, nrow, 1), generator=g, device=dev))
+    wgt = 1.0 - torch.rand((B, nrow, 1), generator=g, device=dev) * 0.5
+    d = torch.complex(torch.randn((B, npix, npix), generator=g, device=dev),
+                      torch.randn((B, npix, npix), generator=g, device=dev))
+    psx = fov * np.pi / 180 / npix
+    bg = BatchGridder(uvws, np.array([1.0e9]), npix, npix, psx, psx, 1e-5, precision="fp32", window=window)
+
+    def step():
+        v = vis.detach().requires_grad_()
+        w = wgt.detach().requires_grad_()
+        loss = ((bg.ms2dirty(v, w) - d).abs() ** 2).sum()
+        loss.backward()
+        return v.grad, w.grad
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    bg.close()
+    return {"value": B * nrow / (ms / 1e3), "unit": "vis/s", "ms_per_step": round(ms, 3),
+            "workload": "8 problems x 1e6 vis (1 ch), 1024^2, fov 2 deg, eps 1e-5, FP32; "
+                        "step = ms2dirty + backward to vis and wgt (points set once)"}
+
+
 def main():
     a = args_()
     rank = int(os.environ.get("RANK", "0"))
@@ -328,6 +376,11 @@ def main():
         if table:
             arms["learned_measured_error_256"] = table[info["kw"]]["eps_reached"]
 
+    # batch of 8 independent problems through the autograd pair (single process)
+    batch8 = None
+    if world == 1 and not a.no_arms:
+        batch8 = batch8_autograd(torch, dev, max(3, a.steps), a.warmup, a.seed, window)
+
     # accuracy at the full image geometry (visibility subset vs the FP64 DFT)
     acc = None
     if rank == 0 and not a.no_cpu:
@@ -430,7 +483,8 @@ def main():
                        "l2": "inputs (>= 1.9 GB per step) larger than L2; no flush needed",
                        "parallelism": f"dp{world} (visibility shards, all-reduce of dirty)" if world > 1 else "single GPU"},
             "e2e": e2e, "gpu_launches": int(head["launches"]), "clocks": head["clocks"],
-            "roofline": roof, "cpu_baseline": cpu, "arms": arms, "accuracy_vs_dft": acc,
+            "roofline": roof, "cpu_baseline": cpu, "arms": arms, "batch8_autograd": batch8,
+            "accuracy_vs_dft": acc,
             "stages_ms": {k: round(v, 3) for k, v in st.items()},
         }
         print(json.dumps(out), flush=True)
