@@ -152,8 +152,8 @@ __global__ void k_wrange(const double *__restrict__ w, int stride, long long nro
 // ------------------------------------------------------------------ binning
 // Sort key of one visibility: bin id in the high bits, then the residue mod 32
 // of its start cell's index in the tile (the shared-memory bank of its first
-// tap), then the start cell in the bin; 0xffffffff marks a visibility that
-// could not be placed.
+// tap); the radix sort is stable, so equal keys keep input order.  0xffffffff
+// marks a visibility that could not be placed.
 __global__ void k_bin_keys(DevGeom g, const double *__restrict__ uu, const double *__restrict__ vv,
                            const double *__restrict__ ww, const double *__restrict__ foc,
                            unsigned *__restrict__ keys, int *__restrict__ vals, int *err) {
@@ -170,12 +170,7 @@ __global__ void k_bin_keys(DevGeom g, const double *__restrict__ uu, const doubl
         if (e) {
             atomicOr(err, e);
         } else {
-            unsigned cell = 0u;
-            if (g.cbits) {
-                unsigned cb = (unsigned)((L.lz * (g.by + 1) + L.ly) * (g.bx + 1) + L.lx);
-                unsigned ct = (unsigned)((L.lz * g.ty + L.ly) * g.tx + L.lx);
-                cell = g.cbits >= 5 ? ((ct & 31u) << (g.cbits - 5)) | (cb >> 5) : cb;
-            }
+            unsigned cell = g.cbits ? (unsigned)((L.lz * g.ty + L.ly) * g.tx + L.lx) & 31u : 0u;
             key = ((unsigned)L.bin << g.cbits) | cell;
         }
         keys[j] = key;
@@ -510,36 +505,6 @@ __device__ __forceinline__ void split_fix(float x, int &h, int &l) {
     l = __float_as_int(lf + M) - 0x4B400000;
 }
 
-// Largest component magnitude and sum of per-visibility largest component
-// magnitudes over the chunk's visibilities (block-wide; every thread gets both).
-template <typename T>
-__device__ __forceinline__ void block_absmax_sum(const C<T> *__restrict__ cs, int start, int stride, int n,
-                                                 T *red, T &mx, T &sm) {
-    T m = 0, a = 0;
-    for (int k = threadIdx.x; k < n; k += TTHREADS) {
-        C<T> c = cs[start + k * stride];
-        T v = fmax(fabs(c.x), fabs(c.y));
-        m = fmax(m, v);
-        a += v;
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-        m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-        a += __shfl_xor_sync(0xffffffffu, a, o);
-    }
-    if ((threadIdx.x & 31) == 0) {
-        red[threadIdx.x >> 5] = m;
-        red[TWARPS + (threadIdx.x >> 5)] = a;
-    }
-    __syncthreads();
-    mx = 0;
-    sm = 0;
-#pragma unroll
-    for (int w = 0; w < TWARPS; ++w) {
-        mx = fmax(mx, red[w]);
-        sm += red[TWARPS + w];
-    }
-}
-
 // One-word fixed point: each term x * q is rounded to an integer by one FMA
 // against 1.5 * 2^23 (valid for |x q| <= 2^22) and added with one int32 atomic
 // per component.  A cell (x, y, z) receives only from visibilities whose start
@@ -560,7 +525,7 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
            const int *__restrict__ sub_end, const R<T> *__restrict__ rec, const C<T> *__restrict__ cs,
            C<T> *__restrict__ grid, const WinTab<T> tab) {
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ T redbuf[2 * TWARPS];
+    __shared__ T redbuf[TWARPS];
     const int ntile = g.tx * g.ty * g.tz;
     const bool fix = sizeof(T) == 4 && g.smode == 0;    // FP32: exact two-word int32 fixed point
     const bool fix1 = sizeof(T) == 4 && g.smode == 2;   // FP32: one-word int32 fixed point
@@ -584,23 +549,36 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
                 reinterpret_cast<C<T> *>(smem)[e] = C<T>{0, 0};
         if (fix1)
             for (int e = threadIdx.x; e < txy; e += TTHREADS) colsum[e] = 0.f;
+        __syncthreads();
+        // Scale statistics of the chunk: largest component of c (gathered into
+        // bin order by k_vis_prep); one word: start-column histogram of it.
+        T m = 0;
+        if (fix || fix1)
+            for (int k = threadIdx.x; k < n; k += TTHREADS) {
+                const int i = start + k * stride;
+                const C<T> c = cs[i];
+                const T mc = fmax(fabs(c.x), fabs(c.y));
+                m = fmax(m, mc);
+                if (fix1) {
+                    const int cb = cell_bits(rec[i].w);
+                    atomicAdd(colsum + ((cb >> 10) & 0x3ff) * tx + (cb & 0x3ff), (float)mc);
+                }
+            }
         T q = 1;
         double qinv = 1;
         if (fix || fix1) {
-            T m, sm;
-            block_absmax_sum<T>(cs, start, stride, n, redbuf, m, sm);
+            for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+            if (lane == 0) redbuf[warp] = m;
+            __syncthreads();
+            m = 0;
+#pragma unroll
+            for (int w = 0; w < TWARPS; ++w) m = fmax(m, redbuf[w]);
             int k;
             if (fix) {
                 int e = m > (T)0 ? ilogb(m) + 1 : 0;       // 2^(e-1) <= m < 2^e
                 k = FIX_BITS - e;
             } else {
-                // start-column histogram of max(|re c|, |im c|), then its kw x kw box sums
-                for (int j = threadIdx.x; j < n; j += TTHREADS) {
-                    int cb = cell_bits(rec[start + j * stride].w);
-                    C<T> c = cs[start + j * stride];
-                    atomicAdd(colsum + ((cb >> 10) & 0x3ff) * tx + (cb & 0x3ff), (float)fmax(fabs(c.x), fabs(c.y)));
-                }
-                __syncthreads();
+                // largest kw x kw box sum of the start-column histogram
                 float bmax = 0.f;
                 for (int e = threadIdx.x; e < txy; e += TTHREADS) {
                     const int x = e % tx, y = e / tx;
@@ -610,7 +588,7 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
                     bmax = fmaxf(bmax, a);
                 }
                 for (int o = 16; o > 0; o >>= 1) bmax = fmaxf(bmax, __shfl_xor_sync(0xffffffffu, bmax, o));
-                __syncthreads();                                  // redbuf reads of block_absmax_sum done
+                __syncthreads();                                  // every thread has read redbuf
                 if (lane == 0) redbuf[warp] = (T)bmax;
                 __syncthreads();
                 T bb = 0;
@@ -733,6 +711,16 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
     }
 }
 
+// vis[idx[i]] = value * wgt * e^{-i o_c w} (ra_exec.cu:56-89; the weight
+// multiplies, utils.cu:189): the scatter of dirty2ms back to input order.
+template <typename T>
+__device__ __forceinline__ void vis_store(const VisIO &io, int i, C<T> v) {
+    const int j = io.idx[i];
+    const C<T> e = static_cast<const C<T> *>(io.ph)[i];
+    const T wt = io.wgt ? static_cast<const T *>(io.wgt)[j] : (T)1;
+    static_cast<C<T> *>(io.vis)[j] = C<T>{(v.x * e.x + v.y * e.y) * wt, (v.y * e.x - v.x * e.y) * wt};
+}
+
 // Stage the tile (wrapped rows of all its planes): rows are walked without
 // divisions and eight rows are in flight per warp before the shared stores.
 template <typename T>
@@ -774,7 +762,7 @@ template <typename T, int KW>
 __global__ void __launch_bounds__(NTHREADS, sizeof(T) == 4 ? 3 : 2)
 k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__ bin_count,
            const int *__restrict__ sub_end, const R<T> *__restrict__ rec, const C<T> *__restrict__ grid,
-           C<T> *__restrict__ os, const WinTab<T> tab) {
+           const WinTab<T> tab, const VisIO io) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ C<T> partial[NTHREADS];      // per (column, part, lane) sums of split visibilities
     C<T> *tile = reinterpret_cast<C<T> *>(smem);
@@ -827,7 +815,7 @@ k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
                 ar = fma(sr, kz, ar);
                 ai = fma(si, kz, ai);
             }
-            if (S == 1) os[i] = C<T>{ar, ai};
+            if (S == 1) vis_store<T>(io, i, C<T>{ar, ai});
             else partial[u * 32 + lane] = C<T>{ar, ai};
         }
         if (S > 1) {                                   // L * S <= NWARPS: one pass
@@ -840,7 +828,7 @@ k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
                     v.x += w.x;
                     v.y += w.y;
                 }
-                os[start + m * stride] = v;
+                vis_store<T>(io, start + m * stride, v);
             }
         }
         __syncthreads();
@@ -1103,8 +1091,8 @@ static WinTab<T> make_tab(const DevGeom &g, const double *ht) {
 
 template <typename T, int KW>
 static int launch_spread_kw(const DevGeom &g, size_t smem, const int *bs, const int *bc, const int *se,
-                            const void *rec, const void *cs, void *grid, const double *wc, const double *ht,
-                            int nsm, cudaStream_t st) {
+                            const void *rec, void *cs, void *grid, const double *wc, const double *ht,
+                            const VisIO &io, long long M, int nsm, cudaStream_t st) {
     int blocks = 0, s;
     if constexpr (KW > 0) {
         auto kern = k_spread_t<T, KW>;
@@ -1126,21 +1114,21 @@ static int launch_spread_kw(const DevGeom &g, size_t smem, const int *bs, const 
 template <typename T, int KW>
 static int launch_interp_kw(const DevGeom &g, size_t smem, const int *bs, const int *bc, const int *se,
                             const void *rec, const void *grid, void *os, const double *wc, const double *ht,
-                            int nsm, cudaStream_t st) {
+                            const VisIO &io, long long M, int nsm, cudaStream_t st) {
     int blocks = 0, s;
     if constexpr (KW > 0) {
         auto kern = k_interp_t<T, KW>;
         if ((s = launch_persistent(kern, smem, nsm, blocks))) return s;
         count_launch();
         kern<<<blocks, NTHREADS, smem, st>>>(g, bs, bc, se, reinterpret_cast<const R<T> *>(rec),
-                                             reinterpret_cast<const C<T> *>(grid), reinterpret_cast<C<T> *>(os),
-                                             make_tab<T>(g, ht));
+                                             reinterpret_cast<const C<T> *>(grid), make_tab<T>(g, ht), io);
     } else {
         auto kern = k_interp<T, 0>;
         if ((s = launch_persistent(kern, smem, nsm, blocks))) return s;
         count_launch();
         kern<<<blocks, NTHREADS, smem, st>>>(g, bs, bc, se, reinterpret_cast<const R<T> *>(rec),
                                              reinterpret_cast<const C<T> *>(grid), reinterpret_cast<C<T> *>(os), wc);
+        launch_vis_out<T>(M, io.idx, io.ph, os, io.wgt, io.vis, st);
     }
     return OK;
 }
@@ -1163,16 +1151,16 @@ static int launch_interp_kw(const DevGeom &g, size_t smem, const int *bs, const 
 
 template <typename T>
 int launch_spread(const DevGeom &g, size_t smem, const int *bs, const int *bc, const int *se,
-                  const void *rec, const void *cs, void *grid, const double *wc, const double *ht, int nsm,
-                  cudaStream_t st) {
-    CURIG_KW_SWITCH(launch_spread_kw, g, smem, bs, bc, se, rec, cs, grid, wc, ht, nsm, st)
+                  const void *rec, void *cs, void *grid, const double *wc, const double *ht, VisIO io,
+                  long long M, int nsm, cudaStream_t st) {
+    CURIG_KW_SWITCH(launch_spread_kw, g, smem, bs, bc, se, rec, cs, grid, wc, ht, io, M, nsm, st)
 }
 
 template <typename T>
 int launch_interp(const DevGeom &g, size_t smem, const int *bs, const int *bc, const int *se,
-                  const void *rec, const void *grid, void *os, const double *wc, const double *ht, int nsm,
-                  cudaStream_t st) {
-    CURIG_KW_SWITCH(launch_interp_kw, g, smem, bs, bc, se, rec, grid, os, wc, ht, nsm, st)
+                  const void *rec, const void *grid, void *os, const double *wc, const double *ht, VisIO io,
+                  long long M, int nsm, cudaStream_t st) {
+    CURIG_KW_SWITCH(launch_interp_kw, g, smem, bs, bc, se, rec, grid, os, wc, ht, io, M, nsm, st)
 }
 
 template <typename T>
@@ -1208,11 +1196,11 @@ void launch_zero_pad(int nx, int ny, int nf1, int nf2, int nf3, void *grid, cuda
     template void launch_vis_out<T>(long long, const int *, const void *, const void *, const void *, \
                                     void *, cudaStream_t);                                            \
     template int launch_spread<T>(const DevGeom &, size_t, const int *, const int *, const int *,     \
-                                  const void *, const void *, void *, const double *, const double *, \
-                                  int, cudaStream_t);                                                 \
+                                  const void *, void *, void *, const double *, const double *,       \
+                                  VisIO, long long, int, cudaStream_t);                               \
     template int launch_interp<T>(const DevGeom &, size_t, const int *, const int *, const int *,     \
                                   const void *, const void *, void *, const double *, const double *, \
-                                  int, cudaStream_t);                                                 \
+                                  VisIO, long long, int, cudaStream_t);                               \
     template void launch_correct_m2d<T>(const DevCorr &, const void *, void *, cudaStream_t);         \
     template void launch_correct_d2m<T>(const DevCorr &, const void *, void *, cudaStream_t);         \
     template void launch_zero_pad<T>(int, int, int, int, int, void *, cudaStream_t);

@@ -51,20 +51,22 @@ static void keep_pool_memory(int device) {
 }
 
 // ------------------------------------------------------------------ cuFFT plan cache
+// Rank-1 batched in-place plans keyed by (device, length, element stride,
+// batch distance, batch, precision): row transforms (stride 1) and column
+// transforms (stride nf1, adjacent columns adjacent in memory).
 namespace {
 std::mutex g_fft_mu;
-std::map<std::tuple<int, int, int, int, int>, cufftHandle> g_fft;   // (dev, nf1, nf2, batch, prec)
+std::map<std::tuple<int, int, int, int, int, int>, cufftHandle> g_fft;
 }
 
-static int fft_plan(int dev, int nf1, int nf2, int batch, int prec, cufftHandle &out) {
+static int fft_plan1(int dev, int n, int stride, int dist, int batch, int prec, cufftHandle &out) {
     std::lock_guard<std::mutex> lk(g_fft_mu);
-    auto key = std::make_tuple(dev, nf1, nf2, batch, prec);
+    auto key = std::make_tuple(dev, n, stride, dist, batch, prec);
     auto it = g_fft.find(key);
     if (it != g_fft.end()) { out = it->second; return OK; }
     cufftHandle h;
-    int n[2] = {nf2, nf1};
-    long long dist = (long long)nf1 * nf2;
-    if (cufftPlanMany(&h, 2, n, n, 1, (int)dist, n, 1, (int)dist, prec ? CUFFT_C2C : CUFFT_Z2Z, batch) !=
+    int nn[1] = {n}, emb[1] = {n};
+    if (cufftPlanMany(&h, 1, nn, emb, stride, dist, emb, stride, dist, prec ? CUFFT_C2C : CUFFT_Z2Z, batch) !=
         CUFFT_SUCCESS)
         return ERR_CUFFT;
     g_fft[key] = h;
@@ -408,17 +410,14 @@ retry_tiles:
     cc.gamma = gp.gamma; cc.h = gp.h; cc.nquad = nq;
     cc.qx = p->d_quad; cc.qg = p->d_quad + MAX_QUAD; cc.psi1 = p->d_psi1; cc.psi2 = p->d_psi2;
 
-    // 4. binning: key per visibility (bin, start cell), radix sort, bin bounds,
+    // 4. binning: key per visibility (bin, start-cell residue), radix sort, bin bounds,
     //    sub-problem scan, records in bin order (replaces the transpose and the
     //    unsorted point order of the reference)
     const long long nb = g.nbins;
     mark(p, EV_SET_WRANGE);
     int binbits = 1;
     while ((1LL << binbits) < nb) ++binbits;
-    long long cells = (long long)(tg.tz - g.kw + 1) * (tg.by + 1) * (tg.bx + 1);
-    int cbits = 0;
-    while ((1LL << cbits) < cells) ++cbits;
-    if (binbits + cbits > 31) cbits = 0;                 // bin-only keys for very large grids
+    int cbits = binbits + 5 <= 31 ? 5 : 0;               // start-cell bank residue; bin-only keys beyond
     if (binbits > 31) return ERR_UNSUPPORTED;
     g.cbits = cbits;
     const int end_bit = binbits + cbits;
@@ -474,39 +473,67 @@ retry_tiles:
     // 5. fine grid and FFT plans
     size_t gbytes = (size_t)gp.nf1 * gp.nf2 * gp.nf3 * 2 * esize;
     CU_TRY(dalloc(&p->d_grid, gbytes, st));
-    long long plane = (long long)gp.nf1 * gp.nf2;
-    int batch = (int)std::max(1LL, std::min((long long)gp.nf3, (1LL << 27) / plane));
-    p->fft_batch = batch;
-    p->fft_rest_batch = gp.nf3 % batch;
-    if (fft_plan(p->device, gp.nf1, gp.nf2, batch, p->opt.precision, p->fft_main)) return ERR_CUFFT;
-    if (p->fft_rest_batch &&
-        fft_plan(p->device, gp.nf1, gp.nf2, p->fft_rest_batch, p->opt.precision, p->fft_rest))
+    // pruned 2-D transforms: rows (x, length nf1) of every plane, columns (y,
+    // length nf2) only for the image's columns x < ny - ny/2 and x >= nf1 - ny/2
+    const long long nrows = (long long)gp.nf2 * gp.nf3;
+    p->fft_rows = (int)std::max(1LL, std::min(nrows, (1LL << 28) / gp.nf1));
+    p->fft_rows_rest = (int)(nrows % p->fft_rows);
+    p->fft_cols_a = p->ny - p->ny / 2;
+    p->fft_cols_b = p->ny / 2;
+    const int pr = p->opt.precision;
+    if (fft_plan1(p->device, gp.nf1, 1, gp.nf1, p->fft_rows, pr, p->fft_h_rows)) return ERR_CUFFT;
+    if (p->fft_rows_rest && fft_plan1(p->device, gp.nf1, 1, gp.nf1, p->fft_rows_rest, pr, p->fft_h_rows_rest))
+        return ERR_CUFFT;
+    if (fft_plan1(p->device, gp.nf2, gp.nf1, 1, p->fft_cols_a, pr, p->fft_h_cols_a)) return ERR_CUFFT;
+    if (p->fft_cols_b && fft_plan1(p->device, gp.nf2, gp.nf1, 1, p->fft_cols_b, pr, p->fft_h_cols_b))
         return ERR_CUFFT;
     mark(p, EV_SET_END);
     p->ready = true;
     return OK;
 }
 
-static int run_fft(Plan *p, int dir) {
-    const GridParams &gp = p->gp;
-    long long plane = (long long)gp.nf1 * gp.nf2;
-    int done = 0;
-    while (done < gp.nf3) {
-        int b = (gp.nf3 - done >= p->fft_batch) ? p->fft_batch : p->fft_rest_batch;
-        cufftHandle h = (b == p->fft_batch) ? p->fft_main : p->fft_rest;
-        if (cufftSetStream(h, p->st) != CUFFT_SUCCESS) return ERR_CUFFT;
-        cufftResult r;
-        if (p->opt.precision) {
-            cufftComplex *d = reinterpret_cast<cufftComplex *>(p->d_grid) + done * plane;
-            r = cufftExecC2C(h, d, d, dir);
-        } else {
-            cufftDoubleComplex *d = reinterpret_cast<cufftDoubleComplex *>(p->d_grid) + done * plane;
-            r = cufftExecZ2Z(h, d, d, dir);
-        }
-        if (r != CUFFT_SUCCESS) return ERR_CUFFT;
-        done += b;
+static int fft_exec(Plan *p, cufftHandle h, long long offset, int dir) {
+    if (cufftSetStream(h, p->st) != CUFFT_SUCCESS) return ERR_CUFFT;
+    cufftResult r;
+    if (p->opt.precision) {
+        cufftComplex *d = reinterpret_cast<cufftComplex *>(p->d_grid) + offset;
+        r = cufftExecC2C(h, d, d, dir);
+    } else {
+        cufftDoubleComplex *d = reinterpret_cast<cufftDoubleComplex *>(p->d_grid) + offset;
+        r = cufftExecZ2Z(h, d, d, dir);
     }
-    return OK;
+    return r == CUFFT_SUCCESS ? OK : ERR_CUFFT;
+}
+
+// 2-D transform of every plane (cuft.cu:127-143), pruned to the image: after
+// ms2dirty's transform only the image columns are read, and before dirty2ms's
+// transform only they are non-zero (the rest was zeroed by k_zero_pad), so the
+// column pass runs over those columns only — rows first for ms2dirty, columns
+// first for dirty2ms.
+static int run_fft(Plan *p, int dir, bool rows_first) {
+    const GridParams &gp = p->gp;
+    const long long plane = (long long)gp.nf1 * gp.nf2, nrows = (long long)gp.nf2 * gp.nf3;
+    auto rows = [&]() {
+        for (long long r = 0; r < nrows;) {
+            const bool full = nrows - r >= p->fft_rows;
+            int s = fft_exec(p, full ? p->fft_h_rows : p->fft_h_rows_rest, r * gp.nf1, dir);
+            if (s) return s;
+            r += full ? p->fft_rows : p->fft_rows_rest;
+        }
+        return (int)OK;
+    };
+    auto cols = [&]() {
+        for (int z = 0; z < gp.nf3; ++z) {
+            int s = fft_exec(p, p->fft_h_cols_a, z * plane, dir);
+            if (s) return s;
+            if (p->fft_cols_b && (s = fft_exec(p, p->fft_h_cols_b, z * plane + gp.nf1 - p->fft_cols_b, dir)))
+                return s;
+        }
+        return (int)OK;
+    };
+    int s = rows_first ? rows() : cols();
+    if (s) return s;
+    return rows_first ? cols() : rows();
 }
 
 template <typename T>
@@ -523,11 +550,13 @@ static int execute_t(Plan *p, int type, void *d_vis, const void *d_wgt, void *d_
         mark(p, EV_M2D_PREP);
         CU_TRY(cudaMemsetAsync(p->d_grid, 0, gbytes, st));
         mark(p, EV_M2D_ZERO);
+        const VisIO io{p->d_idx, p->d_ph, d_wgt, d_vis};
         s = launch_spread<T>(g, p->smem, p->d_bin_start, p->d_bin_count, p->d_sub_end, p->d_rec, p->d_cs,
-                             p->d_grid, p->d_wcoef, p->htab.empty() ? nullptr : p->htab.data(), p->nsm, st);
+                             p->d_grid, p->d_wcoef, p->htab.empty() ? nullptr : p->htab.data(), io, M, p->nsm,
+                             st);
         if (s) return s;
         mark(p, EV_M2D_SPREAD);
-        s = run_fft(p, CUFFT_INVERSE);           // +1, cuft.cu:127-143
+        s = run_fft(p, CUFFT_INVERSE, true);     // +1, cuft.cu:127-143
         if (s) return s;
         mark(p, EV_M2D_FFT);
         launch_correct_m2d<T>(p->dc, p->d_grid, d_dirty, st);
@@ -537,15 +566,15 @@ static int execute_t(Plan *p, int type, void *d_vis, const void *d_wgt, void *d_
         launch_zero_pad<T>(p->nx, p->ny, gp.nf1, gp.nf2, gp.nf3, p->d_grid, st);
         launch_correct_d2m<T>(p->dc, d_dirty, p->d_grid, st);
         mark(p, EV_D2M_CORRECT);
-        s = run_fft(p, CUFFT_FORWARD);           // -1
+        s = run_fft(p, CUFFT_FORWARD, false);    // -1
         if (s) return s;
         mark(p, EV_D2M_FFT);
+        const VisIO io{p->d_idx, p->d_ph, d_wgt, d_vis};
         s = launch_interp<T>(g, p->smem_interp, p->d_bin_start, p->d_bin_count, p->d_sub_end, p->d_rec, p->d_grid,
-                             p->d_cs, p->d_wcoef, p->htab.empty() ? nullptr : p->htab.data(), p->nsm, st);
+                             p->d_cs, p->d_wcoef, p->htab.empty() ? nullptr : p->htab.data(), io, M, p->nsm, st);
         if (s) return s;
         mark(p, EV_D2M_INTERP);
-        launch_vis_out<T>(M, p->d_idx, p->d_ph, p->d_cs, d_wgt, d_vis, st);
-        mark(p, EV_D2M_END);
+        mark(p, EV_D2M_END);                     // the scatter runs inside the interpolator
     }
     CU_TRY(cudaGetLastError());
     return OK;

@@ -55,8 +55,8 @@ struct Plan {
     void *d_rec = nullptr, *d_ph = nullptr, *d_cs = nullptr, *d_grid = nullptr, *d_tmp = nullptr;
     size_t tmp_bytes = 0;
 
-    cufftHandle fft_main = 0, fft_rest = 0;
-    int fft_batch = 0, fft_rest_batch = 0;
+    cufftHandle fft_h_rows = 0, fft_h_rows_rest = 0, fft_h_cols_a = 0, fft_h_cols_b = 0;
+    int fft_rows = 0, fft_rows_rest = 0, fft_cols_a = 0, fft_cols_b = 0;   // rows per call, image columns
 
     // learned-window tables per width (coefficients [kw][deg+1]); empty -> ES only
     std::vector<Window> learned;
@@ -112,14 +112,19 @@ void launch_vis_prep(long long M, const int *idx, const void *ph, const void *vi
 template <typename T>
 void launch_vis_out(long long M, const int *idx, const void *ph, const void *os, const void *wgt, void *vis,
                     cudaStream_t st);
+// Tile kernels.  launch_spread spreads cs (vis * wgt * phase in bin order,
+// written by k_vis_prep); launch_interp interpolates and scatters
+// wgt * conj(phase) * value to io.vis — inside the tile kernel for widths up to
+// 12 (the random writes overlap the shared-memory work), through os and
+// k_vis_out for the generic wider kernel.
 template <typename T>
 int launch_spread(const DevGeom &g, size_t smem, const int *bs, const int *bc, const int *se,
-                  const void *rec, const void *cs, void *grid, const double *wc, const double *ht, int nsm,
-                  cudaStream_t st);
+                  const void *rec, void *cs, void *grid, const double *wc, const double *ht, VisIO io,
+                  long long M, int nsm, cudaStream_t st);
 template <typename T>
 int launch_interp(const DevGeom &g, size_t smem, const int *bs, const int *bc, const int *se,
-                  const void *rec, const void *grid, void *os, const double *wc, const double *ht, int nsm,
-                  cudaStream_t st);
+                  const void *rec, const void *grid, void *os, const double *wc, const double *ht, VisIO io,
+                  long long M, int nsm, cudaStream_t st);
 template <typename T>
 void launch_correct_m2d(const DevCorr &cc, const void *grid, void *dirty, cudaStream_t st);
 template <typename T>
