@@ -60,6 +60,8 @@ def args_():
     ap.add_argument("--bin", type=int, default=0, help="bin edge in cells (0 automatic)")
     ap.add_argument("--smem", type=int, default=0, help="shared-memory budget per tile CTA (bytes)")
     ap.add_argument("--sub", type=int, default=0, help="visibilities per tile chunk (0 automatic)")
+    ap.add_argument("--error-table", action="store_true",
+                    help="print errors per epsilon and precision form (FP64 DFT, FP64 GPU) and exit")
     return ap.parse_args()
 
 
@@ -271,6 +273,63 @@ def batch8_autograd(torch, dev, steps, warmup, seed, window):
                         "step = ms2dirty + backward to vis and wgt (points set once)"}
 
 
+def error_table(a, torch, dev):
+    """Errors per epsilon and precision form on the bench workload's geometry.
+    DFT columns: one ms2dirty / dirty2ms of a visibility subset against the FP64
+    DFT (2000 pixels / 2000 visibilities); full-density columns: FP32 ms2dirty of
+    all visibilities against the FP64 one (isolates the FP32 arithmetic)."""
+    from curig_b200.plan import GridderPlan
+    from oracle import dft
+    freq, uvw, vis, wgt = workload(torch, a.nrow, a.nchan, a.npix, a.fov, a.seed, dev)
+    psx = a.fov * np.pi / 180 / a.npix
+    rng = np.random.default_rng(11)
+    pix = rng.integers(0, a.npix * a.npix, 2000)
+    ns = 2000 // a.nchan + 1
+    u_s, v_s, w_s = uvw[:ns].contiguous(), vis[:ns].contiguous(), wgt[:ns].contiguous()
+    ref = dft.ms2dirty_dft(u_s.cpu().numpy(), freq, v_s.cpu().numpy().astype(np.complex128),
+                           w_s.cpu().numpy().astype(np.float64), a.npix, a.npix, psx, psx, -1, pix=pix)
+    img = rng.standard_normal((a.npix, a.npix)) + 1j * rng.standard_normal((a.npix, a.npix))
+    vref = dft.dirty2ms_dft(u_s.cpu().numpy(), freq, img, w_s.cpu().numpy().astype(np.float64), psx, psx, -1)
+
+    def rel(x, y):
+        return float(np.linalg.norm(x - y) / np.linalg.norm(y))
+
+    def run(prec, acc, eps, u, v, w, direction, dirty_in=None):
+        cdt = torch.complex64 if prec == "fp32" else torch.complex128
+        rdt = torch.float32 if prec == "fp32" else torch.float64
+        p = GridderPlan(1, a.npix, a.npix, psx, psx, eps, 2.0, -1, precision=prec, window="es", accumulate=acc)
+        p.setpts(u, freq)
+        vv, ww = v.to(cdt), w.to(rdt)
+        if direction == 1:
+            out = torch.empty((a.npix, a.npix), dtype=cdt, device=dev)
+            p.execute_dir(1, vv, ww, out)
+        else:
+            out = torch.empty_like(vv)
+            p.execute_dir(2, out, ww, torch.from_numpy(dirty_in).to(cdt).to(dev))
+        torch.cuda.synchronize()
+        p.close()
+        return out
+
+    forms = [("fp64", 0, "FP64"), ("fp32", 3, "FP32 two-word (exact tiles)"), ("fp32", 2, "FP32 one-word"),
+             ("fp32", 1, "FP32 float atomics")]
+    table = []
+    for eps in (1e-4, 1e-5, 1e-6):
+        full64 = run("fp64", 0, eps, uvw, vis, wgt, 1)
+        for prec, acc, name in forms:
+            d = run(prec, acc, eps, u_s, v_s, w_s, 1).reshape(-1)[torch.from_numpy(pix).to(dev)].cpu().numpy()
+            vo = run(prec, acc, eps, u_s, v_s, w_s, 2, img).cpu().numpy()
+            row = {"eps": eps, "form": name, "ms2dirty_vs_dft": rel(d, ref), "dirty2ms_vs_dft": rel(vo, vref)}
+            if prec == "fp32":
+                full = run(prec, acc, eps, uvw, vis, wgt, 1)
+                row["ms2dirty_full_vs_fp64"] = float(torch.linalg.vector_norm(full.to(torch.complex128) - full64)
+                                                     / torch.linalg.vector_norm(full64))
+                del full
+            table.append(row)
+        del full64
+    return {"error_table": table, "workload": f"{a.nrow} rows x {a.nchan} ch, {a.npix}^2, fov {a.fov} deg, ES window; "
+            f"DFT columns: {ns} rows on 2000 pixels / all their visibilities"}
+
+
 def main():
     a = args_()
     rank = int(os.environ.get("RANK", "0"))
@@ -279,6 +338,10 @@ def main():
     if a.impl == "reference":
         return reference_arm(a, rank, world)
     import torch
+    if a.error_table:
+        torch.cuda.set_device(local)
+        print(json.dumps(error_table(a, torch, torch.device("cuda", local))))
+        return 0
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     if world > 1:
