@@ -68,16 +68,27 @@ static int oneshot(int type, long long nrow, int nchan, int nx, int ny, double p
         }
         return s == OK;
     };
-    if (chk(cudaMallocAsync((void **)&d_uvw, 3 * nrow * sizeof(double), st)) &&
+    // uvw goes up on the compute stream (set points needs it first); the
+    // visibilities / weights / image go up on a copy stream meanwhile (with
+    // pinned host buffers the copies overlap the binning), joined by an event
+    cudaStream_t cp = nullptr;
+    cudaEvent_t ev_alloc = nullptr, ev_up = nullptr;
+    if (chk(cudaStreamCreateWithFlags(&cp, cudaStreamNonBlocking)) &&
+        chk(cudaEventCreateWithFlags(&ev_alloc, cudaEventDisableTiming)) &&
+        chk(cudaEventCreateWithFlags(&ev_up, cudaEventDisableTiming)) &&
+        chk(cudaMallocAsync((void **)&d_uvw, 3 * nrow * sizeof(double), st)) &&
         chk(cudaMallocAsync(&d_vis, M * cs, st)) &&
         (!wgt || chk(cudaMallocAsync(&d_wgt, M * rs, st))) &&
         chk(cudaMallocAsync(&d_dirty, npix * cs, st)) &&
+        chk(cudaEventRecord(ev_alloc, st)) && chk(cudaStreamWaitEvent(cp, ev_alloc, 0)) &&
         chk(cudaMemcpyAsync(d_uvw, uvw, 3 * nrow * sizeof(double), cudaMemcpyHostToDevice, st)) &&
-        (type != 1 || chk(cudaMemcpyAsync(d_vis, vis, M * cs, cudaMemcpyHostToDevice, st))) &&
-        (!wgt || chk(cudaMemcpyAsync(d_wgt, wgt, M * rs, cudaMemcpyHostToDevice, st))) &&
-        (type != 2 || chk(cudaMemcpyAsync(d_dirty, dirty, npix * cs, cudaMemcpyHostToDevice, st)))) {
+        (type != 1 || chk(cudaMemcpyAsync(d_vis, vis, M * cs, cudaMemcpyHostToDevice, cp))) &&
+        (!wgt || chk(cudaMemcpyAsync(d_wgt, wgt, M * rs, cudaMemcpyHostToDevice, cp))) &&
+        (type != 2 || chk(cudaMemcpyAsync(d_dirty, dirty, npix * cs, cudaMemcpyHostToDevice, cp))) &&
+        chk(cudaEventRecord(ev_up, cp))) {
         s = plan_create(type, nx, ny, psx, psy, eps, sigma, sign, opt, &p);
         if (s == OK) s = plan_setpts(p, nrow, nchan, d_uvw, d_uvw + 1, d_uvw + 2, 3, freq);
+        if (s == OK && !chk(cudaStreamWaitEvent(st, ev_up, 0))) s = ERR_CUDA;
         if (s == OK) s = plan_execute(p, d_vis, d_wgt, d_dirty);
         if (s == OK) {
             if (type == 1) chk(cudaMemcpyAsync(dirty, d_dirty, npix * cs, cudaMemcpyDeviceToHost, st));
@@ -86,6 +97,12 @@ static int oneshot(int type, long long nrow, int nchan, int nx, int ny, double p
         if (p && s != OK && !p->last_error.empty()) g_last_error = p->last_error;
         if (p) plan_destroy(p);
     }
+    if (cp) {                              // nothing freed while an upload may still run
+        cudaStreamSynchronize(cp);
+        cudaStreamDestroy(cp);
+    }
+    if (ev_alloc) cudaEventDestroy(ev_alloc);
+    if (ev_up) cudaEventDestroy(ev_up);
     if (d_uvw) cudaFreeAsync(d_uvw, st);
     if (d_vis) cudaFreeAsync(d_vis, st);
     if (d_wgt) cudaFreeAsync(d_wgt, st);
