@@ -8,8 +8,9 @@
 //   w_term_dft + deconv_2d + w_term_deconv + div_n_lm
 //       (cuft.cu:520-572, deconv.cu:236-417, ra_exec.cu:22-52) -> k_correct_m2d (one pass)
 //   div_n_lm + w_term_deconv + deconv_2d + w_term_idft
-//       (ra_exec.cu:325-373, cuft.cu:575-612)              -> k_correct_d2m + k_zero_pad
-//   matrix_elementwise_multiply + shift_corr (utils.cu:156-192, ra_exec.cu:56-89) -> k_vis_out
+//       (ra_exec.cu:325-373, cuft.cu:575-612)              -> k_correct_d2m + k_zero_tpad
+//   cura_cufft plane transforms (cuft.cu:127-143)            -> cuFFT rows + k_cols_to_t / k_t_to_grid
+//   matrix_elementwise_multiply + shift_corr (utils.cu:156-192, ra_exec.cu:56-89) -> k_vis_out / k_interp_t
 //   thrust min/max over w (utils.cu:42-53)                  -> k_wrange
 #include "kernels.cuh"
 #include "plan.h"
@@ -854,15 +855,21 @@ __device__ __forceinline__ QuarterPix quarter(const DevCorr &cc, int r, int s) {
     return q;
 }
 
+// The transformed planes are read and written in the column-transposed
+// layout T[z][x'][y] (x' over the ny image columns in FFT order: grid column
+// x' for x' < ny - ny/2, nf1 - ny + x' above; y over nf2, contiguous), so the
+// y transforms are contiguous rows for cuFFT.  Thread index: r (the y side)
+// fastest, so a warp's plane accesses are contiguous.
+
 // ms2dirty epilogue: w-screen sum over planes + all corrections, one pass.
 template <typename T>
 __global__ void k_correct_m2d(DevCorr cc, const C<T> *__restrict__ grid, C<T> *__restrict__ dirty) {
     const int hx = cc.nx / 2, hy = cc.ny / 2;
     const long long nq = (long long)(hx + 1) * (hy + 1);
-    const long long plane = (long long)cc.nf1 * cc.nf2;
+    const long long plane = (long long)cc.ny * cc.nf2;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nq;
          q += (long long)gridDim.x * blockDim.x) {
-        int r = (int)(q / (hy + 1)), s = (int)(q - (long long)r * (hy + 1));
+        int s = (int)(q / (hx + 1)), r = (int)(q - (long long)s * (hx + 1));
         QuarterPix Q = quarter(cc, r, s);
         double sc, cs;
         sincos(Q.ph, &sc, &cs);
@@ -878,10 +885,10 @@ __global__ void k_correct_m2d(DevCorr cc, const C<T> *__restrict__ grid, C<T> *_
             for (int sy = 0; sy < 2; ++sy) {
                 int iy = sy ? hy - s : hy + s;
                 if (iy < 0 || iy >= cc.ny || (sy && s == 0)) continue;
-                int w1 = sy ? cc.nf1 - s : s;
+                int xp = sy ? cc.ny - s : s;               // image column of grid column nf1 - s / s
                 ixs[np] = ix;
                 iys[np] = iy;
-                off[np] = (long long)w2 * cc.nf1 + w1;
+                off[np] = (long long)xp * cc.nf2 + w2;
                 ++np;
             }
         }
@@ -913,15 +920,15 @@ __global__ void k_correct_m2d(DevCorr cc, const C<T> *__restrict__ grid, C<T> *_
 }
 
 // dirty2ms prologue: corrections + per-plane screen, written at the image cells
-// of every plane (the rest of the planes is zeroed by k_zero_pad).
+// of every plane of T (its other rows are zeroed by k_zero_tpad).
 template <typename T>
 __global__ void k_correct_d2m(DevCorr cc, const C<T> *__restrict__ dirty, C<T> *__restrict__ grid) {
     const int hx = cc.nx / 2, hy = cc.ny / 2;
     const long long nq = (long long)(hx + 1) * (hy + 1);
-    const long long plane = (long long)cc.nf1 * cc.nf2;
+    const long long plane = (long long)cc.ny * cc.nf2;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nq;
          q += (long long)gridDim.x * blockDim.x) {
-        int r = (int)(q / (hy + 1)), s = (int)(q - (long long)r * (hy + 1));
+        int s = (int)(q / (hx + 1)), r = (int)(q - (long long)s * (hx + 1));
         QuarterPix Q = quarter(cc, r, s);
         double sc, cs;
         sincos(-Q.ph, &sc, &cs);
@@ -937,11 +944,11 @@ __global__ void k_correct_d2m(DevCorr cc, const C<T> *__restrict__ dirty, C<T> *
             for (int sy = 0; sy < 2; ++sy) {
                 int iy = sy ? hy - s : hy + s;
                 if (iy < 0 || iy >= cc.ny || (sy && s == 0)) continue;
-                int w1 = sy ? cc.nf1 - s : s;
+                int xp = sy ? cc.ny - s : s;
                 C<T> d = dirty[(long long)ix * cc.ny + iy];
                 vr[np] = (double)d.x * fr - (double)d.y * fi;
                 vi[np] = (double)d.x * fi + (double)d.y * fr;
-                off[np] = (long long)w2 * cc.nf1 + w1;
+                off[np] = (long long)xp * cc.nf2 + w2;
                 ++np;
             }
         }
@@ -966,16 +973,67 @@ __global__ void k_correct_d2m(DevCorr cc, const C<T> *__restrict__ dirty, C<T> *
     }
 }
 
-// Zero every cell of every plane that k_correct_d2m does not write.
+// Grid column of image column x' (FFT order: the two corners of the x axis).
+__device__ __forceinline__ int grid_col(int xp, int ny, int nf1) { return xp < ny - ny / 2 ? xp : xp + nf1 - ny; }
+// Image column of grid column x, or -1 outside the image's columns.
+__device__ __forceinline__ int image_col(int x, int ny, int nf1) {
+    return x < ny - ny / 2 ? x : (x >= nf1 - ny / 2 ? x - nf1 + ny : -1);
+}
+
+// T[z][x'][y] = grid[z][y][grid_col(x')]: 32 x 32 tiles through shared memory,
+// reads along x, writes along y (both coalesced).  Grid: (ny/32, nf2/32, nf3).
 template <typename T>
-__global__ void k_zero_pad(int nx, int ny, int nf1, int nf2, int nf3, C<T> *__restrict__ grid) {
-    const long long rows = (long long)nf3 * nf2;
-    for (long long rr = blockIdx.x; rr < rows; rr += gridDim.x) {
-        int y = (int)(rr % nf2);
-        bool img = (y < nx - nx / 2) || (y >= nf2 - nx / 2);
-        int x0 = img ? ny - ny / 2 : 0, x1 = img ? nf1 - ny / 2 : nf1;
-        C<T> *row = grid + rr * nf1;
-        for (int x = x0 + threadIdx.x; x < x1; x += blockDim.x) row[x] = C<T>{0, 0};
+__global__ void __launch_bounds__(256) k_cols_to_t(int ny, int nf1, int nf2, const C<T> *__restrict__ grid,
+                                                   C<T> *__restrict__ t) {
+    __shared__ C<T> tile[32][33];
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+    const C<T> *gp = grid + (long long)blockIdx.z * nf1 * nf2;
+    C<T> *tp = t + (long long)blockIdx.z * ny * nf2;
+    const int xp = x0 + threadIdx.x;
+    const int gx = xp < ny ? grid_col(xp, ny, nf1) : 0;
+    for (int j = threadIdx.y; j < 32; j += 8) {
+        const int y = y0 + j;
+        if (xp < ny && y < nf2) tile[j][threadIdx.x] = gp[(long long)y * nf1 + gx];
+    }
+    __syncthreads();
+    const int y = y0 + threadIdx.x;
+    for (int j = threadIdx.y; j < 32; j += 8) {
+        const int xq = x0 + j;
+        if (xq < ny && y < nf2) tp[(long long)xq * nf2 + y] = tile[threadIdx.x][j];
+    }
+}
+
+// grid[z][y][x] = T[z][image_col(x)][y] for the image's columns, 0 elsewhere.
+// Grid: (nf1/32, nf2/32, nf3).
+template <typename T>
+__global__ void __launch_bounds__(256) k_t_to_grid(int ny, int nf1, int nf2, const C<T> *__restrict__ t,
+                                                   C<T> *__restrict__ grid) {
+    __shared__ C<T> tile[32][33];
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+    C<T> *gp = grid + (long long)blockIdx.z * nf1 * nf2;
+    const C<T> *tp = t + (long long)blockIdx.z * ny * nf2;
+    const int y = y0 + threadIdx.x;
+    for (int j = threadIdx.y; j < 32; j += 8) {
+        const int x = x0 + j;
+        const int xp = x < nf1 ? image_col(x, ny, nf1) : -1;
+        tile[j][threadIdx.x] = (xp >= 0 && y < nf2) ? tp[(long long)xp * nf2 + y] : C<T>{0, 0};
+    }
+    __syncthreads();
+    const int x = x0 + threadIdx.x;
+    for (int j = threadIdx.y; j < 32; j += 8) {
+        const int yy = y0 + j;
+        if (x < nf1 && yy < nf2) gp[(long long)yy * nf1 + x] = tile[threadIdx.x][j];
+    }
+}
+
+// Zero the rows of T that are not image rows (y in [nx - nx/2, nf2 - nx/2)),
+// which k_correct_d2m does not write.
+template <typename T>
+__global__ void k_zero_tpad(int nx, int nf2, long long nrows, C<T> *__restrict__ t) {
+    const int y0 = nx - nx / 2, y1 = nf2 - nx / 2;
+    for (long long rr = blockIdx.x; rr < nrows; rr += gridDim.x) {
+        C<T> *row = t + rr * nf2;
+        for (int y = y0 + threadIdx.x; y < y1; y += blockDim.x) row[y] = C<T>{0, 0};
     }
 }
 
@@ -1180,11 +1238,26 @@ void launch_correct_d2m(const DevCorr &cc, const void *dirty, void *grid, cudaSt
 }
 
 template <typename T>
-void launch_zero_pad(int nx, int ny, int nf1, int nf2, int nf3, void *grid, cudaStream_t st) {
-    long long rows = (long long)nf3 * nf2;
-    int blocks = rows > 148LL * 64 ? 148 * 64 : (int)rows;
+void launch_cols_to_t(int ny, int nf1, int nf2, int nf3, const void *grid, void *t, cudaStream_t st) {
     count_launch();
-    k_zero_pad<T><<<blocks, 256, 0, st>>>(nx, ny, nf1, nf2, nf3, reinterpret_cast<C<T> *>(grid));
+    dim3 g((ny + 31) / 32, (nf2 + 31) / 32, nf3);
+    k_cols_to_t<T><<<g, dim3(32, 8), 0, st>>>(ny, nf1, nf2, reinterpret_cast<const C<T> *>(grid),
+                                              reinterpret_cast<C<T> *>(t));
+}
+
+template <typename T>
+void launch_t_to_grid(int ny, int nf1, int nf2, int nf3, const void *t, void *grid, cudaStream_t st) {
+    count_launch();
+    dim3 g((nf1 + 31) / 32, (nf2 + 31) / 32, nf3);
+    k_t_to_grid<T><<<g, dim3(32, 8), 0, st>>>(ny, nf1, nf2, reinterpret_cast<const C<T> *>(t),
+                                              reinterpret_cast<C<T> *>(grid));
+}
+
+template <typename T>
+void launch_zero_tpad(int nx, int ny, int nf2, int nf3, void *t, cudaStream_t st) {
+    const long long rows = (long long)nf3 * ny;
+    count_launch();
+    k_zero_tpad<T><<<grid_for(rows, 1), 256, 0, st>>>(nx, nf2, rows, reinterpret_cast<C<T> *>(t));
 }
 
 #define CURIG_INSTANTIATE(T)                                                                          \
@@ -1203,7 +1276,9 @@ void launch_zero_pad(int nx, int ny, int nf1, int nf2, int nf3, void *grid, cuda
                                   VisIO, long long, int, cudaStream_t);                               \
     template void launch_correct_m2d<T>(const DevCorr &, const void *, void *, cudaStream_t);         \
     template void launch_correct_d2m<T>(const DevCorr &, const void *, void *, cudaStream_t);         \
-    template void launch_zero_pad<T>(int, int, int, int, int, void *, cudaStream_t);
+    template void launch_cols_to_t<T>(int, int, int, int, const void *, void *, cudaStream_t);         \
+    template void launch_t_to_grid<T>(int, int, int, int, const void *, void *, cudaStream_t);         \
+    template void launch_zero_tpad<T>(int, int, int, int, void *, cudaStream_t);
 
 CURIG_INSTANTIATE(float)
 CURIG_INSTANTIATE(double)

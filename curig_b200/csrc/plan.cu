@@ -187,6 +187,7 @@ void plan_release_points(Plan *p) {
     dfree(p->d_nsub, st); dfree(p->d_sub_end, st); dfree(p->d_key_a, st); dfree(p->d_key_b, st);
     dfree(p->d_val_a, st); dfree(p->d_idx, st); dfree(p->d_err, st); dfree(p->d_keys, st);
     dfree(p->d_rec, st); dfree(p->d_ph, st); dfree(p->d_cs, st); dfree(p->d_grid, st); dfree(p->d_tmp, st);
+    dfree(p->d_tgrid, st);
     p->ready = false;
 }
 
@@ -473,67 +474,72 @@ retry_tiles:
     // 5. fine grid and FFT plans
     size_t gbytes = (size_t)gp.nf1 * gp.nf2 * gp.nf3 * 2 * esize;
     CU_TRY(dalloc(&p->d_grid, gbytes, st));
-    // pruned 2-D transforms: rows (x, length nf1) of every plane, columns (y,
-    // length nf2) only for the image's columns x < ny - ny/2 and x >= nf1 - ny/2
-    const long long nrows = (long long)gp.nf2 * gp.nf3;
-    p->fft_rows = (int)std::max(1LL, std::min(nrows, (1LL << 28) / gp.nf1));
-    p->fft_rows_rest = (int)(nrows % p->fft_rows);
-    p->fft_cols_a = p->ny - p->ny / 2;
-    p->fft_cols_b = p->ny / 2;
+    // 2-D transforms as two passes of contiguous rows: x rows of every plane
+    // (length nf1), and y rows (length nf2) of the image's columns only, kept
+    // transposed in d_tgrid [nf3][ny][nf2]
+    CU_TRY(dalloc(&p->d_tgrid, (size_t)gp.nf3 * p->ny * gp.nf2 * 2 * esize, st));
+    const long long nxrows = (long long)gp.nf2 * gp.nf3, nyrows = (long long)p->ny * gp.nf3;
+    p->fft_bx = (int)std::max(1LL, std::min(nxrows, (1LL << 28) / gp.nf1));
+    p->fft_bx_rest = (int)(nxrows % p->fft_bx);
+    p->fft_by = (int)std::max(1LL, std::min(nyrows, (1LL << 28) / gp.nf2));
+    p->fft_by_rest = (int)(nyrows % p->fft_by);
     const int pr = p->opt.precision;
-    if (fft_plan1(p->device, gp.nf1, 1, gp.nf1, p->fft_rows, pr, p->fft_h_rows)) return ERR_CUFFT;
-    if (p->fft_rows_rest && fft_plan1(p->device, gp.nf1, 1, gp.nf1, p->fft_rows_rest, pr, p->fft_h_rows_rest))
+    if (fft_plan1(p->device, gp.nf1, 1, gp.nf1, p->fft_bx, pr, p->fft_hx)) return ERR_CUFFT;
+    if (p->fft_bx_rest && fft_plan1(p->device, gp.nf1, 1, gp.nf1, p->fft_bx_rest, pr, p->fft_hx_rest))
         return ERR_CUFFT;
-    if (fft_plan1(p->device, gp.nf2, gp.nf1, 1, p->fft_cols_a, pr, p->fft_h_cols_a)) return ERR_CUFFT;
-    if (p->fft_cols_b && fft_plan1(p->device, gp.nf2, gp.nf1, 1, p->fft_cols_b, pr, p->fft_h_cols_b))
+    if (fft_plan1(p->device, gp.nf2, 1, gp.nf2, p->fft_by, pr, p->fft_hy)) return ERR_CUFFT;
+    if (p->fft_by_rest && fft_plan1(p->device, gp.nf2, 1, gp.nf2, p->fft_by_rest, pr, p->fft_hy_rest))
         return ERR_CUFFT;
     mark(p, EV_SET_END);
     p->ready = true;
     return OK;
 }
 
-static int fft_exec(Plan *p, cufftHandle h, long long offset, int dir) {
+static int fft_exec(Plan *p, cufftHandle h, void *base, long long offset, int dir) {
     if (cufftSetStream(h, p->st) != CUFFT_SUCCESS) return ERR_CUFFT;
     cufftResult r;
     if (p->opt.precision) {
-        cufftComplex *d = reinterpret_cast<cufftComplex *>(p->d_grid) + offset;
+        cufftComplex *d = reinterpret_cast<cufftComplex *>(base) + offset;
         r = cufftExecC2C(h, d, d, dir);
     } else {
-        cufftDoubleComplex *d = reinterpret_cast<cufftDoubleComplex *>(p->d_grid) + offset;
+        cufftDoubleComplex *d = reinterpret_cast<cufftDoubleComplex *>(base) + offset;
         r = cufftExecZ2Z(h, d, d, dir);
     }
     return r == CUFFT_SUCCESS ? OK : ERR_CUFFT;
 }
 
-// 2-D transform of every plane (cuft.cu:127-143), pruned to the image: after
-// ms2dirty's transform only the image columns are read, and before dirty2ms's
-// transform only they are non-zero (the rest was zeroed by k_zero_pad), so the
-// column pass runs over those columns only — rows first for ms2dirty, columns
-// first for dirty2ms.
-static int run_fft(Plan *p, int dir, bool rows_first) {
+// Batched contiguous row transforms of length n over nrows rows of buf.
+static int fft_rows(Plan *p, void *buf, long long nrows, int n, cufftHandle h, int b, cufftHandle h_rest,
+                    int b_rest, int dir) {
+    for (long long r = 0; r < nrows;) {
+        const bool full = nrows - r >= b;
+        int s = fft_exec(p, full ? h : h_rest, buf, r * n, dir);
+        if (s) return s;
+        r += full ? b : b_rest;
+    }
+    return OK;
+}
+
+// 2-D transform of every plane (cuft.cu:127-143) restricted to what the image
+// needs.  ms2dirty: x rows of the whole grid, then the image's columns are
+// transposed into d_tgrid and transformed along y there (the correction reads
+// d_tgrid).  dirty2ms: the correction writes d_tgrid, y rows are transformed,
+// the columns go back into the grid (other columns zeroed), then x rows.
+template <typename T>
+static int plane_fft(Plan *p, int dir, bool m2d) {
     const GridParams &gp = p->gp;
-    const long long plane = (long long)gp.nf1 * gp.nf2, nrows = (long long)gp.nf2 * gp.nf3;
-    auto rows = [&]() {
-        for (long long r = 0; r < nrows;) {
-            const bool full = nrows - r >= p->fft_rows;
-            int s = fft_exec(p, full ? p->fft_h_rows : p->fft_h_rows_rest, r * gp.nf1, dir);
-            if (s) return s;
-            r += full ? p->fft_rows : p->fft_rows_rest;
-        }
-        return (int)OK;
-    };
-    auto cols = [&]() {
-        for (int z = 0; z < gp.nf3; ++z) {
-            int s = fft_exec(p, p->fft_h_cols_a, z * plane, dir);
-            if (s) return s;
-            if (p->fft_cols_b && (s = fft_exec(p, p->fft_h_cols_b, z * plane + gp.nf1 - p->fft_cols_b, dir)))
-                return s;
-        }
-        return (int)OK;
-    };
-    int s = rows_first ? rows() : cols();
-    if (s) return s;
-    return rows_first ? cols() : rows();
+    const long long nx_rows = (long long)gp.nf2 * gp.nf3, ny_rows = (long long)p->ny * gp.nf3;
+    int s;
+    if (m2d) {
+        if ((s = fft_rows(p, p->d_grid, nx_rows, gp.nf1, p->fft_hx, p->fft_bx, p->fft_hx_rest, p->fft_bx_rest, dir)))
+            return s;
+        launch_cols_to_t<T>(p->ny, gp.nf1, gp.nf2, gp.nf3, p->d_grid, p->d_tgrid, p->st);
+        return fft_rows(p, p->d_tgrid, ny_rows, gp.nf2, p->fft_hy, p->fft_by, p->fft_hy_rest, p->fft_by_rest, dir);
+    }
+    if ((s = fft_rows(p, p->d_tgrid, ny_rows, gp.nf2, p->fft_hy, p->fft_by, p->fft_hy_rest, p->fft_by_rest, dir)))
+        return s;
+    launch_t_to_grid<T>(p->ny, gp.nf1, gp.nf2, gp.nf3, p->d_tgrid, p->d_grid, p->st);
+    return fft_rows(p, p->d_grid, nx_rows, gp.nf1, p->fft_hx, p->fft_bx, p->fft_hx_rest, p->fft_bx_rest, dir);
 }
 
 template <typename T>
@@ -556,17 +562,17 @@ static int execute_t(Plan *p, int type, void *d_vis, const void *d_wgt, void *d_
                              st);
         if (s) return s;
         mark(p, EV_M2D_SPREAD);
-        s = run_fft(p, CUFFT_INVERSE, true);     // +1, cuft.cu:127-143
+        s = plane_fft<T>(p, CUFFT_INVERSE, true);    // +1, cuft.cu:127-143
         if (s) return s;
         mark(p, EV_M2D_FFT);
-        launch_correct_m2d<T>(p->dc, p->d_grid, d_dirty, st);
+        launch_correct_m2d<T>(p->dc, p->d_tgrid, d_dirty, st);
         mark(p, EV_M2D_END);
     } else {
         mark(p, EV_D2M_BEGIN);
-        launch_zero_pad<T>(p->nx, p->ny, gp.nf1, gp.nf2, gp.nf3, p->d_grid, st);
-        launch_correct_d2m<T>(p->dc, d_dirty, p->d_grid, st);
+        launch_zero_tpad<T>(p->nx, p->ny, gp.nf2, gp.nf3, p->d_tgrid, st);
+        launch_correct_d2m<T>(p->dc, d_dirty, p->d_tgrid, st);
         mark(p, EV_D2M_CORRECT);
-        s = run_fft(p, CUFFT_FORWARD, false);    // -1
+        s = plane_fft<T>(p, CUFFT_FORWARD, false);   // -1
         if (s) return s;
         mark(p, EV_D2M_FFT);
         const VisIO io{p->d_idx, p->d_ph, d_wgt, d_vis};

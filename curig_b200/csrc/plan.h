@@ -53,10 +53,12 @@ struct Plan {
     int *d_err = nullptr;
     unsigned long long *d_keys = nullptr;
     void *d_rec = nullptr, *d_ph = nullptr, *d_cs = nullptr, *d_grid = nullptr, *d_tmp = nullptr;
+    void *d_tgrid = nullptr;           // image columns of every plane, transposed: [nf3][ny][nf2]
     size_t tmp_bytes = 0;
 
-    cufftHandle fft_h_rows = 0, fft_h_rows_rest = 0, fft_h_cols_a = 0, fft_h_cols_b = 0;
-    int fft_rows = 0, fft_rows_rest = 0, fft_cols_a = 0, fft_cols_b = 0;   // rows per call, image columns
+    // x transforms on grid rows, y transforms on rows of the column-transposed planes
+    cufftHandle fft_hx = 0, fft_hx_rest = 0, fft_hy = 0, fft_hy_rest = 0;
+    int fft_bx = 0, fft_bx_rest = 0, fft_by = 0, fft_by_rest = 0;         // rows per call
 
     // learned-window tables per width (coefficients [kw][deg+1]); empty -> ES only
     std::vector<Window> learned;
@@ -130,7 +132,11 @@ void launch_correct_m2d(const DevCorr &cc, const void *grid, void *dirty, cudaSt
 template <typename T>
 void launch_correct_d2m(const DevCorr &cc, const void *dirty, void *grid, cudaStream_t st);
 template <typename T>
-void launch_zero_pad(int nx, int ny, int nf1, int nf2, int nf3, void *grid, cudaStream_t st);
+void launch_cols_to_t(int ny, int nf1, int nf2, int nf3, const void *grid, void *t, cudaStream_t st);
+template <typename T>
+void launch_t_to_grid(int ny, int nf1, int nf2, int nf3, const void *t, void *grid, cudaStream_t st);
+template <typename T>
+void launch_zero_tpad(int nx, int ny, int nf2, int nf3, void *t, cudaStream_t st);
 
 // global learned-window registry (set through the C ABI)
 int registry_set_window(int kw, int degree, const double *coef, double eps_reached);
