@@ -973,6 +973,18 @@ __global__ void k_correct_d2m(DevCorr cc, const C<T> *__restrict__ dirty, C<T> *
     }
 }
 
+// psi-hat of the window on the grid (deconv.cu:60-103): out[k] =
+// 2 sum_i g_i cos((x_i - N + 1) / (N - 1) pi k), N = nf/2 + 1, the same
+// arithmetic as the host psi_hat_grid.
+__global__ void k_psi_grid(int n, int nq, const double *__restrict__ qx, const double *__restrict__ qg,
+                           double *__restrict__ out) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int i = 0; i < nq; ++i) s += qg[i] * cos((qx[i] - n + 1) / (double)(n - 1) * PI_D * k);
+        out[k] = 2 * s;
+    }
+}
+
 // Grid column of image column x' (FFT order: the two corners of the x axis).
 __device__ __forceinline__ int grid_col(int xp, int ny, int nf1) { return xp < ny - ny / 2 ? xp : xp + nf1 - ny; }
 // Image column of grid column x, or -1 outside the image's columns.
@@ -1251,6 +1263,11 @@ void launch_t_to_grid(int ny, int nf1, int nf2, int nf3, const void *t, void *gr
     dim3 g((nf1 + 31) / 32, (nf2 + 31) / 32, nf3);
     k_t_to_grid<T><<<g, dim3(32, 8), 0, st>>>(ny, nf1, nf2, reinterpret_cast<const C<T> *>(t),
                                               reinterpret_cast<C<T> *>(grid));
+}
+
+void launch_psi_grid(int n, int nq, const double *qx, const double *qg, double *out, cudaStream_t st) {
+    count_launch();
+    k_psi_grid<<<grid_for(n, 128), 128, 0, st>>>(n, nq, qx, qg, out);
 }
 
 template <typename T>

@@ -386,20 +386,19 @@ retry_tiles:
     g.o_center = gp.o_center; g.sign = (double)gp.sign;
 
     // 3. correction tables (deconv.cu:60-197): psi1, psi2 on the grid, quadrature for psi3
-    std::vector<double> psi1, psi2;
-    psi_hat_grid(gp.nf1, gp.kp, p->win, psi1);
-    psi_hat_grid(gp.nf2, gp.kp, p->win, psi2);
+    //    (psi1 / psi2 evaluated on the device from the quadrature: no host work
+    //    while the GPU waits)
     double qx[MAX_QUAD], qg[MAX_QUAD];
     int nq = quadrature_terms(gp.kp, p->win, qx, qg);
     CU_TRY(dalloc(&p->d_foc, nchan * sizeof(double), st));
     CU_TRY(dalloc(&p->d_quad, 2 * MAX_QUAD * sizeof(double), st));
-    CU_TRY(dalloc(&p->d_psi1, psi1.size() * sizeof(double), st));
-    CU_TRY(dalloc(&p->d_psi2, psi2.size() * sizeof(double), st));
+    CU_TRY(dalloc(&p->d_psi1, (gp.nf1 / 2 + 1) * sizeof(double), st));
+    CU_TRY(dalloc(&p->d_psi2, (gp.nf2 / 2 + 1) * sizeof(double), st));
     CU_TRY(cudaMemcpyAsync(p->d_foc, foc.data(), nchan * sizeof(double), cudaMemcpyHostToDevice, st));
     CU_TRY(cudaMemcpyAsync(p->d_quad, qx, nq * sizeof(double), cudaMemcpyHostToDevice, st));
     CU_TRY(cudaMemcpyAsync(p->d_quad + MAX_QUAD, qg, nq * sizeof(double), cudaMemcpyHostToDevice, st));
-    CU_TRY(cudaMemcpyAsync(p->d_psi1, psi1.data(), psi1.size() * sizeof(double), cudaMemcpyHostToDevice, st));
-    CU_TRY(cudaMemcpyAsync(p->d_psi2, psi2.data(), psi2.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    launch_psi_grid(gp.nf1 / 2 + 1, nq, p->d_quad, p->d_quad + MAX_QUAD, p->d_psi1, st);
+    launch_psi_grid(gp.nf2 / 2 + 1, nq, p->d_quad, p->d_quad + MAX_QUAD, p->d_psi2, st);
     if (p->win.kind == 1) {
         CU_TRY(dalloc(&p->d_wcoef, p->win.coef.size() * sizeof(double), st));
         CU_TRY(cudaMemcpyAsync(p->d_wcoef, p->win.coef.data(), p->win.coef.size() * sizeof(double),

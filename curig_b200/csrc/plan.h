@@ -137,6 +137,7 @@ template <typename T>
 void launch_t_to_grid(int ny, int nf1, int nf2, int nf3, const void *t, void *grid, cudaStream_t st);
 template <typename T>
 void launch_zero_tpad(int nx, int ny, int nf2, int nf3, void *t, cudaStream_t st);
+void launch_psi_grid(int n, int nq, const double *qx, const double *qg, double *out, cudaStream_t st);
 
 // global learned-window registry (set through the C ABI)
 int registry_set_window(int kw, int degree, const double *coef, double eps_reached);
