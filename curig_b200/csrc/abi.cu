@@ -94,6 +94,7 @@ static int oneshot(int type, long long nrow, int nchan, int nx, int ny, double p
             if (type == 1) chk(cudaMemcpyAsync(dirty, d_dirty, npix * cs, cudaMemcpyDeviceToHost, st));
             else chk(cudaMemcpyAsync(vis, d_vis, M * cs, cudaMemcpyDeviceToHost, st));
         }
+        if (s == OK) s = plan_device_status(p);   // flags raised by kernels (synchronises)
         if (p && s != OK && !p->last_error.empty()) g_last_error = p->last_error;
         if (p) plan_destroy(p);
     }

@@ -171,7 +171,7 @@ __global__ void k_bin_keys(DevGeom g, const double *__restrict__ uu, const doubl
         if (e) {
             atomicOr(err, e);
         } else {
-            unsigned cell = g.cbits ? (unsigned)((L.lz * g.ty + L.ly) * g.tx + L.lx) & 31u : 0u;
+            unsigned cell = g.cbits ? (unsigned)((L.lz * g.ty + L.ly) * g.tpitch + L.lx) & 31u : 0u;
             key = ((unsigned)L.bin << g.cbits) | cell;
         }
         keys[j] = key;
@@ -314,7 +314,7 @@ __global__ void __launch_bounds__(NTHREADS)
 k_spread(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__ bin_count,
          const int *__restrict__ sub_end, const R<T> *__restrict__ rec, const C<T> *__restrict__ cs,
          C<T> *__restrict__ grid, const double *__restrict__ wcoef) {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     const int kw = KW > 0 ? KW : g.kw;
     const int ntile = g.tx * g.ty * g.tz;
     C<T> *tile = reinterpret_cast<C<T> *>(smem);
@@ -383,7 +383,7 @@ __global__ void __launch_bounds__(NTHREADS)
 k_interp(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__ bin_count,
          const int *__restrict__ sub_end, const R<T> *__restrict__ rec, const C<T> *__restrict__ grid,
          C<T> *__restrict__ os, const double *__restrict__ wcoef) {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     const int kw = KW > 0 ? KW : g.kw;
     const int ntile = g.tx * g.ty * g.tz;
     C<T> *tile = reinterpret_cast<C<T> *>(smem);
@@ -525,15 +525,15 @@ __global__ void __launch_bounds__(TTHREADS, sizeof(T) == 4 ? 2 : 1)
 k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__ bin_count,
            const int *__restrict__ sub_end, const R<T> *__restrict__ rec, const C<T> *__restrict__ cs,
            C<T> *__restrict__ grid, const WinTab<T> tab) {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     __shared__ T redbuf[TWARPS];
-    const int ntile = g.tx * g.ty * g.tz;
+    const int ntile = g.tpitch * g.ty * g.tz;            // tile [tz][ty][tpitch], columns >= tx stay 0
     const bool fix = sizeof(T) == 4 && g.smode == 0;    // FP32: exact two-word int32 fixed point
     const bool fix1 = sizeof(T) == 4 && g.smode == 2;   // FP32: one-word int32 fixed point
     const int csz = fix ? 16 : (int)sizeof(C<T>);       // bytes per complex cell
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int total = sub_end[g.nbins - 1];
-    const int tx = g.tx, txy = g.tx * g.ty;
+    const int tx = g.tpitch, txy = g.tpitch * g.ty;
     const int nvec = (ntile * csz) / 16;
     int *fhr = reinterpret_cast<int *>(smem);          // two-word planes: re-high, re-low, im-high, im-low
     int *flr = fhr + ntile, *fhi = flr + ntile, *fli = fhi + ntile;
@@ -722,20 +722,22 @@ __device__ __forceinline__ void vis_store(const VisIO &io, int i, C<T> v) {
     static_cast<C<T> *>(io.vis)[j] = C<T>{(v.x * e.x + v.y * e.y) * wt, (v.y * e.x - v.x * e.y) * wt};
 }
 
-// Stage the tile (wrapped rows of all its planes): rows are walked without
-// divisions and eight rows are in flight per warp before the shared stores.
+// Interpolator tile layout: [tz][ty][tpitch], column c holding grid x =
+// x_al + c with x_al = ox rounded down to even (so a TMA box may start there),
+// i.e. tile cell lx of the bin at column lx + (ox & 1).
+//
+// Stage the tile (wrapped rows of all its planes) with plain loads: rows are
+// walked without divisions and eight rows are in flight per warp before the
+// shared stores.
 template <typename T>
-__device__ __forceinline__ void load_tile(const DevGeom &g, const C<T> *__restrict__ grid, C<T> *tile,
-                                          long long b, int warp, int lane) {
-    long long bxi = b % g.nbx, byi = (b / g.nbx) % g.nby, bzi = b / ((long long)g.nbx * g.nby);
-    int ox = (int)bxi * g.bx - g.hkw, oy = (int)byi * g.by - g.hkw;
-    int oz = g.zpad ? (int)bzi * g.bz - g.hkw : 0;
-    const int nrows = g.ty * g.tz;
+__device__ __forceinline__ void load_tile(const DevGeom &g, const C<T> *__restrict__ grid, C<T> *tile, int x_al,
+                                          int oy, int oz, int warp, int lane) {
+    const int nrows = g.ty * g.tz, W = g.tpitch;
     constexpr int RB = 8;
-    for (int x0 = 0; x0 < g.tx; x0 += 32) {
+    for (int x0 = 0; x0 < W; x0 += 32) {
         const int x = x0 + lane;
-        const bool xin = x < g.tx;
-        const int gx = wrap3(ox + x, g.nf1);
+        const bool xin = x < W;
+        const int gx = wrap3(x_al + x, g.nf1);
         int row = warp, y = warp % g.ty, z = warp / g.ty;
         while (row < nrows) {
             C<T> v[RB];
@@ -754,28 +756,87 @@ __device__ __forceinline__ void load_tile(const DevGeom &g, const C<T> *__restri
             }
 #pragma unroll
             for (int k = 0; k < RB; ++k)
-                if (xin && rr[k] < nrows) tile[rr[k] * g.tx + x] = v[k];
+                if (xin && rr[k] < nrows) tile[rr[k] * W + x] = v[k];
         }
     }
 }
+
+// mbarrier / TMA helpers (PTX): one-shot barrier per tile, byte-count completion.
+__device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
+    unsigned ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(smem_addr(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+// 3-D tiled box load (no multicast) of {x, y, z} (x in elements, x even) into dst.
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, unsigned long long *bar, int x, int y,
+                                            int z) {
+    asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
+                 ::"r"(smem_addr(dst)), "l"(map), "r"(smem_addr(bar)), "r"(x), "r"(y), "r"(z)
+                 : "memory");
+}
+constexpr long long TMA_WAIT_LIMIT = 1LL << 26;   // try_wait polls (seconds): then the error flag
 
 template <typename T, int KW>
 __global__ void __launch_bounds__(NTHREADS, sizeof(T) == 4 ? 3 : 2)
 k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__ bin_count,
            const int *__restrict__ sub_end, const R<T> *__restrict__ rec, const C<T> *__restrict__ grid,
-           const WinTab<T> tab, const VisIO io) {
-    extern __shared__ __align__(16) unsigned char smem[];
+           const WinTab<T> tab, const VisIO io, const __grid_constant__ CUtensorMap tmap, int *err) {
+    extern __shared__ __align__(128) unsigned char smem[];
     __shared__ C<T> partial[NTHREADS];      // per (column, part, lane) sums of split visibilities
+    __shared__ unsigned long long bar;      // TMA completion barrier
     C<T> *tile = reinterpret_cast<C<T> *>(smem);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int total = sub_end[g.nbins - 1];
-    const int tx = g.tx, txy = g.tx * g.ty;
+    const int tx = g.tpitch, txy = g.tpitch * g.ty;
+    const unsigned tile_bytes = (unsigned)(g.tpitch * g.ty * g.tz * sizeof(C<T>));
+    unsigned parity = 0;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
     for (int s = blockIdx.x; s < total; s += gridDim.x) {
         long long b;
         int start, stride, n;
         sub_range(g, bin_start, bin_count, sub_end, s, b, start, stride, n);
-        load_tile<T>(g, grid, tile, b, warp, lane);
-        __syncthreads();
+        const long long bxi = b % g.nbx, byi = (b / g.nbx) % g.nby, bzi = b / ((long long)g.nbx * g.nby);
+        const int ox = (int)bxi * g.bx - g.hkw, oy = (int)byi * g.by - g.hkw;
+        const int oz = g.zpad ? (int)bzi * g.bz - g.hkw : 0;
+        const int shift = ox & 1, x_al = ox - shift;
+        // interior tiles (no periodic wrap) in one TMA box; the rest with plain loads
+        const bool inner = sizeof(T) == 4 && g.use_tma && x_al >= 0 && x_al + g.tpitch <= g.nf1 && oy >= 0 &&
+                           oy + g.ty <= g.nf2 && (!g.zpad || (oz >= 0 && oz + g.tz <= g.nf3));
+        if (inner) {
+            if (threadIdx.x == 0) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // earlier reads of the tile
+                mbar_expect_tx(&bar, tile_bytes);
+                tma_load_3d(tile, &tmap, &bar, x_al, oy, oz);
+            }
+            long long polls = 0;
+            bool done = false;
+            while (!(done = mbar_try_wait(&bar, parity)) && ++polls < TMA_WAIT_LIMIT) {
+            }
+            parity ^= 1u;
+            if (__syncthreads_or(!done)) {          // the load never completed: flag it and stop
+                if (threadIdx.x == 0) atomicOr(err, EF_TIMEOUT);
+                return;
+            }
+        } else {
+            load_tile<T>(g, grid, tile, x_al, oy, oz, warp, lane);
+            __syncthreads();
+        }
         // same lane / position map and w-plane split as k_spread_t
         const int L = (n + 31) >> 5;
         const int S = max(1, min(KW, NWARPS / max(L, 1)));
@@ -793,7 +854,7 @@ k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
                 ky[d] = win_tap<T>(g, tab, r.y, d);
             }
             int cb = cell_bits(r.w);
-            const C<T> *base = tile + ((cb >> 20) & 0xfff) * txy + ((cb >> 10) & 0x3ff) * tx + (cb & 0x3ff);
+            const C<T> *base = tile + ((cb >> 20) & 0xfff) * txy + ((cb >> 10) & 0x3ff) * tx + (cb & 0x3ff) + shift;
             T ar = 0, ai = 0;
 #pragma unroll 1
             for (int dz = dz0; dz < dz1; ++dz) {
@@ -1132,8 +1193,11 @@ void launch_vis_out(long long M, const int *idx, const void *ph, const void *os,
 }
 
 size_t tile_smem_bytes(const TileGeom &tg, int esize, int kw, int wdeg) {
-    size_t s = (size_t)tg.tx * tg.ty * tg.tz * 2 * (tg.fix == 1 ? 8 : esize);   // two-word: 4 int32 per cell
-    if (tg.fix == 2) s += (size_t)tg.tx * tg.ty * 4;                           // one-word: column load histogram
+    // rows padded to an even pitch (tx + 1 rounded up): the same cell index in
+    // the spreader's and the interpolator's tiles (bank order of the sort key)
+    const size_t pitch = (size_t)((tg.tx + 2) & ~1);
+    size_t s = pitch * tg.ty * tg.tz * 2 * (tg.fix == 1 ? 8 : esize);   // two-word: 4 int32 per cell
+    if (tg.fix == 2) s += pitch * tg.ty * 4;                           // one-word: column load histogram
     s += (size_t)NWARPS * 3 * KSTR * esize;
     s += (size_t)kw * (wdeg + 1) * esize;
     return (s + 15) & ~(size_t)15;
@@ -1184,14 +1248,16 @@ static int launch_spread_kw(const DevGeom &g, size_t smem, const int *bs, const 
 template <typename T, int KW>
 static int launch_interp_kw(const DevGeom &g, size_t smem, const int *bs, const int *bc, const int *se,
                             const void *rec, const void *grid, void *os, const double *wc, const double *ht,
-                            const VisIO &io, long long M, int nsm, cudaStream_t st) {
+                            const VisIO &io, long long M, const CUtensorMap *tmap, int *err, int nsm,
+                            cudaStream_t st) {
     int blocks = 0, s;
     if constexpr (KW > 0) {
         auto kern = k_interp_t<T, KW>;
         if ((s = launch_persistent(kern, smem, nsm, blocks))) return s;
         count_launch();
         kern<<<blocks, NTHREADS, smem, st>>>(g, bs, bc, se, reinterpret_cast<const R<T> *>(rec),
-                                             reinterpret_cast<const C<T> *>(grid), make_tab<T>(g, ht), io);
+                                             reinterpret_cast<const C<T> *>(grid), make_tab<T>(g, ht), io,
+                                             *tmap, err);
     } else {
         auto kern = k_interp<T, 0>;
         if ((s = launch_persistent(kern, smem, nsm, blocks))) return s;
@@ -1229,8 +1295,8 @@ int launch_spread(const DevGeom &g, size_t smem, const int *bs, const int *bc, c
 template <typename T>
 int launch_interp(const DevGeom &g, size_t smem, const int *bs, const int *bc, const int *se,
                   const void *rec, const void *grid, void *os, const double *wc, const double *ht, VisIO io,
-                  long long M, int nsm, cudaStream_t st) {
-    CURIG_KW_SWITCH(launch_interp_kw, g, smem, bs, bc, se, rec, grid, os, wc, ht, io, M, nsm, st)
+                  long long M, const CUtensorMap *tmap, int *err, int nsm, cudaStream_t st) {
+    CURIG_KW_SWITCH(launch_interp_kw, g, smem, bs, bc, se, rec, grid, os, wc, ht, io, M, tmap, err, nsm, st)
 }
 
 template <typename T>
@@ -1290,7 +1356,7 @@ void launch_zero_tpad(int nx, int ny, int nf2, int nf3, void *t, cudaStream_t st
                                   VisIO, long long, int, cudaStream_t);                               \
     template int launch_interp<T>(const DevGeom &, size_t, const int *, const int *, const int *,     \
                                   const void *, const void *, void *, const double *, const double *, \
-                                  VisIO, long long, int, cudaStream_t);                               \
+                                  VisIO, long long, const CUtensorMap *, int *, int, cudaStream_t);   \
     template void launch_correct_m2d<T>(const DevCorr &, const void *, void *, cudaStream_t);         \
     template void launch_correct_d2m<T>(const DevCorr &, const void *, void *, cudaStream_t);         \
     template void launch_cols_to_t<T>(int, int, int, int, const void *, void *, cudaStream_t);         \

@@ -3,6 +3,8 @@
 
 #include "curig_internal.h"
 
+#include <cuda.h>                   // CUtensorMap (TMA descriptor of the grid)
+
 namespace curig {
 
 template <typename T> struct cplx_t;
@@ -18,6 +20,9 @@ struct DevGeom {
     int sub;                       // visibilities per sub-problem
     int cbits;                     // bits of the in-tile start cell in the sort key (0: bin only)
     int smode;                     // FP32 tile accumulation: 0 two-word int32, 1 float atomics, 2 one-word int32
+    int tpitch;                    // tile row pitch of the thread-per-visibility kernels: tx + 1 rounded up
+                                   // to even (the interpolator's rows start at an even x for TMA)
+    int use_tma;                   // interpolator stages interior tiles with one TMA box load (FP32)
     float wmax3;                   // bound on |kx ky kz| of the tabulated window
     long long nbins;
     double beta, c;                // ES parameters
@@ -40,7 +45,7 @@ struct DevCorr {
     const double *psi2;            // [nf2/2+1]
 };
 
-enum ErrFlag : int { EF_NONFINITE = 1, EF_RANGE = 2 };
+enum ErrFlag : int { EF_NONFINITE = 1, EF_RANGE = 2, EF_TIMEOUT = 4 };
 
 // Piecewise-polynomial window passed by value (kernel-parameter space, so the
 // Horner coefficients are uniform constant operands): c[d][i], interval d,

@@ -6,6 +6,8 @@
 // inside execute.
 #include "plan.h"
 
+#include <cudaTypedefs.h>        // PFN_cuTensorMapEncodeTiled
+
 #include <algorithm>
 #include <atomic>
 #include <climits>
@@ -49,6 +51,8 @@ static void keep_pool_memory(int device) {
     }
     done[device] = true;
 }
+
+static int encode_grid_map(Plan *p);
 
 // ------------------------------------------------------------------ cuFFT plan cache
 // Rank-1 batched in-place plans keyed by (device, length, element stride,
@@ -350,6 +354,8 @@ retry_tiles:
     g.kw = gp.kp.kw; g.hkw = gp.kp.kw / 2;
     g.bx = tg.bx; g.by = tg.by; g.bz = tg.bz; g.nbx = tg.nbx; g.nby = tg.nby; g.nbz = tg.nbz;
     g.tx = tg.tx; g.ty = tg.ty; g.tz = tg.tz; g.zpad = tg.zpad; g.sub = tg.sub;
+    g.tpitch = (tg.tx + 2) & ~1;
+    g.use_tma = 0;                          // set once the grid's TMA descriptor exists
     g.nbins = tg.nbins();
     g.beta = gp.kp.beta; g.c = gp.kp.c;
     g.wkind = p->win.kind; g.wdeg = p->win.kind ? p->win.degree : 0;
@@ -473,6 +479,11 @@ retry_tiles:
     // 5. fine grid and FFT plans
     size_t gbytes = (size_t)gp.nf1 * gp.nf2 * gp.nf3 * 2 * esize;
     CU_TRY(dalloc(&p->d_grid, gbytes, st));
+    // TMA descriptor of the grid for the interpolator's interior tile boxes
+    // ({tpitch, ty, tz} elements of 8 bytes; box edges <= 256, x starts even)
+    if (p->opt.precision && g.tpitch <= 256 && g.ty <= 256 && g.tz <= 256)
+        g.use_tma = encode_grid_map(p) == OK ? 1 : 0;
+
     // 2-D transforms as two passes of contiguous rows: x rows of every plane
     // (length nf1), and y rows (length nf2) of the image's columns only, kept
     // transposed in d_tgrid [nf3][ny][nf2]
@@ -492,6 +503,36 @@ retry_tiles:
     mark(p, EV_SET_END);
     p->ready = true;
     return OK;
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    }
+    return fn;
+}
+
+static int encode_grid_map(Plan *p) {
+    auto enc = tensor_map_encoder();
+    if (!enc) return ERR_UNSUPPORTED;
+    const GridParams &gp = p->gp;
+    const DevGeom &g = p->dg;
+    cuuint64_t dims[3] = {(cuuint64_t)gp.nf1, (cuuint64_t)gp.nf2, (cuuint64_t)gp.nf3};
+    cuuint64_t strides[2] = {(cuuint64_t)gp.nf1 * 8, (cuuint64_t)gp.nf1 * gp.nf2 * 8};
+    cuuint32_t box[3] = {(cuuint32_t)g.tpitch, (cuuint32_t)g.ty, (cuuint32_t)g.tz};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc(&p->tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, p->d_grid, dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? OK : ERR_UNSUPPORTED;
 }
 
 static int fft_exec(Plan *p, cufftHandle h, void *base, long long offset, int dir) {
@@ -576,12 +617,27 @@ static int execute_t(Plan *p, int type, void *d_vis, const void *d_wgt, void *d_
         mark(p, EV_D2M_FFT);
         const VisIO io{p->d_idx, p->d_ph, d_wgt, d_vis};
         s = launch_interp<T>(g, p->smem_interp, p->d_bin_start, p->d_bin_count, p->d_sub_end, p->d_rec, p->d_grid,
-                             p->d_cs, p->d_wcoef, p->htab.empty() ? nullptr : p->htab.data(), io, M, p->nsm, st);
+                             p->d_cs, p->d_wcoef, p->htab.empty() ? nullptr : p->htab.data(), io, M, &p->tmap,
+                             p->d_err, p->nsm, st);
         if (s) return s;
         mark(p, EV_D2M_INTERP);
         mark(p, EV_D2M_END);                     // the scatter runs inside the interpolator
     }
     CU_TRY(cudaGetLastError());
+    return OK;
+}
+
+// Error flags raised by kernels of earlier executes (an interpolator tile load
+// that never completed); waits for the plan's stream.
+int plan_device_status(Plan *p) {
+    if (!p || !p->d_err) return OK;
+    int herr = 0;
+    CU_TRY(cudaMemcpyAsync(&herr, p->d_err, sizeof(int), cudaMemcpyDeviceToHost, p->st));
+    CU_TRY(cudaStreamSynchronize(p->st));
+    if (herr & EF_TIMEOUT) {
+        p->last_error = "a tile load did not complete (timed out)";
+        return ERR_CUDA;
+    }
     return OK;
 }
 

@@ -54,6 +54,7 @@ struct Plan {
     unsigned long long *d_keys = nullptr;
     void *d_rec = nullptr, *d_ph = nullptr, *d_cs = nullptr, *d_grid = nullptr, *d_tmp = nullptr;
     void *d_tgrid = nullptr;           // image columns of every plane, transposed: [nf3][ny][nf2]
+    CUtensorMap tmap{};                // TMA descriptor of d_grid for the interpolator's tile boxes (FP32)
     size_t tmp_bytes = 0;
 
     // x transforms on grid rows, y transforms on rows of the column-transposed planes
@@ -126,7 +127,7 @@ int launch_spread(const DevGeom &g, size_t smem, const int *bs, const int *bc, c
 template <typename T>
 int launch_interp(const DevGeom &g, size_t smem, const int *bs, const int *bc, const int *se,
                   const void *rec, const void *grid, void *os, const double *wc, const double *ht, VisIO io,
-                  long long M, int nsm, cudaStream_t st);
+                  long long M, const CUtensorMap *tmap, int *err, int nsm, cudaStream_t st);
 template <typename T>
 void launch_correct_m2d(const DevCorr &cc, const void *grid, void *dirty, cudaStream_t st);
 template <typename T>
@@ -138,6 +139,8 @@ void launch_t_to_grid(int ny, int nf1, int nf2, int nf3, const void *t, void *gr
 template <typename T>
 void launch_zero_tpad(int nx, int ny, int nf2, int nf3, void *t, cudaStream_t st);
 void launch_psi_grid(int n, int nq, const double *qx, const double *qg, double *out, cudaStream_t st);
+
+int plan_device_status(Plan *p);
 
 // global learned-window registry (set through the C ABI)
 int registry_set_window(int kw, int degree, const double *coef, double eps_reached);
