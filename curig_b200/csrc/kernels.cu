@@ -298,6 +298,11 @@ __device__ __forceinline__ long long find_bin(const int *__restrict__ sub_end, l
 }
 
 __device__ __forceinline__ void atomic_add_c(float2 *p, float2 v) { atomicAdd(p, v); }
+// 16-byte vector reduction into global memory (address 16-byte aligned).
+__device__ __forceinline__ void red_add_v4(float *p, float a, float b, float c, float d) {
+    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(d)
+                 : "memory");
+}
 __device__ __forceinline__ void atomic_add_c(double2 *p, double2 v) {
     atomicAdd(&p->x, v.x);
     atomicAdd(&p->y, v.y);
@@ -543,6 +548,12 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
         long long b;
         int start, stride, n;
         sub_range(g, bin_start, bin_count, sub_end, s, b, start, stride, n);
+        // tile origin; columns are stored from x_al = ox rounded down to even
+        // (column lx + shift), the layout of the interpolator's tiles
+        const long long bxi = b % g.nbx, byi = (b / g.nbx) % g.nby, bzi = b / ((long long)g.nbx * g.nby);
+        const int ox = (int)bxi * g.bx - g.hkw, oy = (int)byi * g.by - g.hkw;
+        const int oz = g.zpad ? (int)bzi * g.bz - g.hkw : 0;
+        const int shift = ox & 1, x_al = ox - shift;
         float4 *tv = reinterpret_cast<float4 *>(smem);
         for (int e = threadIdx.x; e < nvec; e += TTHREADS) tv[e] = make_float4(0.f, 0.f, 0.f, 0.f);
         if (!fix)
@@ -628,7 +639,7 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
                 ky[d] = win_tap<T>(g, tab, r.y, d);
             }
             int cb = cell_bits(r.w);
-            int cell = ((cb >> 20) & 0xfff) * txy + ((cb >> 10) & 0x3ff) * tx + (cb & 0x3ff);
+            int cell = ((cb >> 20) & 0xfff) * txy + ((cb >> 10) & 0x3ff) * tx + (cb & 0x3ff) + shift;
             c.x *= q;
             c.y *= q;
 #pragma unroll 1
@@ -673,19 +684,21 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
             }
         }
         __syncthreads();
-        long long bxi = b % g.nbx, byi = (b / g.nbx) % g.nby, bzi = b / ((long long)g.nbx * g.nby);
-        int ox = (int)bxi * g.bx - g.hkw, oy = (int)byi * g.by - g.hkw;
-        int oz = g.zpad ? (int)bzi * g.bz - g.hkw : 0;
-        // Flush: thread t walks cells t, t + TTHREADS, ... of the tile in
-        // memory order with (x, y, z) advanced incrementally; fixed-point
-        // cells convert in FP32 (one rounding of each word, then one FMA).
+        // Flush: thread t walks the cell pairs (2p, 2p + 1) of the tile in memory
+        // order ((x, y, z) of the pair advanced incrementally; the pitch is even,
+        // so a pair never straddles rows); fixed-point cells convert in FP32 (one
+        // rounding of each word, then one FMA).  Tiles that do not wrap the
+        // periodic grid in x add a pair with one 16-byte vector reduction (the
+        // pair's grid column x_al + 2k is even); the rest add cell by cell.
         {
             const float qf = (float)qinv, qf18 = (float)(qinv * 262144.0);
-            const int ty = g.ty, q0 = TTHREADS / tx;
-            const int sx = TTHREADS - q0 * tx, sy = q0 % ty, sz = q0 / ty;
-            int x = threadIdx.x % tx, yz = threadIdx.x / tx;
+            const bool xin = x_al >= 0 && x_al + tx <= g.nf1;
+            const int ty = g.ty, npair = ntile >> 1, hp = tx >> 1;      // pairs per row: hp
+            const int q0 = TTHREADS / hp;
+            const int sx = TTHREADS - q0 * hp, sy = q0 % ty, sz = q0 / ty;
+            int xp = threadIdx.x % hp, yz = threadIdx.x / hp;
             int y = yz % ty, z = yz / ty;
-            for (int e = threadIdx.x; e < ntile; e += TTHREADS) {
+            auto cellv = [&](int e) {
                 C<T> v;
                 if (fix) {
                     v.x = (T)fmaf(__int2float_rn(fhr[e]), qf18, __int2float_rn(flr[e]) * qf);
@@ -696,13 +709,30 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
                 } else {
                     v = reinterpret_cast<const C<T> *>(smem)[e];
                 }
-                if (v.x != (T)0 || v.y != (T)0) {
-                    int gx = wrap3(ox + x, g.nf1), gy = wrap3(oy + y, g.nf2);
-                    int gz = g.zpad ? wrap3(oz + z, g.nf3) : z;
-                    atomic_add_c(grid + ((long long)gz * g.nf2 + gy) * g.nf1 + gx, v);
+                return v;
+            };
+            for (int pr = threadIdx.x; pr < npair; pr += TTHREADS) {
+                const C<T> v0 = cellv(2 * pr), v1 = cellv(2 * pr + 1);
+                const bool nz0 = v0.x != (T)0 || v0.y != (T)0, nz1 = v1.x != (T)0 || v1.y != (T)0;
+                if (nz0 || nz1) {
+                    const int gy = wrap3(oy + y, g.nf2);
+                    const int gz = g.zpad ? wrap3(oz + z, g.nf3) : z;
+                    C<T> *grow = grid + ((long long)gz * g.nf2 + gy) * g.nf1;
+                    const int c0 = 2 * xp;
+                    bool vec = false;
+                    if constexpr (sizeof(T) == 4) {
+                        if (xin) {
+                            red_add_v4(reinterpret_cast<float *>(grow + x_al + c0), v0.x, v0.y, v1.x, v1.y);
+                            vec = true;
+                        }
+                    }
+                    if (!vec) {
+                        if (nz0) atomic_add_c(grow + wrap3(x_al + c0, g.nf1), v0);
+                        if (nz1) atomic_add_c(grow + wrap3(x_al + c0 + 1, g.nf1), v1);
+                    }
                 }
-                x += sx;
-                if (x >= tx) { x -= tx; ++y; }
+                xp += sx;
+                if (xp >= hp) { xp -= hp; ++y; }
                 y += sy;
                 z += sz;
                 if (y >= ty) { y -= ty; ++z; }
