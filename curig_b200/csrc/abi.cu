@@ -30,6 +30,9 @@ static Options to_options(const curig_opts *o) {
         opt.smem_budget = o->smem_budget > 0 ? (size_t)o->smem_budget : 0;
         opt.stream = (cudaStream_t)o->stream;
         opt.smode = o->accumulate;
+        opt.w_term = o->w_term;
+        opt.grid_x = o->grid_x;
+        opt.grid_y = o->grid_y;
     }
     return opt;
 }

@@ -68,6 +68,7 @@ struct GridParams {
     double o_center = 0, o_half = 0;   // n-1 range
     double gamma = 1, h = 0;
     int sign = 1;
+    int no_w = 0;                // w ignored: one plane, n = 1, no w phase
     KernelParams kp;
 };
 
@@ -80,9 +81,15 @@ void gauss_legendre(int n, double *x, double *w);
 int quadrature_terms(const KernelParams &kp, const Window &win, double *xs, double *g);
 double window_value(const KernelParams &kp, const Window &win, double t);
 void psi_hat_grid(int nf, const KernelParams &kp, const Window &win, std::vector<double> &out);
+// Optional sizing requests: an explicit oversampled grid (grid_x along the
+// nxdirty axis, grid_y along nydirty; 0 = the sigma rule) and the no-w mode.
+struct GridRequest {
+    int grid_x = 0, grid_y = 0;
+    int no_w = 0;
+};
 int grid_params(int nx, int ny, double pixsize_x, double pixsize_y, double wmin_eff,
                 double wmax_eff, double eps, double sigma, int sign, GridParams &gp,
-                int kw_override = 0);
+                int kw_override = 0, const GridRequest &req = GridRequest());
 void es_horner_window(const KernelParams &kp, int degree, Window &win);
 
 // ------------------------------------------------------------------ tiles

@@ -106,7 +106,11 @@ __device__ __forceinline__ int locate(const DevGeom &g, double gx, double gy, do
     int bxi, byi, bzi;
     axis_loc(gx, g.nf1, g.bx, g.nbx, g.hkw, g.kw, bxi, L.lx, L.ux);
     axis_loc(gy, g.nf2, g.by, g.nby, g.hkw, g.kw, byi, L.ly, L.uy);
-    if (g.zpad) {
+    if (g.no_w) {                                  // one plane, no z taps
+        L.lz = 0;
+        L.uz = 0.0;
+        bzi = 0;
+    } else if (g.zpad) {
         axis_loc(gz, g.nf3, g.bz, g.nbz, g.hkw, g.kw, bzi, L.lz, L.uz);
     } else {
         double sd = ceil(gz - 0.5 * g.kw);
@@ -119,7 +123,7 @@ __device__ __forceinline__ int locate(const DevGeom &g, double gx, double gy, do
         if (!(sd >= 0.0 && sd <= (double)(g.nf3 - g.kw))) return EF_RANGE;
     }
     if (L.lx < 0 || L.lx > g.tx - g.kw || L.ly < 0 || L.ly > g.ty - g.kw || L.lz < 0 ||
-        L.lz > g.tz - g.kw)
+        (!g.no_w && L.lz > g.tz - g.kw))
         return EF_RANGE;
     L.bin = ((long long)bzi * g.nby + byi) * g.nbx + bxi;
     return 0;
@@ -623,13 +627,14 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
         // fewer than TWARPS columns splits each visibility's w-planes into S
         // parts (one warp per column and part) so that all warps have work.
         const int L = (n + 31) >> 5;
-        const int S = max(1, min(KW, TWARPS / max(L, 1)));
+        const int KZ = g.no_w ? 1 : KW;                   // z taps (2-D: one, weight 1)
+        const int S = max(1, min(KZ, TWARPS / max(L, 1)));
         for (int u = warp; u < L * S; u += TWARPS) {
             const int k = u / S, part = u - k * S;
             const int m = lane * L + k;
             if (m >= n) continue;
             const int i = start + m * stride;
-            const int dz0 = part * KW / S, dz1 = (part + 1) * KW / S;
+            const int dz0 = part * KZ / S, dz1 = (part + 1) * KZ / S;
             R<T> r = rec[i];
             C<T> c = cs[i];
             T kx[KW], ky[KW];
@@ -644,7 +649,7 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
             c.y *= q;
 #pragma unroll 1
             for (int dz = dz0; dz < dz1; ++dz) {
-                T kz = win_tap<T>(g, tab, r.z, dz);
+                T kz = g.no_w ? (T)1 : win_tap<T>(g, tab, r.z, dz);
                 T cr = c.x * kz, ci = c.y * kz;
                 int pz = cell + dz * txy;
 #pragma unroll
@@ -869,13 +874,14 @@ k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
         }
         // same lane / position map and w-plane split as k_spread_t
         const int L = (n + 31) >> 5;
-        const int S = max(1, min(KW, NWARPS / max(L, 1)));
+        const int KZ = g.no_w ? 1 : KW;
+        const int S = max(1, min(KZ, NWARPS / max(L, 1)));
         for (int u = warp; u < L * S; u += NWARPS) {
             const int k = u / S, part = u - k * S;
             const int m = lane * L + k;
             if (m >= n) continue;
             const int i = start + m * stride;
-            const int dz0 = part * KW / S, dz1 = (part + 1) * KW / S;
+            const int dz0 = part * KZ / S, dz1 = (part + 1) * KZ / S;
             R<T> r = rec[i];
             T kx[KW], ky[KW];
 #pragma unroll
@@ -888,7 +894,7 @@ k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
             T ar = 0, ai = 0;
 #pragma unroll 1
             for (int dz = dz0; dz < dz1; ++dz) {
-                T kz = win_tap<T>(g, tab, r.z, dz);
+                T kz = g.no_w ? (T)1 : win_tap<T>(g, tab, r.z, dz);
                 const C<T> *pz = base + dz * txy;
                 T sr = 0, si = 0;
 #pragma unroll
@@ -935,6 +941,13 @@ struct QuarterPix {
 
 __device__ __forceinline__ QuarterPix quarter(const DevCorr &cc, int r, int s) {
     QuarterPix q;
+    if (cc.no_w) {                                    // 2-D: no n, no w screen, no psi3
+        q.n = 1.0;
+        q.kp = 0.0;
+        q.psi3 = 1.0;
+        q.ph = 0.0;
+        return q;
+    }
     double a = (double)r * cc.psx, b = (double)s * cc.psy;
     q.n = sqrt(1.0 - a * a - b * b);                  // ra_exec.cu:31, precomp.cu:220
     double k = q.n - 1;

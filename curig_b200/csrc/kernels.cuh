@@ -23,6 +23,7 @@ struct DevGeom {
     int tpitch;                    // tile row pitch of the thread-per-visibility kernels: tx + 1 rounded up
                                    // to even (the interpolator's rows start at an even x for TMA)
     int use_tma;                   // interpolator stages interior tiles with one TMA box load (FP32)
+    int no_w;                      // w ignored: one plane, no z taps (window factor 1)
     float wmax3;                   // bound on |kx ky kz| of the tabulated window
     long long nbins;
     double beta, c;                // ES parameters
@@ -37,6 +38,7 @@ struct DevGeom {
 // Quarter-pixel correction geometry (ms2dirty epilogue / dirty2ms prologue).
 struct DevCorr {
     int nx, ny, nf1, nf2, nf3;
+    int no_w;                      // n = 1, psi3 = 1, no w phase
     double psx, psy, o_center, i_center, gamma, h;
     int nquad;
     const double *qx;              // quadrature nodes (grid units)

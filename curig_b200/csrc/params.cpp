@@ -160,11 +160,18 @@ void psi_hat_grid(int nf, const KernelParams &kp, const Window &win, std::vector
 }
 
 int grid_params(int nx, int ny, double psx, double psy, double wmin, double wmax, double eps,
-                double sigma, int sign, GridParams &gp, int kw_override) {
+                double sigma, int sign, GridParams &gp, int kw_override, const GridRequest &req) {
     gp = GridParams();
     if (nx <= 0 || ny <= 0) return ERR_ARG;
     if (!std::isfinite(wmin) || !std::isfinite(wmax) || !std::isfinite(psx) || !std::isfinite(psy))
         return ERR_NONFINITE;
+    // explicit oversampled grid (Nifty's nx, ny): both even and at least the
+    // image; the oversampling factor of the kernel rule is the smaller ratio
+    const bool given = req.grid_x > 0 || req.grid_y > 0;
+    if (given) {
+        if (req.grid_x < nx || req.grid_y < ny || req.grid_x % 2 || req.grid_y % 2) return ERR_ARG;
+        sigma = std::min((double)req.grid_x / nx, (double)req.grid_y / ny);
+    }
     int st = setup_kernel(eps, sigma, gp.kp);
     if (st != OK) return st;
     if (kw_override > 0) gp.kp.kw = kw_override;   // tabulated window of another width
@@ -173,7 +180,19 @@ int grid_params(int nx, int ny, double psx, double psy, double wmin, double wmax
     gp.pixsize_x = psx;
     gp.pixsize_y = psy;
     gp.sign = sign;
+    gp.no_w = req.no_w;
     int N1 = ny, N2 = nx;
+    if (req.no_w) {
+        // w ignored (Nifty's do_wstacking = False): one plane, no n - 1 term,
+        // no w phase, no division by n
+        gp.nf3 = 1;
+        gp.gamma = 1.0;
+        gp.h = 0.0;
+        gp.nf1 = given ? req.grid_y : get_num_cells(N1, gp.kp);
+        gp.nf2 = given ? req.grid_x : get_num_cells(N2, gp.kp);
+        if (gp.nf1 < std::max(ny, 2 * gp.kp.kw) || gp.nf2 < std::max(nx, 2 * gp.kp.kw)) return ERR_ARG;
+        return OK;
+    }
     double l_min = 0 - 0.5 * psx * N2;
     double m_min = 0 - 0.5 * psy * N1;
     double arg = 1.0 - std::pow(l_min, 2) - std::pow(m_min, 2);
@@ -185,9 +204,9 @@ int grid_params(int nx, int ny, double psx, double psy, double wmin, double wmax
     gp.o_center = o_min / 2.0;
     gp.o_half = std::fabs(o_min / 2.0);
     set_nhg_type3(gp.o_half, gp.i_half, gp.kp, gp.nf3, gp.h, gp.gamma);
-    gp.nf1 = get_num_cells(N1, gp.kp);
-    gp.nf2 = get_num_cells(N2, gp.kp);
-    if (gp.nf1 < ny || gp.nf2 < nx) return ERR_ARG;
+    gp.nf1 = given ? req.grid_y : get_num_cells(N1, gp.kp);
+    gp.nf2 = given ? req.grid_x : get_num_cells(N2, gp.kp);
+    if (gp.nf1 < std::max(ny, 2 * gp.kp.kw) || gp.nf2 < std::max(nx, 2 * gp.kp.kw)) return ERR_ARG;
     return OK;
 }
 

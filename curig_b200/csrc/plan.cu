@@ -162,6 +162,8 @@ int plan_create(int type, int nx, int ny, double psx, double psy, double eps, do
         return ERR_ARG;
     if (opt.precision != 0 && opt.precision != 1) return ERR_ARG;
     if (opt.smode < 0 || opt.smode > 3) return ERR_ARG;
+    if (opt.w_term < 0 || opt.w_term > 1 || opt.grid_x < 0 || opt.grid_y < 0 || (opt.grid_x > 0) != (opt.grid_y > 0))
+        return ERR_ARG;
     if (!std::isfinite(psx) || !std::isfinite(psy) || !(psx > 0) || !(psy > 0)) return ERR_ARG;
     KernelParams kp;
     int st = setup_kernel(eps, sigma, kp);
@@ -239,8 +241,8 @@ static int choose_tiles(Plan *p, int esize, bool force_slabs) {
         return std::ceil(gz - 0.5 * kw);
     };
     double z0 = zstart(p->wmin_eff), z1 = zstart(p->wmax_eff);
-    bool nowrap = !force_slabs && z0 >= 0.0 && z1 <= gp.nf3 - kw && gp.nf3 <= 4000;
-    const int cand[] = {64, 48, 32, 24, 20, 16, 12, 10, 8, 6, 4, 2};
+    bool nowrap = gp.no_w || (!force_slabs && z0 >= 0.0 && z1 <= gp.nf3 - kw && gp.nf3 <= 4000);
+    const int cand[] = {96, 64, 48, 32, 24, 20, 16, 12, 10, 8, 6, 4, 2};
     double best = 1e30;
     int bb = 0, bz_best = 0;
     auto consider = [&](int b, int bz, int tz) {
@@ -332,8 +334,13 @@ int plan_setpts(Plan *p, long long nrow, int nchan, const double *du, const doub
         p->win = *lw;
         kw_override = lw->kw;
     }
-    int s = grid_params(p->nx, p->ny, p->psx, p->psy, lo, hi, p->eps, p->sigma, p->sign, p->gp, kw_override);
+    GridRequest req;
+    req.grid_x = p->opt.grid_x;
+    req.grid_y = p->opt.grid_y;
+    req.no_w = p->opt.w_term == 1;
+    int s = grid_params(p->nx, p->ny, p->psx, p->psy, lo, hi, p->eps, p->sigma, p->sign, p->gp, kw_override, req);
     if (s != OK) return s;
+    if (req.no_w && p->gp.kp.kw > TAB_KW) return ERR_UNSUPPORTED;   // thread-per-visibility kernels only
     p->win.kw = p->gp.kp.kw;
     bool force_slabs = false;
 retry_tiles:
@@ -360,6 +367,7 @@ retry_tiles:
     g.beta = gp.kp.beta; g.c = gp.kp.c;
     g.wkind = p->win.kind; g.wdeg = p->win.kind ? p->win.degree : 0;
     g.smode = tile_mode(p);
+    g.no_w = gp.no_w;
     // window table for the thread-per-visibility kernels: the learned window, or
     // in FP32 the ES window as degree-(TAB_DEG-1) Horner polynomials
     p->htab.clear();
@@ -385,7 +393,7 @@ retry_tiles:
                 for (int i = 0; i < TAB_DEG; ++i) v = v * x + p->htab[(size_t)d * TAB_DEG + i];
                 wm = std::max(wm, std::fabs(v));
             }
-        g.wmax3 = (float)(wm * wm * wm * 1.01);
+        g.wmax3 = (float)(std::max(wm * wm, wm * wm * wm) * 1.01);   // 2-D: two factors
     }
     g.nrow = nrow; g.nchan = nchan; g.uvw_stride = stride;
     g.psx = gp.pixsize_x; g.psy = gp.pixsize_y; g.i_center = gp.i_center; g.gamma = gp.gamma;
@@ -413,7 +421,7 @@ retry_tiles:
     DevCorr &cc = p->dc;
     cc.nx = p->nx; cc.ny = p->ny; cc.nf1 = gp.nf1; cc.nf2 = gp.nf2; cc.nf3 = gp.nf3;
     cc.psx = gp.pixsize_x; cc.psy = gp.pixsize_y; cc.o_center = gp.o_center; cc.i_center = gp.i_center;
-    cc.gamma = gp.gamma; cc.h = gp.h; cc.nquad = nq;
+    cc.gamma = gp.gamma; cc.h = gp.h; cc.nquad = nq; cc.no_w = gp.no_w;
     cc.qx = p->d_quad; cc.qg = p->d_quad + MAX_QUAD; cc.psi1 = p->d_psi1; cc.psi2 = p->d_psi2;
 
     // 4. binning: key per visibility (bin, start-cell residue), radix sort, bin bounds,

@@ -17,6 +17,8 @@ struct Options {
                               // 2 one-word int32 fixed point, 3 exact two-word int32 fixed point
     size_t smem_budget = 0;   // bytes of shared memory per CTA for tiles (0: default)
     cudaStream_t stream = nullptr;
+    int w_term = 0;           // 0: improved w-stacking, 1: w ignored (2-D gridding, no n - 1, n = 1)
+    int grid_x = 0, grid_y = 0;   // oversampled grid along the nxdirty / nydirty axes (0: sigma rule)
 };
 
 struct Plan {

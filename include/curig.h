@@ -68,6 +68,13 @@ typedef struct curig_opts {
                              epsilon >= 1e-5, else two-word), 1 float atomics, 2 one-word
                              int32 fixed point (22-bit terms, deterministic), 3 two-word
                              int32 fixed point (exact sums, deterministic) */
+    int w_term;           /* 0: improved w-stacking (default); 1: w ignored -- 2-D gridding
+                             without the n-1 term or the 1/n factor (the Nifty gridder's
+                             do_wstacking = False; no counterpart in the reference, whose
+                             w_term_method 0 is not functional, ra_exec.cu:124) */
+    int grid_x;           /* oversampled grid size along the nxdirty axis (the Nifty gridder's
+                             nx), even and >= nxdirty; 0 = sigma rule (cugridder.cu:180-181) */
+    int grid_y;           /* the same along the nydirty axis (Nifty's ny); both or neither */
     int reserved;
 } curig_opts;
 
