@@ -757,6 +757,27 @@ __device__ __forceinline__ void vis_store(const VisIO &io, int i, C<T> v) {
     static_cast<C<T> *>(io.vis)[j] = C<T>{(v.x * e.x + v.y * e.y) * wt, (v.y * e.x - v.x * e.y) * wt};
 }
 
+// The same scatter in two halves: the loads (index, phase, weight) issued
+// before the gather so that their latency overlaps the shared-memory work.
+template <typename T> struct VisDst {
+    int j;
+    C<T> e;
+    T wt;
+};
+template <typename T>
+__device__ __forceinline__ VisDst<T> vis_dst(const VisIO &io, int i) {
+    VisDst<T> d;
+    d.j = io.idx[i];
+    d.e = static_cast<const C<T> *>(io.ph)[i];
+    d.wt = io.wgt ? static_cast<const T *>(io.wgt)[d.j] : (T)1;
+    return d;
+}
+template <typename T>
+__device__ __forceinline__ void vis_put(const VisIO &io, const VisDst<T> &d, C<T> v) {
+    static_cast<C<T> *>(io.vis)[d.j] =
+        C<T>{(v.x * d.e.x + v.y * d.e.y) * d.wt, (v.y * d.e.x - v.x * d.e.y) * d.wt};
+}
+
 // Interpolator tile layout: [tz][ty][tpitch], column c holding grid x =
 // x_al + c with x_al = ox rounded down to even (so a TMA box may start there),
 // i.e. tile cell lx of the bin at column lx + (ox & 1).
@@ -883,6 +904,8 @@ k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
             const int i = start + m * stride;
             const int dz0 = part * KZ / S, dz1 = (part + 1) * KZ / S;
             R<T> r = rec[i];
+            VisDst<T> dst;
+            if (S == 1) dst = vis_dst<T>(io, i);
             T kx[KW], ky[KW];
 #pragma unroll
             for (int d = 0; d < KW; ++d) {
@@ -913,7 +936,7 @@ k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
                 ar = fma(sr, kz, ar);
                 ai = fma(si, kz, ai);
             }
-            if (S == 1) vis_store<T>(io, i, C<T>{ar, ai});
+            if (S == 1) vis_put<T>(io, dst, C<T>{ar, ai});
             else partial[u * 32 + lane] = C<T>{ar, ai};
         }
         if (S > 1) {                                   // L * S <= NWARPS: one pass
