@@ -33,6 +33,7 @@ static Options to_options(const curig_opts *o) {
         opt.w_term = o->w_term;
         opt.grid_x = o->grid_x;
         opt.grid_y = o->grid_y;
+        opt.bin_z = o->bin_z;
     }
     return opt;
 }

@@ -164,6 +164,7 @@ int plan_create(int type, int nx, int ny, double psx, double psy, double eps, do
     if (opt.smode < 0 || opt.smode > 3) return ERR_ARG;
     if (opt.w_term < 0 || opt.w_term > 1 || opt.grid_x < 0 || opt.grid_y < 0 || (opt.grid_x > 0) != (opt.grid_y > 0))
         return ERR_ARG;
+    if (opt.bin_z < 0) return ERR_ARG;
     if (!std::isfinite(psx) || !std::isfinite(psy) || !(psx > 0) || !(psy > 0)) return ERR_ARG;
     KernelParams kp;
     int st = setup_kernel(eps, sigma, kp);
@@ -253,9 +254,17 @@ static int choose_tiles(Plan *p, int esize, bool force_slabs) {
         double ratio = (double)q.tx * q.ty * tz / ((double)b * b * bz);
         if (ratio < best - 1e-9) { best = ratio; bb = b; bz_best = bz; }
     };
-    for (int b : cand) {
-        if (nowrap) consider(b, gp.nf3, gp.nf3);
-        for (int bz : {8, 4, 2}) if (bz < gp.nf3) consider(b, bz, bz + kw);
+    std::vector<int> edges(cand, cand + sizeof(cand) / sizeof(cand[0]));
+    if (p->opt.bin_xy > 0) edges.assign(1, p->opt.bin_xy);   // a requested edge, any size
+    if (p->opt.bin_z > 0 && !gp.no_w) {                 // requested slab depth
+        if (p->opt.bin_z >= gp.nf3) return ERR_ARG;
+        nowrap = false;
+        for (int b : edges) consider(b, p->opt.bin_z, p->opt.bin_z + kw);
+    } else {
+        for (int b : edges) {
+            if (nowrap) consider(b, gp.nf3, gp.nf3);
+            for (int bz : {8, 4, 2}) if (bz < gp.nf3) consider(b, bz, bz + kw);
+        }
     }
     if (!bb) return ERR_UNSUPPORTED;
     if (nowrap && bz_best == gp.nf3) {

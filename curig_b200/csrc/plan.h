@@ -19,6 +19,7 @@ struct Options {
     cudaStream_t stream = nullptr;
     int w_term = 0;           // 0: improved w-stacking, 1: w ignored (2-D gridding, no n - 1, n = 1)
     int grid_x = 0, grid_y = 0;   // oversampled grid along the nxdirty / nydirty axes (0: sigma rule)
+    int bin_z = 0;                // w-planes per tile slab (0: automatic)
 };
 
 struct Plan {

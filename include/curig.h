@@ -75,7 +75,8 @@ typedef struct curig_opts {
     int grid_x;           /* oversampled grid size along the nxdirty axis (the Nifty gridder's
                              nx), even and >= nxdirty; 0 = sigma rule (cugridder.cu:180-181) */
     int grid_y;           /* the same along the nydirty axis (Nifty's ny); both or neither */
-    int reserved;
+    int bin_z;            /* w-planes per tile slab (1 .. nf3 - 1), 0 = automatic (all planes in
+                             one tile unless a w support could wrap) */
 } curig_opts;
 
 void curig_default_opts(curig_opts *opts);
