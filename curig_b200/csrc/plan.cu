@@ -15,6 +15,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <thread>
 #include <tuple>
 
 namespace curig {
@@ -56,16 +57,20 @@ static int encode_grid_map(Plan *p);
 
 // ------------------------------------------------------------------ cuFFT plan cache
 // Rank-1 batched in-place plans keyed by (device, length, element stride,
-// batch distance, batch, precision): row transforms (stride 1) and column
-// transforms (stride nf1, adjacent columns adjacent in memory).
+// batch distance, batch, precision, stream, thread).  A cuFFT handle owns one
+// work area, so handles are shared only by plans whose transforms are ordered
+// on one stream: the stream is part of the key, and for the per-thread default
+// stream (one handle value naming each thread's own stream) so is the thread.
 namespace {
 std::mutex g_fft_mu;
-std::map<std::tuple<int, int, int, int, int, int>, cufftHandle> g_fft;
+std::map<std::tuple<int, int, int, int, int, int, uintptr_t, std::thread::id>, cufftHandle> g_fft;
 }
 
-static int fft_plan1(int dev, int n, int stride, int dist, int batch, int prec, cufftHandle &out) {
+static int fft_plan1(int dev, int n, int stride, int dist, int batch, int prec, cudaStream_t st,
+                     cufftHandle &out) {
     std::lock_guard<std::mutex> lk(g_fft_mu);
-    auto key = std::make_tuple(dev, n, stride, dist, batch, prec);
+    const std::thread::id tid = st == cudaStreamPerThread ? std::this_thread::get_id() : std::thread::id();
+    auto key = std::make_tuple(dev, n, stride, dist, batch, prec, (uintptr_t)st, tid);
     auto it = g_fft.find(key);
     if (it != g_fft.end()) { out = it->second; return OK; }
     cufftHandle h;
@@ -511,11 +516,11 @@ retry_tiles:
     p->fft_by = (int)std::max(1LL, std::min(nyrows, (1LL << 28) / gp.nf2));
     p->fft_by_rest = (int)(nyrows % p->fft_by);
     const int pr = p->opt.precision;
-    if (fft_plan1(p->device, gp.nf1, 1, gp.nf1, p->fft_bx, pr, p->fft_hx)) return ERR_CUFFT;
-    if (p->fft_bx_rest && fft_plan1(p->device, gp.nf1, 1, gp.nf1, p->fft_bx_rest, pr, p->fft_hx_rest))
+    if (fft_plan1(p->device, gp.nf1, 1, gp.nf1, p->fft_bx, pr, p->st, p->fft_hx)) return ERR_CUFFT;
+    if (p->fft_bx_rest && fft_plan1(p->device, gp.nf1, 1, gp.nf1, p->fft_bx_rest, pr, p->st, p->fft_hx_rest))
         return ERR_CUFFT;
-    if (fft_plan1(p->device, gp.nf2, 1, gp.nf2, p->fft_by, pr, p->fft_hy)) return ERR_CUFFT;
-    if (p->fft_by_rest && fft_plan1(p->device, gp.nf2, 1, gp.nf2, p->fft_by_rest, pr, p->fft_hy_rest))
+    if (fft_plan1(p->device, gp.nf2, 1, gp.nf2, p->fft_by, pr, p->st, p->fft_hy)) return ERR_CUFFT;
+    if (p->fft_by_rest && fft_plan1(p->device, gp.nf2, 1, gp.nf2, p->fft_by_rest, pr, p->st, p->fft_hy_rest))
         return ERR_CUFFT;
     mark(p, EV_SET_END);
     p->ready = true;
@@ -524,16 +529,14 @@ retry_tiles:
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda).
 static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    static bool tried = false;
-    if (!tried) {
-        tried = true;
-        void *f = nullptr;
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = []() -> PFN_cuTensorMapEncodeTiled_v12000 {
+        void *f = nullptr;                            // initialised once, thread-safe
         cudaDriverEntryPointQueryResult q;
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
-    }
+            return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+        return nullptr;
+    }();
     return fn;
 }
 
