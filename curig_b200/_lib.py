@@ -106,6 +106,15 @@ lib.curig_window_loss_grad_static.argtypes = [c_int, c_double, _P, _P, _P]
 lib.curig_window_loss_grad_static.restype = c_int
 lib.curig_window_table.restype = c_int
 lib.curig_default_opts.argtypes = [ctypes.POINTER(CurigOpts)]
+lib.curig_nufft_makeplan.argtypes = [c_int, c_int, c_int, c_int, c_double, c_int, c_double,
+                                     ctypes.POINTER(CurigOpts), ctypes.POINTER(c_void_p)]
+lib.curig_nufft_makeplan.restype = c_int
+lib.curig_nufft_setpts.argtypes = [c_void_p, c_int64, _P, _P]
+lib.curig_nufft_setpts.restype = c_int
+lib.curig_nufft_execute.argtypes = [c_void_p, _P, _P]
+lib.curig_nufft_execute.restype = c_int
+lib.curig_nufft_destroy.argtypes = [c_void_p]
+lib.curig_nufft_destroy.restype = c_int
 lib.curig_default_opts.restype = None
 
 ERRORS = {

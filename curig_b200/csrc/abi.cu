@@ -183,6 +183,74 @@ extern "C" int curig_makeplan(int type, int nx, int ny, double psx, double psy, 
     return OK;
 }
 
+// ------------------------------------------------------------------ generic NUFFT
+// Type 1 (points -> modes) and type 2 (modes -> points) in one or two
+// dimensions on the w-free gridder: a point (x, y) becomes the row
+// (s x / 2pi, s y / 2pi, 0) at frequency c with unit pixel sizes, so the
+// gridder's phases e^{+-i 2pi (l u + m v)} are e^{+-i (k1 x + k2 y)}; s = +iflag
+// for type 1 (ms2dirty's sign) and -iflag for type 2 (dirty2ms's).  Modes are
+// [n1][n2] with mode k = index - n/2, as the dirty image.  Plays the part of
+// the reference's cunufft_setting / cunufft exec path (cuft.cu:249) for types
+// 1 and 2 with the same kernel-width, grid-size and correction rules.
+struct curig_nufft_s {
+    Plan *p = nullptr;
+    int type = 1, dim = 1, n1 = 0, n2 = 1, iflag = 1;
+    double *d_uvw = nullptr;
+};
+
+extern "C" int curig_nufft_makeplan(int type, int dim, int n1, int n2, double eps, int iflag, double sigma,
+                                    const curig_opts *opts, curig_nufft *out) {
+    if (!out) return fail(ERR_ARG, "null plan pointer");
+    *out = nullptr;
+    if ((type != 1 && type != 2) || (dim != 1 && dim != 2) || n1 <= 0 || (dim == 2 && n2 <= 0) ||
+        (iflag != 1 && iflag != -1))
+        return fail(ERR_ARG, "invalid NUFFT plan arguments");
+    Options o = to_options(opts);
+    o.w_term = 1;
+    Plan *p = nullptr;
+    const int ny = dim == 2 ? n2 : 1;
+    int s = plan_create(type, n1, ny, 1.0, 1.0, eps, sigma, 1, o, &p);
+    if (s != OK) return fail(s, "NUFFT plan creation failed");
+    *out = new curig_nufft_s;
+    (*out)->p = p;
+    (*out)->type = type;
+    (*out)->dim = dim;
+    (*out)->n1 = n1;
+    (*out)->n2 = ny;
+    (*out)->iflag = iflag;
+    return OK;
+}
+
+extern "C" int curig_nufft_setpts(curig_nufft h, int64_t m, const double *d_x, const double *d_y) {
+    if (!h || !d_x || m <= 0 || (h->dim == 2 && !d_y)) return fail(ERR_ARG, "invalid NUFFT points");
+    Plan *p = h->p;
+    if (h->d_uvw) cudaFreeAsync(h->d_uvw, p->st);
+    h->d_uvw = nullptr;
+    if (cudaMallocAsync((void **)&h->d_uvw, 3 * m * sizeof(double), p->st) != cudaSuccess)
+        return fail(ERR_NOMEM, "out of device memory");
+    const double sgn = h->type == 1 ? (double)h->iflag : -(double)h->iflag;
+    launch_nupts_uvw(m, d_x, h->dim == 2 ? d_y : nullptr, sgn, h->d_uvw, p->st);
+    const double freq = SPEEDOFLIGHT;                   // f / c = 1
+    int s = plan_setpts(p, m, 1, h->d_uvw, h->d_uvw + 1, h->d_uvw + 2, 3, &freq);
+    if (s != OK) return fail(s, p->last_error.empty() ? "NUFFT setpts failed" : p->last_error);
+    return OK;
+}
+
+extern "C" int curig_nufft_execute(curig_nufft h, void *d_c, void *d_fk) {
+    if (!h || !d_c || !d_fk) return fail(ERR_ARG, "invalid NUFFT execute arguments");
+    int s = plan_execute(h->p, d_c, nullptr, d_fk, h->type);
+    if (s != OK) return fail(s, h->p->last_error.empty() ? "NUFFT execute failed" : h->p->last_error);
+    return OK;
+}
+
+extern "C" int curig_nufft_destroy(curig_nufft h) {
+    if (!h) return OK;
+    if (h->d_uvw) cudaFreeAsync(h->d_uvw, h->p->st);
+    plan_destroy(h->p);
+    delete h;
+    return OK;
+}
+
 extern "C" int curig_setpts_uvw(curig_plan h, int64_t nrow, int nchan, const double *du, const double *dv,
                                 const double *dw, int stride, const double *freq) {
     if (!h) return fail(ERR_ARG, "null plan");

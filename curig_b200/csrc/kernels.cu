@@ -1397,6 +1397,23 @@ void launch_t_to_grid(int ny, int nf1, int nf2, int nf3, const void *t, void *gr
                                               reinterpret_cast<C<T> *>(grid));
 }
 
+// Nonuniform points of the generic NUFFT as gridder rows: (s x / 2pi, s y / 2pi, 0)
+// (with unit pixels and frequency c the gridder's phase is then +-k.x).
+__global__ void k_nupts_uvw(long long m, const double *__restrict__ x, const double *__restrict__ y, double s,
+                            double *__restrict__ uvw) {
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < m;
+         j += (long long)gridDim.x * blockDim.x) {
+        uvw[3 * j] = s * x[j] * INV_2PI;
+        uvw[3 * j + 1] = y ? s * y[j] * INV_2PI : 0.0;
+        uvw[3 * j + 2] = 0.0;
+    }
+}
+
+void launch_nupts_uvw(long long m, const double *x, const double *y, double s, double *uvw, cudaStream_t st) {
+    count_launch();
+    k_nupts_uvw<<<grid_for(m), NTHREADS, 0, st>>>(m, x, y, s, uvw);
+}
+
 void launch_psi_grid(int n, int nq, const double *qx, const double *qg, double *out, cudaStream_t st) {
     count_launch();
     k_psi_grid<<<grid_for(n, 128), 128, 0, st>>>(n, nq, qx, qg, out);

@@ -142,6 +142,7 @@ void launch_t_to_grid(int ny, int nf1, int nf2, int nf3, const void *t, void *gr
 template <typename T>
 void launch_zero_tpad(int nx, int ny, int nf2, int nf3, void *t, cudaStream_t st);
 void launch_psi_grid(int n, int nq, const double *qx, const double *qg, double *out, cudaStream_t st);
+void launch_nupts_uvw(long long m, const double *x, const double *y, double s, double *uvw, cudaStream_t st);
 
 int plan_device_status(Plan *p);
 

@@ -189,6 +189,22 @@ void curig_set_timing(int on);
 int curig_plan_timings(curig_plan plan, double *out, int n);
 int64_t curig_launch_count(void);
 
+/* Generic NUFFT, types 1 (points -> modes) and 2 (modes -> points) in one or two
+ * dimensions, on the w-free gridder (same kernel-width, grid-size and correction
+ * rules as the gridder; takes the place of the reference's cunufft_setting /
+ * exec path for these types, src/fourier/cuft.cu:249).  Points x (and y for
+ * dim 2) are device float64 arrays of m coordinates in radians (periodic,
+ * any range); strengths c are device complex [m] (complex64 when
+ * opts->precision = 1); modes fk are device complex [n1][n2] (dim 1: [n1]), mode
+ * k = index - n/2.  Type 1: fk[k] = sum_j c_j e^{i iflag k.x_j}; type 2: c_j =
+ * sum_k fk[k] e^{i iflag k.x_j}.  sigma: upsampling factor (2 = reference rule). */
+typedef struct curig_nufft_s *curig_nufft;
+int curig_nufft_makeplan(int type, int dim, int n1, int n2, double epsilon, int iflag, double sigma,
+                         const curig_opts *opts, curig_nufft *plan);
+int curig_nufft_setpts(curig_nufft plan, int64_t m, const double *d_x, const double *d_y);
+int curig_nufft_execute(curig_nufft plan, void *d_c, void *d_fk);
+int curig_nufft_destroy(curig_nufft plan);
+
 /* Last error text of this thread (static storage, empty if none). */
 const char *curig_last_error(void);
 

@@ -1,0 +1,68 @@
+"""Generic NUFFT (types 1 and 2, one and two dimensions) against the direct
+nonuniform DFT (numpy, FP64), with points inside and beyond [-pi, pi)."""
+import numpy as np
+import pytest
+
+
+def _direct(x, y, n_modes, iflag):
+    """Matrix E[j, k] = exp(i iflag k.x_j) over the modes k = index - n/2."""
+    k1 = np.arange(n_modes[0]) - n_modes[0] // 2
+    ph = np.outer(x, k1)
+    if len(n_modes) == 2:
+        k2 = np.arange(n_modes[1]) - n_modes[1] // 2
+        ph = ph[:, :, None] + np.outer(y, k2)[:, None, :]
+    return np.exp(1j * iflag * ph).reshape(len(x), -1)
+
+
+def test_nufft_symbols_exported():
+    from curig_b200 import _lib
+    for name in ("curig_nufft_makeplan", "curig_nufft_setpts", "curig_nufft_execute", "curig_nufft_destroy"):
+        assert hasattr(_lib.lib, name)
+
+
+CASES = [((64,), 1), ((64,), -1), ((40, 36), 1), ((40, 36), -1), ((33, 17), 1)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n_modes,iflag", CASES)
+@pytest.mark.parametrize("precision,eps,tol", [("fp64", 1e-10, 1e-9), ("fp32", 1e-5, 3e-5)])
+def test_nufft_types_1_and_2_match_direct(n_modes, iflag, precision, eps, tol):
+    import torch
+    from curig_b200.nufft import Nufft
+    rng = np.random.default_rng(sum(n_modes) + iflag)
+    m = 700
+    x = rng.uniform(-np.pi, np.pi, m)
+    x[:50] *= 2.5                                   # periodic beyond [-pi, pi)
+    y = rng.uniform(-np.pi, np.pi, m)
+    c = rng.standard_normal(m) + 1j * rng.standard_normal(m)
+    fk = rng.standard_normal(n_modes) + 1j * rng.standard_normal(n_modes)
+    E = _direct(x, y, n_modes, iflag)
+    cdt = torch.complex128 if precision == "fp64" else torch.complex64
+    dx = torch.from_numpy(x).cuda()
+    dy = torch.from_numpy(y).cuda() if len(n_modes) == 2 else None
+    p1 = Nufft(1, n_modes, eps, iflag, precision=precision)
+    p1.setpts(dx, dy)
+    out = torch.empty(n_modes, dtype=cdt, device="cuda")
+    p1.execute(torch.from_numpy(c).to(cdt).cuda(), out)
+    ref1 = (c @ E).reshape(n_modes)
+    got1 = out.cpu().numpy()
+    assert np.linalg.norm(got1 - ref1) <= tol * np.linalg.norm(ref1)
+    p2 = Nufft(2, n_modes, eps, iflag, precision=precision)
+    p2.setpts(dx, dy)
+    cout = torch.empty(m, dtype=cdt, device="cuda")
+    p2.execute(cout, torch.from_numpy(fk).to(cdt).cuda())
+    ref2 = E @ fk.reshape(-1)
+    got2 = cout.cpu().numpy()
+    assert np.linalg.norm(got2 - ref2) <= tol * np.linalg.norm(ref2)
+    p1.close()
+    p2.close()
+
+
+@pytest.mark.gpu
+def test_nufft_rejects_bad_arguments():
+    from curig_b200._lib import CurigError
+    from curig_b200.nufft import Nufft
+    with pytest.raises(CurigError):
+        Nufft(3, (16,), 1e-6)
+    with pytest.raises(CurigError):
+        Nufft(1, (16, 16), 1e-6, iflag=2)
