@@ -28,9 +28,11 @@ template <typename T> using R = typename rec_t<T>::type;
 constexpr int NTHREADS = 256;
 constexpr int NWARPS = NTHREADS / 32;
 // k_spread_t: 16 warps per CTA, two CTAs per SM at the shared-memory budget of
-// one fixed-point tile
+// one fixed-point tile.  k_interp_t: 8 warps per CTA, two CTAs per SM.
 constexpr int TTHREADS = 512;
 constexpr int TWARPS = TTHREADS / 32;
+// (384-thread FP32 interpolator CTAs measured slower: 18.4 against 17.8 ms)
+template <typename T> constexpr int interp_threads() { return 256; }
 constexpr int KSTR = 32;                 // per-axis stride of the per-warp kernel-value scratch
 constexpr double TWO_PI = 2.0 * PI_D;
 
@@ -785,7 +787,7 @@ __device__ __forceinline__ void vis_put(const VisIO &io, const VisDst<T> &d, C<T
 // Stage the tile (wrapped rows of all its planes) with plain loads: rows are
 // walked without divisions and eight rows are in flight per warp before the
 // shared stores.
-template <typename T>
+template <typename T, int NW>
 __device__ __forceinline__ void load_tile(const DevGeom &g, const C<T> *__restrict__ grid, C<T> *tile, int x_al,
                                           int oy, int oz, int warp, int lane) {
     const int nrows = g.ty * g.tz, W = g.tpitch;
@@ -806,8 +808,8 @@ __device__ __forceinline__ void load_tile(const DevGeom &g, const C<T> *__restri
                     int gz = g.zpad ? wrap3(oz + z, g.nf3) : z;
                     v[k] = grid[((long long)gz * g.nf2 + gy) * g.nf1 + gx];
                 }
-                row += NWARPS;
-                y += NWARPS;
+                row += NW;
+                y += NW;
                 while (y >= g.ty) { y -= g.ty; ++z; }
             }
 #pragma unroll
@@ -845,12 +847,13 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
 constexpr long long TMA_WAIT_LIMIT = 1LL << 26;   // try_wait polls (seconds): then the error flag
 
 template <typename T, int KW>
-__global__ void __launch_bounds__(NTHREADS, sizeof(T) == 4 ? 3 : 2)
+__global__ void __launch_bounds__(interp_threads<T>(), 2)
 k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__ bin_count,
            const int *__restrict__ sub_end, const R<T> *__restrict__ rec, const C<T> *__restrict__ grid,
            const WinTab<T> tab, const VisIO io, const __grid_constant__ CUtensorMap tmap, int *err) {
+    constexpr int IT = interp_threads<T>(), IW = IT / 32;
     extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ C<T> partial[NTHREADS];      // per (column, part, lane) sums of split visibilities
+    __shared__ C<T> partial[IT];      // per (column, part, lane) sums of split visibilities
     __shared__ unsigned long long bar;      // TMA completion barrier
     C<T> *tile = reinterpret_cast<C<T> *>(smem);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -890,14 +893,14 @@ k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
                 return;
             }
         } else {
-            load_tile<T>(g, grid, tile, x_al, oy, oz, warp, lane);
+            load_tile<T, IW>(g, grid, tile, x_al, oy, oz, warp, lane);
             __syncthreads();
         }
         // same lane / position map and w-plane split as k_spread_t
         const int L = (n + 31) >> 5;
         const int KZ = g.no_w ? 1 : KW;
-        const int S = max(1, min(KZ, NWARPS / max(L, 1)));
-        for (int u = warp; u < L * S; u += NWARPS) {
+        const int S = max(1, min(KZ, IW / max(L, 1)));
+        for (int u = warp; u < L * S; u += IW) {
             const int k = u / S, part = u - k * S;
             const int m = lane * L + k;
             if (m >= n) continue;
@@ -939,9 +942,9 @@ k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
             if (S == 1) vis_put<T>(io, dst, C<T>{ar, ai});
             else partial[u * 32 + lane] = C<T>{ar, ai};
         }
-        if (S > 1) {                                   // L * S <= NWARPS: one pass
+        if (S > 1) {                                   // L * S <= IW: one pass
             __syncthreads();
-            for (int m = threadIdx.x; m < n; m += NTHREADS) {
+            for (int m = threadIdx.x; m < n; m += IT) {
                 const int ln = m / L, k = m - ln * L;
                 C<T> v = partial[(k * S) * 32 + ln];
                 for (int p = 1; p < S; ++p) {
@@ -1319,9 +1322,9 @@ static int launch_interp_kw(const DevGeom &g, size_t smem, const int *bs, const 
     int blocks = 0, s;
     if constexpr (KW > 0) {
         auto kern = k_interp_t<T, KW>;
-        if ((s = launch_persistent(kern, smem, nsm, blocks))) return s;
+        if ((s = launch_persistent(kern, smem, nsm, blocks, interp_threads<T>()))) return s;
         count_launch();
-        kern<<<blocks, NTHREADS, smem, st>>>(g, bs, bc, se, reinterpret_cast<const R<T> *>(rec),
+        kern<<<blocks, interp_threads<T>(), smem, st>>>(g, bs, bc, se, reinterpret_cast<const R<T> *>(rec),
                                              reinterpret_cast<const C<T> *>(grid), make_tab<T>(g, ht), io,
                                              *tmap, err);
     } else {
