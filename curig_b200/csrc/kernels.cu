@@ -847,7 +847,7 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
 constexpr long long TMA_WAIT_LIMIT = 1LL << 26;   // try_wait polls (seconds): then the error flag
 
 template <typename T, int KW>
-__global__ void __launch_bounds__(interp_threads<T>(), 2)
+__global__ void __launch_bounds__(interp_threads<T>(), sizeof(T) == 4 ? 3 : 2)
 k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__ bin_count,
            const int *__restrict__ sub_end, const R<T> *__restrict__ rec, const C<T> *__restrict__ grid,
            const WinTab<T> tab, const VisIO io, const __grid_constant__ CUtensorMap tmap, int *err) {
