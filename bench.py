@@ -513,16 +513,23 @@ def main():
             e2e_step()
         ke = max(1, min(a.steps, 3))
         torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
         ev0.record(stream)
         for _ in range(ke):
             e2e_step()
         ev1.record(stream)
         torch.cuda.synchronize()
         ems = ev0.elapsed_time(ev1) / ke
+        if world > 1:                                    # whole job: slowest rank
+            t = torch.tensor([ems], device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ems = float(t.item())
         bi = 2 * h_uvw.numel() * 8 + h_vis.numel() * h_vis.element_size() + \
             2 * h_wgt.numel() * h_wgt.element_size() + h_dirty.numel() * h_dirty.element_size()
         bo = h_dirty.numel() * h_dirty.element_size() + h_vout.numel() * h_vout.element_size()
-        e2e = {"value": M / (ems / 1e3), "unit": "vis/s", "h2d_bytes_per_step": int(bi),
+        e2e = {"value": M * world / (ems / 1e3), "unit": "vis/s", "h2d_bytes_per_step": int(bi),
                "d2h_bytes_per_step": int(bo), "ms_per_step": round(ems, 3), "steps": ke,
                "api": "curig_ms2dirty + curig_dirty2ms (C ABI, pinned host buffers)"}
 

@@ -457,19 +457,9 @@ k_interp(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__ b
 // ------------------------------------------------------------------ thread-per-visibility
 // Same sub-problem / tile structure, one thread per visibility: the kernel
 // values along x and y live in registers (compile-time width), the taps are
-// fully unrolled with immediate offsets, the w-axis value is evaluated per
-// plane, and shared-memory accumulation uses the native reduction
-// (red.shared.add).  Visibilities are sorted by start cell inside a bin, so
-// the 32 lanes of a warp update / read neighbouring cells.
-
-__device__ __forceinline__ void red_shared(float *p, float v) {
-    unsigned a = (unsigned)__cvta_generic_to_shared(p);
-    asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
-}
-__device__ __forceinline__ void red_shared(double *p, double v) {
-    unsigned a = (unsigned)__cvta_generic_to_shared(p);
-    asm volatile("red.shared.add.f64 [%0], %1;" ::"r"(a), "d"(v) : "memory");
-}
+// unrolled along x and y with immediate offsets and the w-axis value is
+// evaluated per plane.  Visibilities are sorted by the bank residue of their
+// start cell inside a bin, so the 32 lanes of a warp touch distinct banks.
 
 // Window value for tap d: ES (direct) or the Horner table in parameter space.
 template <typename T>
