@@ -37,10 +37,33 @@ class GridderOperator:
         self.cdt = torch.complex64 if precision == "fp32" else torch.complex128
         self.rdt = torch.float32 if precision == "fp32" else torch.float64
         self.device = uvw.device
+        # the plan's stream: given, or the caller's current stream
+        self.stream = stream if stream is not None else torch.cuda.current_stream(uvw.device)
         self.plan = GridderPlan(1, nxdirty, nydirty, pixsize_x, pixsize_y, epsilon, sigma, sign,
-                                precision=precision, window=window, stream=stream, accumulate=accumulate)
-        self.plan.setpts(uvw, np.atleast_1d(np.asarray(freq, dtype=np.float64)))
+                                precision=precision, window=window, stream=self.stream, accumulate=accumulate)
+        with self._ordered():
+            self.plan.setpts(uvw, np.atleast_1d(np.asarray(freq, dtype=np.float64)))
         self.nrow, self.nchan = self.plan.nrow, self.plan.nchan
+
+    class _Order:
+        """Orders the plan's stream after the caller's current stream on entry
+        and the caller's after the plan's on exit (no-op when they are one)."""
+
+        def __init__(self, op):
+            self.op = op
+
+        def __enter__(self):
+            self.cur = torch.cuda.current_stream(self.op.device)
+            if self.cur != self.op.stream:
+                self.op.stream.wait_stream(self.cur)
+
+        def __exit__(self, *exc):
+            if self.cur != self.op.stream:
+                self.cur.wait_stream(self.op.stream)
+            return False
+
+    def _ordered(self):
+        return GridderOperator._Order(self)
 
     # raw products (no autograd) --------------------------------------------------
     def _check(self, t, dtype, shape, what):
@@ -55,7 +78,8 @@ class GridderOperator:
         if wgt is not None:
             wgt = self._check(wgt, self.rdt, (self.nrow, self.nchan), "wgt")
         out = torch.empty((self.nx, self.ny), dtype=self.cdt, device=self.device)
-        self.plan.execute_dir(1, vis, wgt, out)
+        with self._ordered():
+            self.plan.execute_dir(1, vis, wgt, out)
         return out
 
     def adjoint(self, dirty, wgt=None):
@@ -64,7 +88,8 @@ class GridderOperator:
         if wgt is not None:
             wgt = self._check(wgt, self.rdt, (self.nrow, self.nchan), "wgt")
         out = torch.empty((self.nrow, self.nchan), dtype=self.cdt, device=self.device)
-        self.plan.execute_dir(2, out, wgt, dirty)
+        with self._ordered():
+            self.plan.execute_dir(2, out, wgt, dirty)
         return out
 
     # differentiable products -----------------------------------------------------
@@ -125,22 +150,123 @@ class _Dirty2MS(torch.autograd.Function):
 
 
 class BatchGridder:
-    """Independent problems, one plan each (own points, same image geometry),
-    executed one after another on the current stream.  Inputs are stacked:
-    vis / wgt [B, nrow, nchan], dirty [B, nx, ny]; problems share nrow, nchan."""
+    """Independent problems, one plan each (own points, same image geometry).
+    Inputs are stacked: vis / wgt [B, nrow, nchan], dirty [B, nx, ny]; problems
+    share nrow and nchan.  Each problem runs on its own CUDA stream, launched
+    one after another and joined to the caller's stream at the end (forward and
+    backward), so the small transforms of the batch overlap on the GPU."""
 
     def __init__(self, uvws, freq, nxdirty, nydirty, pixsize_x, pixsize_y, epsilon, **kw):
-        self.ops = [GridderOperator(u, freq, nxdirty, nydirty, pixsize_x, pixsize_y, epsilon, **kw) for u in uvws]
+        cur = torch.cuda.current_stream()
+        self.streams = [torch.cuda.Stream() for _ in uvws]
+        self.ops = []
+        for u, st in zip(uvws, self.streams):
+            st.wait_stream(cur)                          # uvw written on the caller's stream
+            with torch.cuda.stream(st):
+                self.ops.append(GridderOperator(u, freq, nxdirty, nydirty, pixsize_x, pixsize_y, epsilon,
+                                                stream=st, **kw))
+        for st in self.streams:
+            cur.wait_stream(st)
 
     def __len__(self):
         return len(self.ops)
 
     def ms2dirty(self, vis, wgt=None):
-        return torch.stack([op.ms2dirty(vis[b], None if wgt is None else wgt[b]) for b, op in enumerate(self.ops)])
+        return _BatchMS2Dirty.apply(vis, wgt, self)
 
     def dirty2ms(self, dirty, wgt=None):
-        return torch.stack([op.dirty2ms(dirty[b], None if wgt is None else wgt[b]) for b, op in enumerate(self.ops)])
+        return _BatchDirty2MS.apply(dirty, wgt, self)
+
+    def _each(self, fn):
+        """fn(b, op) for every problem on its stream; then join to the caller's stream."""
+        cur = torch.cuda.current_stream()
+        for b, (op, st) in enumerate(zip(self.ops, self.streams)):
+            st.wait_stream(cur)
+            with torch.cuda.stream(st):
+                fn(b, op)
+        for st in self.streams:
+            cur.wait_stream(st)
 
     def close(self):
         for op in self.ops:
             op.close()
+
+
+class _BatchMS2Dirty(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, vis, wgt, bg):
+        ctx.bg = bg
+        ctx.save_for_backward(vis, wgt)
+        op0 = bg.ops[0]
+        out = torch.empty((len(bg), op0.nx, op0.ny), dtype=op0.cdt, device=vis.device)
+        vis_d = vis.detach()
+        wgt_d = None if wgt is None else wgt.detach()
+
+        def run(b, op):
+            op.plan.execute_dir(1, op._check(vis_d[b], op.cdt, (op.nrow, op.nchan), "vis"),
+                                None if wgt_d is None else op._check(wgt_d[b], op.rdt, (op.nrow, op.nchan), "wgt"),
+                                out[b])
+        bg._each(run)
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        vis, wgt = ctx.saved_tensors
+        bg = ctx.bg
+        g = g.contiguous()
+        need_v, need_w = ctx.needs_input_grad[0], ctx.needs_input_grad[1] and wgt is not None
+        gv = torch.empty_like(vis) if need_v else None
+        gw = torch.empty_like(wgt) if need_w else None
+        vis_d = vis.detach()
+        wgt_d = None if wgt is None else wgt.detach()
+
+        def run(b, op):
+            if need_w:
+                t = op.adjoint(g[b], None)                    # A^H g
+                gw[b].copy_((vis_d[b].conj() * t).real)
+                if need_v:
+                    gv[b].copy_(t * wgt_d[b])
+            elif need_v:
+                gv[b].copy_(op.adjoint(g[b], None if wgt_d is None else wgt_d[b]))
+        bg._each(run)
+        return gv, gw, None
+
+
+class _BatchDirty2MS(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, dirty, wgt, bg):
+        ctx.bg = bg
+        op0 = bg.ops[0]
+        keep_t = wgt is not None and wgt.requires_grad
+        out = torch.empty((len(bg), op0.nrow, op0.nchan), dtype=op0.cdt, device=dirty.device)
+        ts = torch.empty_like(out) if keep_t else None
+        dirty_d = dirty.detach()
+        wgt_d = None if wgt is None else wgt.detach()
+
+        def run(b, op):
+            if keep_t:
+                t = op.adjoint(dirty_d[b], None)              # A^H dirty
+                ts[b].copy_(t)
+                out[b].copy_(t * wgt_d[b])
+            else:
+                out[b].copy_(op.adjoint(dirty_d[b], None if wgt_d is None else wgt_d[b]))
+        bg._each(run)
+        ctx.save_for_backward(wgt, ts)
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        wgt, ts = ctx.saved_tensors
+        bg = ctx.bg
+        g = g.contiguous()
+        need_d, need_w = ctx.needs_input_grad[0], ctx.needs_input_grad[1] and wgt is not None
+        op0 = bg.ops[0]
+        gd = torch.empty((len(bg), op0.nx, op0.ny), dtype=op0.cdt, device=g.device) if need_d else None
+        gw = (g * ts.conj()).real.to(wgt.dtype) if need_w else None
+        wgt_d = None if wgt is None else wgt.detach()
+
+        def run(b, op):
+            op.plan.execute_dir(1, g[b], None if wgt_d is None else wgt_d[b], gd[b])
+        if need_d:
+            bg._each(run)
+        return gd, gw, None
