@@ -484,6 +484,18 @@ def main():
     roof = {"bound": "hbm", "kernel": f"k_{dom}_t", "achieved": round(achieved, 1), "peak": peak,
             "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
             "traffic": traffic, "algorithmic_bytes": alg[dom], "kernel_ms": round(st[dom], 3)}
+    # The spreader's binding limit is shared-memory integer atomics (FP32 tiles: two
+    # per tap, one per component); measured on this part: 27.6 int32 atomics per
+    # clock per SM without bank conflicts.  Taps per second against that peak at
+    # the SM clock sampled during the timed region.
+    clk_mhz = (head["clocks"] or {}).get("sm_mhz")
+    if a.precision == "fp32" and clk_mhz:
+        taps = M * info["kw"] ** 3 / (st["spread"] / 1e3)
+        tap_peak = 27.6 / 2 * torch.cuda.get_device_properties(dev).multi_processor_count * clk_mhz * 1e6
+        roof["shared_atomic_bound"] = {"kernel": "k_spread_t", "achieved_taps_per_s": taps,
+                                       "peak_taps_per_s": tap_peak, "frac": round(taps / tap_peak, 4),
+                                       "peak_basis": "27.6 int32 shared atomics / clock / SM (measured), "
+                                                     "2 per tap, sampled SM clock"}
 
     # e2e through the C ABI with pinned host buffers
     e2e = None
