@@ -56,7 +56,7 @@ def args_():
     ap.add_argument("--no-arms", action="store_true", help="skip the ES comparison arms")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--accumulate", type=int, default=0, help="FP32 tile accumulation: 0 automatic, 1 float atomics, 2 one-word int32 fixed point, 3 two-word (exact)")
+    ap.add_argument("--accumulate", type=int, default=0, help="tile accumulation: 0 automatic, 1 float atomics, 2 one-word int32 fixed point, 3 two-word (exact); FP64: 1 double atomics, else exact int64 + int32")
     ap.add_argument("--bin", type=int, default=0, help="bin edge in cells (0 automatic)")
     ap.add_argument("--smem", type=int, default=0, help="shared-memory budget per tile CTA (bytes)")
     ap.add_argument("--sub", type=int, default=0, help="visibilities per tile chunk (0 automatic)")
@@ -561,7 +561,8 @@ def main():
                                    f"({a.nrow * a.nchan} vis), {a.npix}^2, fov {a.fov} deg, "
                                    f"eps {a.eps}, sigma 2", "window": window,
                        "precision": a.precision, "kw": info["kw"], "nf": [info["nf1"], info["nf2"], info["nf3"]],
-                       "bin_xy": info["bin_xy"], "accumulate": ({1: "float atomics", 2: "one-word int32 fixed point", 3: "two-word int32 fixed point (exact)"}[acc_mode] if a.precision == "fp32" else "float atomics"),
+                       "bin_xy": info["bin_xy"], "accumulate": ({1: "float atomics", 2: "one-word int32 fixed point", 3: "two-word int32 fixed point (exact)"}[acc_mode] if a.precision == "fp32" else
+                                      "double atomics" if acc_mode == 1 else "int64 + int32 fixed point (exact)"),
                        "l2": "inputs (>= 1.9 GB per step) larger than L2; no flush needed",
                        "parallelism": f"dp{world} (visibility shards, all-reduce of dirty)" if world > 1 else "single GPU"},
             "e2e": e2e, "gpu_launches": int(head["launches"]), "clocks": head["clocks"],

@@ -521,6 +521,23 @@ __device__ __forceinline__ int round_fix(float a, float k) {
     return __float_as_int(fmaf(a, k, 12582912.0f)) - 0x4B400000;
 }
 
+// FP64 tiles (shared-memory double atomics are compare-and-swap loops): each
+// scaled term x is split exactly as h * 2^18 + l, h rounded to an integer by
+// one FMA against 1.5 * 2^52, l = x - h 2^18 (exact) rounded to an integer
+// (|l| <= 2^17); h goes to an int64 plane (two's complement in the unsigned
+// add), l to an int32 plane.  The chunk scale q = 2^k takes the largest k with
+// max|c| wmax3 q <= 2^68, so |h| <= 2^50 and, with at most 4096 terms per cell
+// (sub <= 4096), the high sums stay below 2^62 and the low sums below 2^29:
+// cell sums are exact and order-independent, and a term's rounding is at most
+// 2^-68 of max|c| wmax3, below the FP64 rounding of the product itself.
+__device__ __forceinline__ void split_fix64(double x, unsigned long long &h, int &l) {
+    const double M = 6755399441055744.0;                  // 1.5 * 2^52
+    const double t = fma(x, 3.814697265625e-06, M);       // x * 2^-18, rounded to an integer
+    h = (unsigned long long)(__double_as_longlong(t) - 0x4338000000000000LL);
+    const double lf = fma(t - M, -262144.0, x);           // x - h * 2^18, exact
+    l = (int)(__double_as_longlong(lf + M) - 0x4338000000000000LL);
+}
+
 template <typename T, int KW>
 __global__ void __launch_bounds__(TTHREADS, sizeof(T) == 4 ? 2 : 1)
 k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__ bin_count,
@@ -531,7 +548,8 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
     const int ntile = g.tpitch * g.ty * g.tz;            // tile [tz][ty][tpitch], columns >= tx stay 0
     const bool fix = sizeof(T) == 4 && g.smode == 0;    // FP32: exact two-word int32 fixed point
     const bool fix1 = sizeof(T) == 4 && g.smode == 2;   // FP32: one-word int32 fixed point
-    const int csz = fix ? 16 : (int)sizeof(C<T>);       // bytes per complex cell
+    const bool fix64 = sizeof(T) == 8 && g.smode != 1;  // FP64: int64 + int32 fixed point (exact)
+    const int csz = fix ? 16 : fix64 ? 24 : (int)sizeof(C<T>);   // bytes per complex cell
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int total = sub_end[g.nbins - 1];
     const int tx = g.tpitch, txy = g.tpitch * g.ty;
@@ -540,6 +558,9 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
     int *flr = fhr + ntile, *fhi = flr + ntile, *fli = fhi + ntile;
     int *fre = fhr, *fim = flr;                        // one-word planes: re, im
     float *colsum = reinterpret_cast<float *>(fhr + 2 * ntile);   // one-word: per start column sum|c|
+    // FP64 planes: re-high, im-high (int64, units of 2^18), re-low, im-low (int32)
+    unsigned long long *gre = reinterpret_cast<unsigned long long *>(smem), *gim = gre + ntile;
+    int *lre = reinterpret_cast<int *>(gim + ntile), *lim = lre + ntile;
     for (int s = blockIdx.x; s < total; s += gridDim.x) {
         long long b;
         int start, stride, n;
@@ -552,7 +573,7 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
         const int shift = ox & 1, x_al = ox - shift;
         float4 *tv = reinterpret_cast<float4 *>(smem);
         for (int e = threadIdx.x; e < nvec; e += TTHREADS) tv[e] = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (!fix)
+        if (!fix && !fix64)                              // (ntile is even: 24-byte cells fill whole float4s)
             for (int e = nvec * 16 / csz + threadIdx.x; e < ntile; e += TTHREADS)
                 reinterpret_cast<C<T> *>(smem)[e] = C<T>{0, 0};
         if (fix1)
@@ -561,7 +582,7 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
         // Scale statistics of the chunk: largest component of c (gathered into
         // bin order by k_vis_prep); one word: start-column histogram of it.
         T m = 0;
-        if (fix || fix1)
+        if (fix || fix1 || fix64)
             for (int k = threadIdx.x; k < n; k += TTHREADS) {
                 const int i = start + k * stride;
                 const C<T> c = cs[i];
@@ -574,7 +595,7 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
             }
         T q = 1;
         double qinv = 1;
-        if (fix || fix1) {
+        if (fix || fix1 || fix64) {
             for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
             if (lane == 0) redbuf[warp] = m;
             __syncthreads();
@@ -585,6 +606,8 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
             if (fix) {
                 int e = m > (T)0 ? ilogb(m) + 1 : 0;       // 2^(e-1) <= m < 2^e
                 k = FIX_BITS - e;
+            } else if (fix64) {
+                k = 68 - (m > (T)0 ? ilogb(m * g.wmax3) + 1 : 0);
             } else {
                 // largest kw x kw box sum of the start-column histogram
                 float bmax = 0.f;
@@ -670,6 +693,21 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
                             }
                             continue;
                         }
+                    } else {
+                        if (fix64) {
+#pragma unroll
+                            for (int dx = 0; dx < KW; ++dx) {
+                                unsigned long long h;
+                                int l;
+                                split_fix64(ar * kx[dx], h, l);
+                                atomicAdd(gre + prow + dx, h);
+                                atomicAdd(lre + prow + dx, l);
+                                split_fix64(ai * kx[dx], h, l);
+                                atomicAdd(gim + prow + dx, h);
+                                atomicAdd(lim + prow + dx, l);
+                            }
+                            continue;
+                        }
                     }
                     T *row = reinterpret_cast<T *>(smem) + 2 * prow;
 #pragma unroll
@@ -703,6 +741,9 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
                 } else if (fix1) {
                     v.x = (T)(__int2float_rn(fre[e]) * qf);
                     v.y = (T)(__int2float_rn(fim[e]) * qf);
+                } else if (fix64) {
+                    v.x = (T)fma((double)(long long)gre[e], qinv * 262144.0, (double)lre[e] * qinv);
+                    v.y = (T)fma((double)(long long)gim[e], qinv * 262144.0, (double)lim[e] * qinv);
                 } else {
                     v = reinterpret_cast<const C<T> *>(smem)[e];
                 }
@@ -1255,7 +1296,8 @@ size_t tile_smem_bytes(const TileGeom &tg, int esize, int kw, int wdeg) {
     // rows padded to an even pitch (tx + 1 rounded up): the same cell index in
     // the spreader's and the interpolator's tiles (bank order of the sort key)
     const size_t pitch = (size_t)((tg.tx + 2) & ~1);
-    size_t s = pitch * tg.ty * tg.tz * 2 * (tg.fix == 1 ? 8 : esize);   // two-word: 4 int32 per cell
+    // cell bytes: FP32 two-word 4 int32, FP64 2 int64 + 2 int32, else two words of esize
+    size_t s = pitch * tg.ty * tg.tz * (tg.fix == 1 ? 16 : tg.fix == 3 ? 24 : 2 * esize);
     if (tg.fix == 2) s += pitch * tg.ty * 4;                           // one-word: column load histogram
     s += (size_t)NWARPS * 3 * KSTR * esize;
     s += (size_t)kw * (wdeg + 1) * esize;

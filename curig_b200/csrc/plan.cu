@@ -220,7 +220,8 @@ int plan_destroy(Plan *p) {
 // FP32 tile accumulation of the spreader (kernel numbering: 0 two-word int32,
 // 1 float atomics, 2 one-word int32).  Automatic: one word when the requested
 // epsilon is at least 1e-5 (its rounding, about 1.5e-6 relative, stays well
-// inside the error budget), else the exact two-word form.
+// inside the error budget), else the exact two-word form.  FP64 tiles take the
+// exact int64 + int32 form in every mode but 1 (double atomics).
 static int tile_mode(const Plan *p) {
     switch (p->opt.smode) {
     case 1: return 1;
@@ -234,10 +235,14 @@ static int choose_tiles(Plan *p, int esize, bool force_slabs) {
     const GridParams &gp = p->gp;
     const int kw = gp.kp.kw;
     TileGeom &t = p->tg;
-    // FP32 spreader: int32 fixed point, two words (exact) or one word per component
+    // FP32 spreader: int32 fixed point, two words (exact) or one word per component;
+    // FP64: int64 + int32 fixed point (exact)
     const int mode = tile_mode(p);
-    t.fix = (esize == 4 && kw <= TAB_KW) ? (mode == 0 ? 1 : mode == 2 ? 2 : 0) : 0;
-    size_t budget = p->opt.smem_budget ? p->opt.smem_budget : (t.fix ? 112 * 1024 : esize == 4 ? 72 * 1024 : 100 * 1024);
+    t.fix = kw > TAB_KW ? 0 : esize == 4 ? (mode == 0 ? 1 : mode == 2 ? 2 : 0) : (mode != 1 ? 3 : 0);
+    // FP32 tiles: two CTAs per SM (<= 112 KB each); FP64 fixed-point tiles: one
+    // CTA per SM (its registers), so a larger tile with less halo
+    size_t budget = p->opt.smem_budget ? p->opt.smem_budget
+                    : (t.fix == 3 ? 200 * 1024 : t.fix ? 112 * 1024 : esize == 4 ? 72 * 1024 : 100 * 1024);
     int wdeg = p->win.kind ? p->win.degree : 0;
     // does the w support stay inside [0, nf3)?  (z grows monotonically with w;
     // same arithmetic as the binning kernel, which rejects any start outside)

@@ -250,6 +250,23 @@ def test_one_word_fixed_point_all_in_one_cell(C):
     assert l2err(d3, d2) < 1e-5
 
 
+def test_fp64_fixed_point_all_in_one_cell_wide_range(C):
+    """FP64 int64 + int32 tiles: a 4000-visibility chunk at one uv point with
+    magnitudes over sixteen decades (the chunk scale follows the largest; the
+    high words of one cell take every term) against double atomics."""
+    rng = np.random.default_rng(8)
+    n = 4000
+    uvw = np.tile(np.array([[120.0, -80.0, 15.0]]), (n, 1))
+    freq = np.array([1.0e9])
+    mag = 10.0 ** rng.uniform(-8, 8, (n, 1))
+    ms = mag * (rng.standard_normal((n, 1)) + 1j * rng.standard_normal((n, 1)))
+    wgt = np.ones((n, 1))
+    psx = 1.0 * np.pi / 180 / 64
+    d0, _ = _plan_run(1, 64, 64, psx, psx, 1e-9, -1, uvw, freq, vis=ms, wgt=wgt, accumulate=0)
+    d1, _ = _plan_run(1, 64, 64, psx, psx, 1e-9, -1, uvw, freq, vis=ms, wgt=wgt, accumulate=1)
+    assert l2err(d1, d0) < 1e-13
+
+
 def test_bad_accumulate_option_is_rejected(C):
     from curig_b200 import GridderPlan
     from curig_b200._lib import CurigError
