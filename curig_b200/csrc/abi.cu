@@ -46,12 +46,19 @@ extern "C" void curig_default_opts(curig_opts *o) {
 extern "C" const char *curig_last_error(void) { return g_last_error.c_str(); }
 
 // One call with host buffers: allocate, copy in, plan, execute, copy out, free
-// (the reference's ms2dirty_exec / dirty2ms_exec life cycle, cugridder.cu:330-582).
+// (the reference's ms2dirty_exec / dirty2ms_exec life cycle, cugridder.cu:330-582),
+// pipelined over row slabs.  A copy stream uploads uvw first (set points needs
+// it), then for dirty2ms the image, then each slab's visibilities / weights
+// with an event per slab; the plan's stream spreads slab k as soon as it is on
+// the device (ms2dirty), or interpolates slab k and a download stream returns
+// its rows while slab k+1 is interpolated (dirty2ms).  With pinned host
+// buffers the transfers in both directions overlap the kernels.
 static int oneshot(int type, long long nrow, int nchan, int nx, int ny, double psx, double psy,
                    const double *freq, const double *uvw, void *vis, const void *wgt, void *dirty,
                    double eps, double sigma, int sign, const curig_opts *opts) {
     if (nrow < 0 || nchan <= 0 || nx <= 0 || ny <= 0 || !freq || !dirty || (nrow > 0 && (!uvw || !vis)))
         return fail(ERR_ARG, "invalid argument");
+    if (opts && (opts->slabs < 0 || opts->slabs > MAX_SLABS)) return fail(ERR_ARG, "slabs outside 0 .. 8");
     if (nrow == 0) {                      // no visibilities: empty sum / nothing to degrid
         if (type == 1) std::memset(dirty, 0, (size_t)nx * ny * 2 * (opts && opts->precision ? 4 : 8));
         return OK;
@@ -61,6 +68,14 @@ static int oneshot(int type, long long nrow, int nchan, int nx, int ny, double p
     opt.stream = st;
     const size_t rs = opt.precision ? 4 : 8, cs = 2 * rs;
     const size_t M = (size_t)nrow * nchan, npix = (size_t)nx * ny;
+    const size_t row_bytes = (size_t)nchan * (cs + (wgt ? rs : 0));
+    // automatic: 3 slabs from 1 GiB of visibilities + weights, 2 from 64 MiB
+    // (at 1.9 GB, 1 / 2 / 3 / 4 slabs: 142 / 124 / 122 / 131 ms per ms2dirty + dirty2ms)
+    const size_t up_bytes = (size_t)nrow * row_bytes;
+    int nslab = opts && opts->slabs > 0 ? opts->slabs
+                                        : up_bytes >= ((size_t)1 << 30) ? 3 : up_bytes >= ((size_t)64 << 20) ? 2 : 1;
+    if (nslab > nrow) nslab = (int)nrow;
+    opt.slabs = nslab;
     double *d_uvw = nullptr;
     void *d_vis = nullptr, *d_wgt = nullptr, *d_dirty = nullptr;
     Plan *p = nullptr;
@@ -72,42 +87,72 @@ static int oneshot(int type, long long nrow, int nchan, int nx, int ny, double p
         }
         return s == OK;
     };
-    // uvw goes up on the compute stream (set points needs it first); the
-    // visibilities / weights / image go up on a copy stream meanwhile (with
-    // pinned host buffers the copies overlap the binning), joined by an event
-    cudaStream_t cp = nullptr;
-    cudaEvent_t ev_alloc = nullptr, ev_up = nullptr;
-    if (chk(cudaStreamCreateWithFlags(&cp, cudaStreamNonBlocking)) &&
-        chk(cudaEventCreateWithFlags(&ev_alloc, cudaEventDisableTiming)) &&
-        chk(cudaEventCreateWithFlags(&ev_up, cudaEventDisableTiming)) &&
-        chk(cudaMallocAsync((void **)&d_uvw, 3 * nrow * sizeof(double), st)) &&
-        chk(cudaMallocAsync(&d_vis, M * cs, st)) &&
-        (!wgt || chk(cudaMallocAsync(&d_wgt, M * rs, st))) &&
-        chk(cudaMallocAsync(&d_dirty, npix * cs, st)) &&
-        chk(cudaEventRecord(ev_alloc, st)) && chk(cudaStreamWaitEvent(cp, ev_alloc, 0)) &&
-        chk(cudaMemcpyAsync(d_uvw, uvw, 3 * nrow * sizeof(double), cudaMemcpyHostToDevice, st)) &&
-        (type != 1 || chk(cudaMemcpyAsync(d_vis, vis, M * cs, cudaMemcpyHostToDevice, cp))) &&
-        (!wgt || chk(cudaMemcpyAsync(d_wgt, wgt, M * rs, cudaMemcpyHostToDevice, cp))) &&
-        (type != 2 || chk(cudaMemcpyAsync(d_dirty, dirty, npix * cs, cudaMemcpyHostToDevice, cp))) &&
-        chk(cudaEventRecord(ev_up, cp))) {
+    cudaStream_t cp = nullptr, dn = nullptr;        // uploads, downloads
+    cudaEvent_t ev_alloc = nullptr, ev_uvw = nullptr, ev_img = nullptr;
+    cudaEvent_t ev_ready[MAX_SLABS] = {}, ev_done[MAX_SLABS] = {};
+    bool ok = chk(cudaStreamCreateWithFlags(&cp, cudaStreamNonBlocking)) &&
+              chk(cudaStreamCreateWithFlags(&dn, cudaStreamNonBlocking)) &&
+              chk(cudaEventCreateWithFlags(&ev_alloc, cudaEventDisableTiming)) &&
+              chk(cudaEventCreateWithFlags(&ev_uvw, cudaEventDisableTiming)) &&
+              chk(cudaEventCreateWithFlags(&ev_img, cudaEventDisableTiming));
+    for (int k = 0; ok && k < nslab; ++k)
+        ok = chk(cudaEventCreateWithFlags(&ev_ready[k], cudaEventDisableTiming)) &&
+             chk(cudaEventCreateWithFlags(&ev_done[k], cudaEventDisableTiming));
+    ok = ok && chk(cudaMallocAsync((void **)&d_uvw, 3 * nrow * sizeof(double), st)) &&
+         chk(cudaMallocAsync(&d_vis, M * cs, st)) && (!wgt || chk(cudaMallocAsync(&d_wgt, M * rs, st))) &&
+         chk(cudaMallocAsync(&d_dirty, npix * cs, st)) && chk(cudaEventRecord(ev_alloc, st)) &&
+         chk(cudaStreamWaitEvent(cp, ev_alloc, 0)) &&
+         chk(cudaMemcpyAsync(d_uvw, uvw, 3 * nrow * sizeof(double), cudaMemcpyHostToDevice, cp)) &&
+         chk(cudaEventRecord(ev_uvw, cp)) &&
+         (type != 2 || chk(cudaMemcpyAsync(d_dirty, dirty, npix * cs, cudaMemcpyHostToDevice, cp))) &&
+         chk(cudaEventRecord(ev_img, cp));
+    for (int k = 0; ok && k < nslab; ++k) {          // slab k: rows [r0, r1)
+        const long long r0 = slab_first_row(nrow, nslab, k), r1 = slab_first_row(nrow, nslab, k + 1);
+        const size_t e0 = (size_t)r0 * nchan, ne = (size_t)(r1 - r0) * nchan;
+        ok = (type != 1 || chk(cudaMemcpyAsync(static_cast<char *>(d_vis) + e0 * cs,
+                                               static_cast<const char *>(vis) + e0 * cs, ne * cs,
+                                               cudaMemcpyHostToDevice, cp))) &&
+             (!wgt || chk(cudaMemcpyAsync(static_cast<char *>(d_wgt) + e0 * rs,
+                                          static_cast<const char *>(wgt) + e0 * rs, ne * rs,
+                                          cudaMemcpyHostToDevice, cp))) &&
+             chk(cudaEventRecord(ev_ready[k], cp));
+    }
+    if (ok) {
         s = plan_create(type, nx, ny, psx, psy, eps, sigma, sign, opt, &p);
+        if (s == OK && !chk(cudaStreamWaitEvent(st, ev_uvw, 0))) s = ERR_CUDA;
         if (s == OK) s = plan_setpts(p, nrow, nchan, d_uvw, d_uvw + 1, d_uvw + 2, 3, freq);
-        if (s == OK && !chk(cudaStreamWaitEvent(st, ev_up, 0))) s = ERR_CUDA;
-        if (s == OK) s = plan_execute(p, d_vis, d_wgt, d_dirty);
+        if (s == OK && !chk(cudaStreamWaitEvent(st, ev_img, 0))) s = ERR_CUDA;
+        if (s == OK)
+            s = plan_execute_slabs(p, type, d_vis, d_wgt, d_dirty, ev_ready, type == 2 ? ev_done : nullptr, nslab);
         if (s == OK) {
-            if (type == 1) chk(cudaMemcpyAsync(dirty, d_dirty, npix * cs, cudaMemcpyDeviceToHost, st));
-            else chk(cudaMemcpyAsync(vis, d_vis, M * cs, cudaMemcpyDeviceToHost, st));
+            if (type == 1) {
+                chk(cudaMemcpyAsync(dirty, d_dirty, npix * cs, cudaMemcpyDeviceToHost, st));
+            } else {
+                for (int k = 0; s == OK && k < nslab; ++k) {
+                    const long long r0 = slab_first_row(nrow, nslab, k), r1 = slab_first_row(nrow, nslab, k + 1);
+                    const size_t e0 = (size_t)r0 * nchan, ne = (size_t)(r1 - r0) * nchan;
+                    if (chk(cudaStreamWaitEvent(dn, ev_done[k], 0)))
+                        chk(cudaMemcpyAsync(static_cast<char *>(vis) + e0 * cs,
+                                            static_cast<const char *>(d_vis) + e0 * cs, ne * cs,
+                                            cudaMemcpyDeviceToHost, dn));
+                }
+            }
         }
         if (s == OK) s = plan_device_status(p);   // flags raised by kernels (synchronises)
         if (p && s != OK && !p->last_error.empty()) g_last_error = p->last_error;
-        if (p) plan_destroy(p);
     }
-    if (cp) {                              // nothing freed while an upload may still run
-        cudaStreamSynchronize(cp);
-        cudaStreamDestroy(cp);
+    // nothing is freed while a transfer may still run
+    if (cp) cudaStreamSynchronize(cp);
+    if (dn) cudaStreamSynchronize(dn);
+    if (p) plan_destroy(p);
+    if (cp) cudaStreamDestroy(cp);
+    if (dn) cudaStreamDestroy(dn);
+    for (cudaEvent_t e : {ev_alloc, ev_uvw, ev_img})
+        if (e) cudaEventDestroy(e);
+    for (int k = 0; k < MAX_SLABS; ++k) {
+        if (ev_ready[k]) cudaEventDestroy(ev_ready[k]);
+        if (ev_done[k]) cudaEventDestroy(ev_done[k]);
     }
-    if (ev_alloc) cudaEventDestroy(ev_alloc);
-    if (ev_up) cudaEventDestroy(ev_up);
     if (d_uvw) cudaFreeAsync(d_uvw, st);
     if (d_vis) cudaFreeAsync(d_vis, st);
     if (d_wgt) cudaFreeAsync(d_wgt, st);

@@ -159,8 +159,10 @@ __global__ void k_wrange(const double *__restrict__ w, int stride, long long nro
 // ------------------------------------------------------------------ binning
 // Sort key of one visibility: bin id in the high bits, then the residue mod 32
 // of its start cell's index in the tile (the shared-memory bank of its first
-// tap); the radix sort is stable, so equal keys keep input order.  0xffffffff
-// marks a visibility that could not be placed.
+// tap); the radix sort is stable, so equal keys keep input order.  With row
+// slabs the bin id is slab * nbins_slab + bin (slab = row * nslab / nrow), so
+// each slab's visibilities are contiguous in sorted order.  0xffffffff marks a
+// visibility that could not be placed.
 __global__ void k_bin_keys(DevGeom g, const double *__restrict__ uu, const double *__restrict__ vv,
                            const double *__restrict__ ww, const double *__restrict__ foc,
                            unsigned *__restrict__ keys, int *__restrict__ vals, int *err) {
@@ -178,7 +180,8 @@ __global__ void k_bin_keys(DevGeom g, const double *__restrict__ uu, const doubl
             atomicOr(err, e);
         } else {
             unsigned cell = g.cbits ? (unsigned)((L.lz * g.ty + L.ly) * g.tpitch + L.lx) & 31u : 0u;
-            key = ((unsigned)L.bin << g.cbits) | cell;
+            const long long slab = g.nslab > 1 ? row * g.nslab / g.nrow : 0;
+            key = ((unsigned)(slab * g.nbins_slab + L.bin) << g.cbits) | cell;
         }
         keys[j] = key;
         vals[j] = (int)j;
@@ -335,10 +338,10 @@ k_spread(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__ b
     T *ks = ksall + warp * 3 * KSTR;
     if (g.wkind == 1)
         for (int i = threadIdx.x; i < kw * (g.wdeg + 1); i += NTHREADS) coef[i] = (T)wcoef[i];
-    const int total = sub_end[g.nbins - 1];
+    const int total = g.sub_hi ? g.sub_hi : sub_end[g.nbins - 1];   // sub-problem window [sub_lo, total)
     const int kk = kw * kw, k3 = kk * kw;
     const int txy = g.tx * g.ty;
-    for (int s = blockIdx.x; s < total; s += gridDim.x) {
+    for (int s = g.sub_lo + blockIdx.x; s < total; s += gridDim.x) {
         long long b = find_bin(sub_end, g.nbins, s);
         int cnt = bin_count[b];
         int nsb = (cnt + g.sub - 1) / g.sub;
@@ -367,7 +370,8 @@ k_spread(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__ b
             __syncwarp();
         }
         __syncthreads();
-        long long bxi = b % g.nbx, byi = (b / g.nbx) % g.nby, bzi = b / ((long long)g.nbx * g.nby);
+        const long long bl = b % g.nbins_slab;
+        long long bxi = bl % g.nbx, byi = (bl / g.nbx) % g.nby, bzi = bl / ((long long)g.nbx * g.nby);
         int ox = (int)bxi * g.bx - g.hkw, oy = (int)byi * g.by - g.hkw;
         int oz = g.zpad ? (int)bzi * g.bz - g.hkw : 0;
         for (int row = warp; row < g.ty * g.tz; row += NWARPS) {
@@ -404,17 +408,18 @@ k_interp(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__ b
     T *ks = ksall + warp * 3 * KSTR;
     if (g.wkind == 1)
         for (int i = threadIdx.x; i < kw * (g.wdeg + 1); i += NTHREADS) coef[i] = (T)wcoef[i];
-    const int total = sub_end[g.nbins - 1];
+    const int total = g.sub_hi ? g.sub_hi : sub_end[g.nbins - 1];   // sub-problem window [sub_lo, total)
     const int kk = kw * kw, k3 = kk * kw;
     const int txy = g.tx * g.ty;
-    for (int s = blockIdx.x; s < total; s += gridDim.x) {
+    for (int s = g.sub_lo + blockIdx.x; s < total; s += gridDim.x) {
         long long b = find_bin(sub_end, g.nbins, s);
         int cnt = bin_count[b];
         int nsb = (cnt + g.sub - 1) / g.sub;
         int chunk = s - (sub_end[b] - nsb);
         int first = bin_start[b] + chunk * g.sub;
         int last = min(first + g.sub, bin_start[b] + cnt);
-        long long bxi = b % g.nbx, byi = (b / g.nbx) % g.nby, bzi = b / ((long long)g.nbx * g.nby);
+        const long long bl = b % g.nbins_slab;
+        long long bxi = bl % g.nbx, byi = (bl / g.nbx) % g.nby, bzi = bl / ((long long)g.nbx * g.nby);
         int ox = (int)bxi * g.bx - g.hkw, oy = (int)byi * g.by - g.hkw;
         int oz = g.zpad ? (int)bzi * g.bz - g.hkw : 0;
         for (int row = warp; row < g.ty * g.tz; row += NWARPS) {
@@ -551,7 +556,7 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
     const bool fix64 = sizeof(T) == 8 && g.smode != 1;  // FP64: int64 + int32 fixed point (exact)
     const int csz = fix ? 16 : fix64 ? 24 : (int)sizeof(C<T>);   // bytes per complex cell
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int total = sub_end[g.nbins - 1];
+    const int total = g.sub_hi ? g.sub_hi : sub_end[g.nbins - 1];   // sub-problem window [sub_lo, total)
     const int tx = g.tpitch, txy = g.tpitch * g.ty;
     const int nvec = (ntile * csz) / 16;
     int *fhr = reinterpret_cast<int *>(smem);          // two-word planes: re-high, re-low, im-high, im-low
@@ -561,13 +566,14 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
     // FP64 planes: re-high, im-high (int64, units of 2^18), re-low, im-low (int32)
     unsigned long long *gre = reinterpret_cast<unsigned long long *>(smem), *gim = gre + ntile;
     int *lre = reinterpret_cast<int *>(gim + ntile), *lim = lre + ntile;
-    for (int s = blockIdx.x; s < total; s += gridDim.x) {
+    for (int s = g.sub_lo + blockIdx.x; s < total; s += gridDim.x) {
         long long b;
         int start, stride, n;
         sub_range(g, bin_start, bin_count, sub_end, s, b, start, stride, n);
         // tile origin; columns are stored from x_al = ox rounded down to even
         // (column lx + shift), the layout of the interpolator's tiles
-        const long long bxi = b % g.nbx, byi = (b / g.nbx) % g.nby, bzi = b / ((long long)g.nbx * g.nby);
+        const long long bl = b % g.nbins_slab;     // bin within its row slab
+        const long long bxi = bl % g.nbx, byi = (bl / g.nbx) % g.nby, bzi = bl / ((long long)g.nbx * g.nby);
         const int ox = (int)bxi * g.bx - g.hkw, oy = (int)byi * g.by - g.hkw;
         const int oz = g.zpad ? (int)bzi * g.bz - g.hkw : 0;
         const int shift = ox & 1, x_al = ox - shift;
@@ -888,7 +894,7 @@ k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
     __shared__ unsigned long long bar;      // TMA completion barrier
     C<T> *tile = reinterpret_cast<C<T> *>(smem);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int total = sub_end[g.nbins - 1];
+    const int total = g.sub_hi ? g.sub_hi : sub_end[g.nbins - 1];   // sub-problem window [sub_lo, total)
     const int tx = g.tpitch, txy = g.tpitch * g.ty;
     const unsigned tile_bytes = (unsigned)(g.tpitch * g.ty * g.tz * sizeof(C<T>));
     unsigned parity = 0;
@@ -897,11 +903,12 @@ k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    for (int s = blockIdx.x; s < total; s += gridDim.x) {
+    for (int s = g.sub_lo + blockIdx.x; s < total; s += gridDim.x) {
         long long b;
         int start, stride, n;
         sub_range(g, bin_start, bin_count, sub_end, s, b, start, stride, n);
-        const long long bxi = b % g.nbx, byi = (b / g.nbx) % g.nby, bzi = b / ((long long)g.nbx * g.nby);
+        const long long bl = b % g.nbins_slab;     // bin within its row slab
+        const long long bxi = bl % g.nbx, byi = (bl / g.nbx) % g.nby, bzi = bl / ((long long)g.nbx * g.nby);
         const int ox = (int)bxi * g.bx - g.hkw, oy = (int)byi * g.by - g.hkw;
         const int oz = g.zpad ? (int)bzi * g.bz - g.hkw : 0;
         const int shift = ox & 1, x_al = ox - shift;

@@ -26,7 +26,10 @@ struct DevGeom {
     int use_tma;                   // interpolator stages interior tiles with one TMA box load (FP32)
     int no_w;                      // w ignored: one plane, no z taps (window factor 1)
     float wmax3;                   // bound on |kx ky kz| of the tabulated window
-    long long nbins;
+    long long nbins;               // bins of all row slabs: nslab * nbins_slab
+    long long nbins_slab;          // bins of one row slab (nbx * nby * nbz)
+    int nslab;                     // row slabs (sort key major part; 1 = none)
+    int sub_lo, sub_hi;            // sub-problem window of one launch (sub_hi 0: all)
     double beta, c;                // ES parameters
     int wkind, wdeg;               // window kind (0 ES, 1 polynomial), degree
     // visibility geometry

@@ -382,7 +382,16 @@ retry_tiles:
     g.tx = tg.tx; g.ty = tg.ty; g.tz = tg.tz; g.zpad = tg.zpad; g.sub = tg.sub;
     g.tpitch = (tg.tx + 2) & ~1;
     g.use_tma = 0;                          // set once the grid's TMA descriptor exists
-    g.nbins = tg.nbins();
+    // row slabs (tile kernels only): bins of slab k are k * nbins_slab + bin
+    int nslab = std::max(1, std::min(p->opt.slabs, MAX_SLABS));
+    if (g.kw > TAB_KW || nrow < nslab || (long long)nslab * tg.nbins() > INT_MAX / 2) nslab = 1;
+    p->nslab = nslab;
+    g.nslab = nslab;
+    g.nbins_slab = tg.nbins();
+    g.nbins = nslab * tg.nbins();
+    g.sub_lo = g.sub_hi = 0;
+    p->slab_row.resize(nslab + 1);
+    for (int k = 0; k <= nslab; ++k) p->slab_row[k] = slab_first_row(nrow, nslab, k);
     g.beta = gp.kp.beta; g.c = gp.kp.c;
     g.wkind = p->win.kind; g.wdeg = p->win.kind ? p->win.degree : 0;
     g.smode = tile_mode(p);
@@ -473,6 +482,10 @@ retry_tiles:
     launch_bin_bounds(p->d_key_b, M, cbits, p->d_bin_start, p->d_bin_last, st);
     launch_nsub(p->d_bin_start, p->d_bin_last, p->d_bin_count, p->d_nsub, nb, g.sub, st);
     if (scan_inclusive(p->d_tmp, p->tmp_bytes, p->d_nsub, p->d_sub_end, nb, st)) return ERR_CUDA;
+    p->slab_sub_end.assign(nslab, 0);               // last sub-problem end of every slab
+    for (int k = 0; k < nslab; ++k)
+        CU_TRY(cudaMemcpyAsync(&p->slab_sub_end[k], p->d_sub_end + (k + 1) * g.nbins_slab - 1, sizeof(int),
+                               cudaMemcpyDeviceToHost, st));
     CU_TRY(cudaMemcpyAsync(&herr, p->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     CU_TRY(cudaStreamSynchronize(st));
     CU_TRY(cudaGetLastError());
@@ -650,6 +663,84 @@ static int execute_t(Plan *p, int type, void *d_vis, const void *d_wgt, void *d_
     }
     CU_TRY(cudaGetLastError());
     return OK;
+}
+
+template <typename T>
+static int execute_slabs_t(Plan *p, int type, void *d_vis, const void *d_wgt, void *d_dirty,
+                           const cudaEvent_t *ready, const cudaEvent_t *done, int nev) {
+    cudaStream_t st = p->st;
+    const GridParams &gp = p->gp;
+    const int ns = p->nslab;
+    if (nev != ns && !(ns == 1 && nev > 0)) return ERR_ARG;
+    auto wait_slab = [&](int k) {
+        if (!ready) return cudaSuccess;
+        if (ns == nev) return cudaStreamWaitEvent(st, ready[k], 0);
+        for (int e = 0; e < nev; ++e) {               // one plan slab: every upload
+            cudaError_t r = cudaStreamWaitEvent(st, ready[e], 0);
+            if (r != cudaSuccess) return r;
+        }
+        return cudaSuccess;
+    };
+    auto done_slab = [&](int k) {
+        if (!done) return cudaSuccess;
+        if (ns == nev) return cudaEventRecord(done[k], st);
+        for (int e = 0; e < nev; ++e) {
+            cudaError_t r = cudaEventRecord(done[e], st);
+            if (r != cudaSuccess) return r;
+        }
+        return cudaSuccess;
+    };
+    // launch geometry of slab k: its sub-problem window
+    auto slab_geom = [&](int k, DevGeom &gk) {
+        gk = p->dg;
+        gk.sub_lo = k ? p->slab_sub_end[k - 1] : 0;
+        gk.sub_hi = p->slab_sub_end[k];
+        return gk.sub_hi > gk.sub_lo;
+    };
+    const VisIO io{p->d_idx, p->d_ph, d_wgt, d_vis};
+    const double *ht = p->htab.empty() ? nullptr : p->htab.data();
+    int s;
+    if (type == 1) {
+        const size_t gbytes = (size_t)gp.nf1 * gp.nf2 * gp.nf3 * 2 * sizeof(T);
+        CU_TRY(cudaMemsetAsync(p->d_grid, 0, gbytes, st));
+        for (int k = 0; k < ns; ++k) {
+            CU_TRY(wait_slab(k));
+            const long long i0 = p->slab_row[k] * p->nchan, i1 = p->slab_row[k + 1] * p->nchan;
+            if (i1 > i0)
+                launch_vis_prep<T>(i1 - i0, p->d_idx + i0, static_cast<const char *>(p->d_ph) + i0 * 2 * sizeof(T),
+                                   d_vis, d_wgt, static_cast<char *>(p->d_cs) + i0 * 2 * sizeof(T), st);
+            DevGeom gk;
+            if (slab_geom(k, gk) &&
+                (s = launch_spread<T>(gk, p->smem, p->d_bin_start, p->d_bin_count, p->d_sub_end, p->d_rec, p->d_cs,
+                                      p->d_grid, p->d_wcoef, ht, io, p->nrow * p->nchan, p->nsm, st)))
+                return s;
+        }
+        if ((s = plane_fft<T>(p, CUFFT_INVERSE, true))) return s;
+        launch_correct_m2d<T>(p->dc, p->d_tgrid, d_dirty, st);
+    } else {
+        launch_zero_tpad<T>(p->nx, p->ny, gp.nf2, gp.nf3, p->d_tgrid, st);
+        launch_correct_d2m<T>(p->dc, d_dirty, p->d_tgrid, st);
+        if ((s = plane_fft<T>(p, CUFFT_FORWARD, false))) return s;
+        for (int k = 0; k < ns; ++k) {
+            CU_TRY(wait_slab(k));
+            DevGeom gk;
+            if (slab_geom(k, gk) &&
+                (s = launch_interp<T>(gk, p->smem_interp, p->d_bin_start, p->d_bin_count, p->d_sub_end, p->d_rec,
+                                      p->d_grid, p->d_cs, p->d_wcoef, ht, io, p->nrow * p->nchan, &p->tmap,
+                                      p->d_err, p->nsm, st)))
+                return s;
+            CU_TRY(done_slab(k));
+        }
+    }
+    CU_TRY(cudaGetLastError());
+    return OK;
+}
+
+int plan_execute_slabs(Plan *p, int type, void *d_vis, const void *d_wgt, void *d_dirty,
+                       const cudaEvent_t *ready, const cudaEvent_t *done, int nev) {
+    if (!p || !p->ready || !d_vis || !d_dirty || (type != 1 && type != 2)) return ERR_ARG;
+    return p->opt.precision ? execute_slabs_t<float>(p, type, d_vis, d_wgt, d_dirty, ready, done, nev)
+                            : execute_slabs_t<double>(p, type, d_vis, d_wgt, d_dirty, ready, done, nev);
 }
 
 // Error flags raised by kernels of earlier executes (an interpolator tile load

@@ -21,6 +21,7 @@ struct Options {
     int w_term = 0;           // 0: improved w-stacking, 1: w ignored (2-D gridding, no n - 1, n = 1)
     int grid_x = 0, grid_y = 0;   // oversampled grid along the nxdirty / nydirty axes (0: sigma rule)
     int bin_z = 0;                // w-planes per tile slab (0: automatic)
+    int slabs = 1;                // row slabs of the sort (one-shot copy / compute pipeline), 1..MAX_SLABS
 };
 
 struct Plan {
@@ -47,6 +48,11 @@ struct Plan {
     size_t smem = 0, smem_interp = 0;
     double wmin_eff = 0, wmax_eff = 0;
     std::vector<double> htab;   // window table [kw][TAB_DEG] for the thread-per-visibility kernels
+    // row slabs: slab k holds rows [slab_row[k], slab_row[k+1]) and the
+    // sub-problems [k ? slab_sub_end[k-1] : 0, slab_sub_end[k])
+    int nslab = 1;
+    std::vector<long long> slab_row;
+    std::vector<int> slab_sub_end;
 
     // device buffers owned by the plan
     double *d_foc = nullptr, *d_quad = nullptr, *d_psi1 = nullptr, *d_psi2 = nullptr, *d_wcoef = nullptr;
@@ -93,6 +99,22 @@ int plan_create(int type, int nx, int ny, double psx, double psy, double eps, do
 int plan_setpts(Plan *p, long long nrow, int nchan, const double *du, const double *dv,
                 const double *dw, int stride, const double *h_freq);
 int plan_execute(Plan *p, void *d_vis, const void *d_wgt, void *d_dirty, int type = 0);
+// The same transform run slab by slab (the one-shot copy / compute pipeline).
+// ms2dirty: before slab k the plan's stream waits for ready[k] (the upload of
+// that slab's visibilities and weights), then gathers and spreads it; the grid
+// transforms follow the last slab.  dirty2ms: the grid is prepared first (the
+// image must be on the device), then slab k is interpolated after ready[k]
+// (its weights) and done[k] is recorded (its rows of d_vis are final).  The
+// events describe the caller's partition of the rows into nev slabs: it must
+// equal the plan's (nev == nslab), or the plan has one slab and waits for /
+// records all of them.  Either array may be null.
+int plan_execute_slabs(Plan *p, int type, void *d_vis, const void *d_wgt, void *d_dirty,
+                       const cudaEvent_t *ready, const cudaEvent_t *done, int nev);
+constexpr int MAX_SLABS = 8;
+// first row of slab k of nslab over nrow rows (k = nslab gives nrow)
+inline long long slab_first_row(long long nrow, int nslab, int k) {
+    return ((long long)k * nrow + nslab - 1) / nslab;
+}
 int plan_destroy(Plan *p);
 void plan_release_points(Plan *p);
 

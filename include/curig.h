@@ -79,6 +79,11 @@ typedef struct curig_opts {
     int grid_y;           /* the same along the nydirty axis (Nifty's ny); both or neither */
     int bin_z;            /* w-planes per tile slab (1 .. nf3 - 1), 0 = automatic (all planes in
                              one tile unless a w support could wrap) */
+    int slabs;            /* one-shot calls only: row slabs of the copy / compute pipeline
+                             (1 .. 8; ms2dirty spreads slab k while slab k+1 is uploaded,
+                             dirty2ms downloads slab k while slab k+1 is interpolated);
+                             0 = automatic (3 from 1 GiB of visibilities and weights,
+                             2 from 64 MiB, else 1).  Plans ignore it. */
 } curig_opts;
 
 void curig_default_opts(curig_opts *opts);
