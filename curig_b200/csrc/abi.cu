@@ -87,11 +87,14 @@ static int oneshot(int type, long long nrow, int nchan, int nx, int ny, double p
         }
         return s == OK;
     };
-    cudaStream_t cp = nullptr, dn = nullptr;        // uploads, downloads
-    cudaEvent_t ev_alloc = nullptr, ev_uvw = nullptr, ev_img = nullptr;
+    cudaStream_t cp = nullptr, dn = nullptr, bn = nullptr;   // uploads, downloads, dirty2ms binning
+    cudaEvent_t ev_alloc = nullptr, ev_uvw = nullptr, ev_img = nullptr, ev_geom = nullptr, ev_bin = nullptr;
     cudaEvent_t ev_ready[MAX_SLABS] = {}, ev_done[MAX_SLABS] = {};
     bool ok = chk(cudaStreamCreateWithFlags(&cp, cudaStreamNonBlocking)) &&
               chk(cudaStreamCreateWithFlags(&dn, cudaStreamNonBlocking)) &&
+              chk(cudaStreamCreateWithFlags(&bn, cudaStreamNonBlocking)) &&
+              chk(cudaEventCreateWithFlags(&ev_geom, cudaEventDisableTiming)) &&
+              chk(cudaEventCreateWithFlags(&ev_bin, cudaEventDisableTiming)) &&
               chk(cudaEventCreateWithFlags(&ev_alloc, cudaEventDisableTiming)) &&
               chk(cudaEventCreateWithFlags(&ev_uvw, cudaEventDisableTiming)) &&
               chk(cudaEventCreateWithFlags(&ev_img, cudaEventDisableTiming));
@@ -120,10 +123,24 @@ static int oneshot(int type, long long nrow, int nchan, int nx, int ny, double p
     if (ok) {
         s = plan_create(type, nx, ny, psx, psy, eps, sigma, sign, opt, &p);
         if (s == OK && !chk(cudaStreamWaitEvent(st, ev_uvw, 0))) s = ERR_CUDA;
-        if (s == OK) s = plan_setpts(p, nrow, nchan, d_uvw, d_uvw + 1, d_uvw + 2, 3, freq);
+        if (s == OK) s = plan_setpts_geometry(p, nrow, nchan, d_uvw, d_uvw + 1, d_uvw + 2, 3, freq);
+        if (s == OK && type == 1) {
+            s = plan_setpts_bin(p, st);
+        } else if (s == OK) {
+            // dirty2ms: the grid preparation (plan's stream) runs while a second
+            // stream bins the visibilities; neither depends on the other
+            if (!chk(cudaEventRecord(ev_geom, st)) || !chk(cudaStreamWaitEvent(bn, ev_geom, 0)) ||
+                !chk(cudaStreamWaitEvent(st, ev_img, 0)))
+                s = ERR_CUDA;
+            if (s == OK) s = plan_d2m_prologue(p, d_dirty);
+            if (s == OK) s = plan_setpts_bin(p, bn);
+            if (s == OK && (!chk(cudaEventRecord(ev_bin, bn)) || !chk(cudaStreamWaitEvent(st, ev_bin, 0))))
+                s = ERR_CUDA;
+        }
         if (s == OK && !chk(cudaStreamWaitEvent(st, ev_img, 0))) s = ERR_CUDA;
         if (s == OK)
-            s = plan_execute_slabs(p, type, d_vis, d_wgt, d_dirty, ev_ready, type == 2 ? ev_done : nullptr, nslab);
+            s = plan_execute_slabs(p, type, d_vis, d_wgt, d_dirty, ev_ready, type == 2 ? ev_done : nullptr, nslab,
+                                   type == 2);
         if (s == OK) {
             if (type == 1) {
                 chk(cudaMemcpyAsync(dirty, d_dirty, npix * cs, cudaMemcpyDeviceToHost, st));
@@ -142,12 +159,12 @@ static int oneshot(int type, long long nrow, int nchan, int nx, int ny, double p
         if (p && s != OK && !p->last_error.empty()) g_last_error = p->last_error;
     }
     // nothing is freed while a transfer may still run
-    if (cp) cudaStreamSynchronize(cp);
-    if (dn) cudaStreamSynchronize(dn);
+    for (cudaStream_t x : {cp, dn, bn})
+        if (x) cudaStreamSynchronize(x);
     if (p) plan_destroy(p);
-    if (cp) cudaStreamDestroy(cp);
-    if (dn) cudaStreamDestroy(dn);
-    for (cudaEvent_t e : {ev_alloc, ev_uvw, ev_img})
+    for (cudaStream_t x : {cp, dn, bn})
+        if (x) cudaStreamDestroy(x);
+    for (cudaEvent_t e : {ev_alloc, ev_uvw, ev_img, ev_geom, ev_bin})
         if (e) cudaEventDestroy(e);
     for (int k = 0; k < MAX_SLABS; ++k) {
         if (ev_ready[k]) cudaEventDestroy(ev_ready[k]);

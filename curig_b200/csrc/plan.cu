@@ -201,6 +201,7 @@ void plan_release_points(Plan *p) {
     dfree(p->d_rec, st); dfree(p->d_ph, st); dfree(p->d_cs, st); dfree(p->d_grid, st); dfree(p->d_tmp, st);
     dfree(p->d_tgrid, st);
     p->ready = false;
+    p->geom_ready = false;
 }
 
 int plan_destroy(Plan *p) {
@@ -299,8 +300,8 @@ static double key_to_double(unsigned long long k) {
     return d;
 }
 
-int plan_setpts(Plan *p, long long nrow, int nchan, const double *du, const double *dv,
-                const double *dw, int stride, const double *h_freq) {
+int plan_setpts_geometry(Plan *p, long long nrow, int nchan, const double *du, const double *dv,
+                         const double *dw, int stride, const double *h_freq) {
     if (!p) return ERR_ARG;
     if (nrow <= 0 || nchan <= 0 || !du || !dv || !dw || !h_freq || stride <= 0) return ERR_ARG;
     if (nrow * (long long)nchan >= INT_MAX) return ERR_ARG;
@@ -313,7 +314,6 @@ int plan_setpts(Plan *p, long long nrow, int nchan, const double *du, const doub
     p->freq.assign(h_freq, h_freq + nchan);
     p->du = du; p->dv = dv; p->dw = dw; p->stride = stride;
     const int esize = p->opt.precision ? 4 : 8;
-    const long long M = nrow * nchan;
 
     // 1. raw w range -> effective range over channels (precomp.cu:61-69, utils.cu:42-53)
     mark(p, EV_SET_BEGIN);
@@ -361,6 +361,68 @@ int plan_setpts(Plan *p, long long nrow, int nchan, const double *du, const doub
     if (s != OK) return s;
     if (req.no_w && p->gp.kp.kw > TAB_KW) return ERR_UNSUPPORTED;   // thread-per-visibility kernels only
     p->win.kw = p->gp.kp.kw;
+    // 3. correction tables (deconv.cu:60-197): psi1, psi2 on the grid, quadrature for psi3
+    //    (psi1 / psi2 evaluated on the device from the quadrature: no host work
+    //    while the GPU waits)
+    const GridParams &gp = p->gp;
+    double qx[MAX_QUAD], qg[MAX_QUAD];
+    int nq = quadrature_terms(gp.kp, p->win, qx, qg);
+    CU_TRY(dalloc(&p->d_foc, nchan * sizeof(double), st));
+    CU_TRY(dalloc(&p->d_quad, 2 * MAX_QUAD * sizeof(double), st));
+    CU_TRY(dalloc(&p->d_psi1, (gp.nf1 / 2 + 1) * sizeof(double), st));
+    CU_TRY(dalloc(&p->d_psi2, (gp.nf2 / 2 + 1) * sizeof(double), st));
+    CU_TRY(cudaMemcpyAsync(p->d_foc, foc.data(), nchan * sizeof(double), cudaMemcpyHostToDevice, st));
+    CU_TRY(cudaMemcpyAsync(p->d_quad, qx, nq * sizeof(double), cudaMemcpyHostToDevice, st));
+    CU_TRY(cudaMemcpyAsync(p->d_quad + MAX_QUAD, qg, nq * sizeof(double), cudaMemcpyHostToDevice, st));
+    launch_psi_grid(gp.nf1 / 2 + 1, nq, p->d_quad, p->d_quad + MAX_QUAD, p->d_psi1, st);
+    launch_psi_grid(gp.nf2 / 2 + 1, nq, p->d_quad, p->d_quad + MAX_QUAD, p->d_psi2, st);
+    if (p->win.kind == 1) {
+        CU_TRY(dalloc(&p->d_wcoef, p->win.coef.size() * sizeof(double), st));
+        CU_TRY(cudaMemcpyAsync(p->d_wcoef, p->win.coef.data(), p->win.coef.size() * sizeof(double),
+                               cudaMemcpyHostToDevice, st));
+    }
+    DevCorr &cc = p->dc;
+    cc.nx = p->nx; cc.ny = p->ny; cc.nf1 = gp.nf1; cc.nf2 = gp.nf2; cc.nf3 = gp.nf3;
+    cc.psx = gp.pixsize_x; cc.psy = gp.pixsize_y; cc.o_center = gp.o_center; cc.i_center = gp.i_center;
+    cc.gamma = gp.gamma; cc.h = gp.h; cc.nquad = nq; cc.no_w = gp.no_w;
+    cc.qx = p->d_quad; cc.qg = p->d_quad + MAX_QUAD; cc.psi1 = p->d_psi1; cc.psi2 = p->d_psi2;
+
+    // 4. fine grid and FFT plans
+    size_t gbytes = (size_t)gp.nf1 * gp.nf2 * gp.nf3 * 2 * esize;
+    CU_TRY(dalloc(&p->d_grid, gbytes, st));
+
+    // 2-D transforms as two passes of contiguous rows: x rows of every plane
+    // (length nf1), and y rows (length nf2) of the image's columns only, kept
+    // transposed in d_tgrid [nf3][ny][nf2]
+    CU_TRY(dalloc(&p->d_tgrid, (size_t)gp.nf3 * p->ny * gp.nf2 * 2 * esize, st));
+    const long long nxrows = (long long)gp.nf2 * gp.nf3, nyrows = (long long)p->ny * gp.nf3;
+    p->fft_bx = (int)std::max(1LL, std::min(nxrows, (1LL << 28) / gp.nf1));
+    p->fft_bx_rest = (int)(nxrows % p->fft_bx);
+    p->fft_by = (int)std::max(1LL, std::min(nyrows, (1LL << 28) / gp.nf2));
+    p->fft_by_rest = (int)(nyrows % p->fft_by);
+    const int pr = p->opt.precision;
+    if (fft_plan1(p->device, gp.nf1, 1, gp.nf1, p->fft_bx, pr, p->st, p->fft_hx)) return ERR_CUFFT;
+    if (p->fft_bx_rest && fft_plan1(p->device, gp.nf1, 1, gp.nf1, p->fft_bx_rest, pr, p->st, p->fft_hx_rest))
+        return ERR_CUFFT;
+    if (fft_plan1(p->device, gp.nf2, 1, gp.nf2, p->fft_by, pr, p->st, p->fft_hy)) return ERR_CUFFT;
+    if (p->fft_by_rest && fft_plan1(p->device, gp.nf2, 1, gp.nf2, p->fft_by_rest, pr, p->st, p->fft_hy_rest))
+        return ERR_CUFFT;
+    p->geom_ready = true;
+    return OK;
+}
+
+// Tiles, bins, the sort and the per-visibility records, on stream st (the
+// plan's stream, or a second stream that the caller joins before executing).
+int plan_setpts_bin(Plan *p, cudaStream_t st) {
+    if (!p || !p->geom_ready) return ERR_ARG;
+    const int esize = p->opt.precision ? 4 : 8;
+    const long long nrow = p->nrow;
+    const int nchan = p->nchan;
+    const long long M = nrow * nchan;
+    const double *du = p->du, *dv = p->dv, *dw = p->dw;
+    const int stride = p->stride;
+    int herr = 0, s;
+    mark(p, EV_SET_WRANGE);
     bool force_slabs = false;
 retry_tiles:
     s = choose_tiles(p, esize, force_slabs);
@@ -427,36 +489,10 @@ retry_tiles:
     g.psx = gp.pixsize_x; g.psy = gp.pixsize_y; g.i_center = gp.i_center; g.gamma = gp.gamma;
     g.o_center = gp.o_center; g.sign = (double)gp.sign;
 
-    // 3. correction tables (deconv.cu:60-197): psi1, psi2 on the grid, quadrature for psi3
-    //    (psi1 / psi2 evaluated on the device from the quadrature: no host work
-    //    while the GPU waits)
-    double qx[MAX_QUAD], qg[MAX_QUAD];
-    int nq = quadrature_terms(gp.kp, p->win, qx, qg);
-    CU_TRY(dalloc(&p->d_foc, nchan * sizeof(double), st));
-    CU_TRY(dalloc(&p->d_quad, 2 * MAX_QUAD * sizeof(double), st));
-    CU_TRY(dalloc(&p->d_psi1, (gp.nf1 / 2 + 1) * sizeof(double), st));
-    CU_TRY(dalloc(&p->d_psi2, (gp.nf2 / 2 + 1) * sizeof(double), st));
-    CU_TRY(cudaMemcpyAsync(p->d_foc, foc.data(), nchan * sizeof(double), cudaMemcpyHostToDevice, st));
-    CU_TRY(cudaMemcpyAsync(p->d_quad, qx, nq * sizeof(double), cudaMemcpyHostToDevice, st));
-    CU_TRY(cudaMemcpyAsync(p->d_quad + MAX_QUAD, qg, nq * sizeof(double), cudaMemcpyHostToDevice, st));
-    launch_psi_grid(gp.nf1 / 2 + 1, nq, p->d_quad, p->d_quad + MAX_QUAD, p->d_psi1, st);
-    launch_psi_grid(gp.nf2 / 2 + 1, nq, p->d_quad, p->d_quad + MAX_QUAD, p->d_psi2, st);
-    if (p->win.kind == 1) {
-        CU_TRY(dalloc(&p->d_wcoef, p->win.coef.size() * sizeof(double), st));
-        CU_TRY(cudaMemcpyAsync(p->d_wcoef, p->win.coef.data(), p->win.coef.size() * sizeof(double),
-                               cudaMemcpyHostToDevice, st));
-    }
-    DevCorr &cc = p->dc;
-    cc.nx = p->nx; cc.ny = p->ny; cc.nf1 = gp.nf1; cc.nf2 = gp.nf2; cc.nf3 = gp.nf3;
-    cc.psx = gp.pixsize_x; cc.psy = gp.pixsize_y; cc.o_center = gp.o_center; cc.i_center = gp.i_center;
-    cc.gamma = gp.gamma; cc.h = gp.h; cc.nquad = nq; cc.no_w = gp.no_w;
-    cc.qx = p->d_quad; cc.qg = p->d_quad + MAX_QUAD; cc.psi1 = p->d_psi1; cc.psi2 = p->d_psi2;
-
-    // 4. binning: key per visibility (bin, start-cell residue), radix sort, bin bounds,
+    // binning: key per visibility (bin, start-cell residue), radix sort, bin bounds,
     //    sub-problem scan, records in bin order (replaces the transpose and the
     //    unsorted point order of the reference)
     const long long nb = g.nbins;
-    mark(p, EV_SET_WRANGE);
     int binbits = 1;
     while ((1LL << binbits) < nb) ++binbits;
     int cbits = binbits + 5 <= 31 ? 5 : 0;               // start-cell bank residue; bin-only keys beyond
@@ -498,8 +534,6 @@ retry_tiles:
             dfree(p->d_key_a, st); dfree(p->d_key_b, st); dfree(p->d_val_a, st); dfree(p->d_idx, st);
             dfree(p->d_bin_start, st); dfree(p->d_bin_last, st); dfree(p->d_bin_count, st);
             dfree(p->d_nsub, st); dfree(p->d_sub_end, st); dfree(p->d_tmp, st);
-            dfree(p->d_foc, st); dfree(p->d_quad, st); dfree(p->d_psi1, st); dfree(p->d_psi2, st);
-            dfree(p->d_wcoef, st);
             goto retry_tiles;
         }
         return ERR_GENERIC;
@@ -515,34 +549,19 @@ retry_tiles:
     dfree(p->d_key_b, st);
     dfree(p->d_val_a, st);
     dfree(p->d_bin_last, st);
-
-    // 5. fine grid and FFT plans
-    size_t gbytes = (size_t)gp.nf1 * gp.nf2 * gp.nf3 * 2 * esize;
-    CU_TRY(dalloc(&p->d_grid, gbytes, st));
     // TMA descriptor of the grid for the interpolator's interior tile boxes
     // ({tpitch, ty, tz} elements of 8 bytes; box edges <= 256, x starts even)
     if (p->opt.precision && g.tpitch <= 256 && g.ty <= 256 && g.tz <= 256)
         g.use_tma = encode_grid_map(p) == OK ? 1 : 0;
-
-    // 2-D transforms as two passes of contiguous rows: x rows of every plane
-    // (length nf1), and y rows (length nf2) of the image's columns only, kept
-    // transposed in d_tgrid [nf3][ny][nf2]
-    CU_TRY(dalloc(&p->d_tgrid, (size_t)gp.nf3 * p->ny * gp.nf2 * 2 * esize, st));
-    const long long nxrows = (long long)gp.nf2 * gp.nf3, nyrows = (long long)p->ny * gp.nf3;
-    p->fft_bx = (int)std::max(1LL, std::min(nxrows, (1LL << 28) / gp.nf1));
-    p->fft_bx_rest = (int)(nxrows % p->fft_bx);
-    p->fft_by = (int)std::max(1LL, std::min(nyrows, (1LL << 28) / gp.nf2));
-    p->fft_by_rest = (int)(nyrows % p->fft_by);
-    const int pr = p->opt.precision;
-    if (fft_plan1(p->device, gp.nf1, 1, gp.nf1, p->fft_bx, pr, p->st, p->fft_hx)) return ERR_CUFFT;
-    if (p->fft_bx_rest && fft_plan1(p->device, gp.nf1, 1, gp.nf1, p->fft_bx_rest, pr, p->st, p->fft_hx_rest))
-        return ERR_CUFFT;
-    if (fft_plan1(p->device, gp.nf2, 1, gp.nf2, p->fft_by, pr, p->st, p->fft_hy)) return ERR_CUFFT;
-    if (p->fft_by_rest && fft_plan1(p->device, gp.nf2, 1, gp.nf2, p->fft_by_rest, pr, p->st, p->fft_hy_rest))
-        return ERR_CUFFT;
     mark(p, EV_SET_END);
     p->ready = true;
     return OK;
+}
+
+int plan_setpts(Plan *p, long long nrow, int nchan, const double *du, const double *dv,
+                const double *dw, int stride, const double *h_freq) {
+    int s = plan_setpts_geometry(p, nrow, nchan, du, dv, dw, stride, h_freq);
+    return s != OK ? s : plan_setpts_bin(p, p->st);
 }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda).
@@ -667,7 +686,7 @@ static int execute_t(Plan *p, int type, void *d_vis, const void *d_wgt, void *d_
 
 template <typename T>
 static int execute_slabs_t(Plan *p, int type, void *d_vis, const void *d_wgt, void *d_dirty,
-                           const cudaEvent_t *ready, const cudaEvent_t *done, int nev) {
+                           const cudaEvent_t *ready, const cudaEvent_t *done, int nev, bool prologue_done) {
     cudaStream_t st = p->st;
     const GridParams &gp = p->gp;
     const int ns = p->nslab;
@@ -718,9 +737,11 @@ static int execute_slabs_t(Plan *p, int type, void *d_vis, const void *d_wgt, vo
         if ((s = plane_fft<T>(p, CUFFT_INVERSE, true))) return s;
         launch_correct_m2d<T>(p->dc, p->d_tgrid, d_dirty, st);
     } else {
-        launch_zero_tpad<T>(p->nx, p->ny, gp.nf2, gp.nf3, p->d_tgrid, st);
-        launch_correct_d2m<T>(p->dc, d_dirty, p->d_tgrid, st);
-        if ((s = plane_fft<T>(p, CUFFT_FORWARD, false))) return s;
+        if (!prologue_done) {
+            launch_zero_tpad<T>(p->nx, p->ny, gp.nf2, gp.nf3, p->d_tgrid, st);
+            launch_correct_d2m<T>(p->dc, d_dirty, p->d_tgrid, st);
+            if ((s = plane_fft<T>(p, CUFFT_FORWARD, false))) return s;
+        }
         for (int k = 0; k < ns; ++k) {
             CU_TRY(wait_slab(k));
             DevGeom gk;
@@ -737,10 +758,27 @@ static int execute_slabs_t(Plan *p, int type, void *d_vis, const void *d_wgt, vo
 }
 
 int plan_execute_slabs(Plan *p, int type, void *d_vis, const void *d_wgt, void *d_dirty,
-                       const cudaEvent_t *ready, const cudaEvent_t *done, int nev) {
+                       const cudaEvent_t *ready, const cudaEvent_t *done, int nev, bool prologue_done) {
     if (!p || !p->ready || !d_vis || !d_dirty || (type != 1 && type != 2)) return ERR_ARG;
-    return p->opt.precision ? execute_slabs_t<float>(p, type, d_vis, d_wgt, d_dirty, ready, done, nev)
-                            : execute_slabs_t<double>(p, type, d_vis, d_wgt, d_dirty, ready, done, nev);
+    return p->opt.precision
+               ? execute_slabs_t<float>(p, type, d_vis, d_wgt, d_dirty, ready, done, nev, prologue_done)
+               : execute_slabs_t<double>(p, type, d_vis, d_wgt, d_dirty, ready, done, nev, prologue_done);
+}
+
+template <typename T>
+static int d2m_prologue_t(Plan *p, const void *d_dirty) {
+    const GridParams &gp = p->gp;
+    launch_zero_tpad<T>(p->nx, p->ny, gp.nf2, gp.nf3, p->d_tgrid, p->st);
+    launch_correct_d2m<T>(p->dc, d_dirty, p->d_tgrid, p->st);
+    int s = plane_fft<T>(p, CUFFT_FORWARD, false);
+    if (s) return s;
+    CU_TRY(cudaGetLastError());
+    return OK;
+}
+
+int plan_d2m_prologue(Plan *p, const void *d_dirty) {
+    if (!p || !p->geom_ready || !d_dirty) return ERR_ARG;
+    return p->opt.precision ? d2m_prologue_t<float>(p, d_dirty) : d2m_prologue_t<double>(p, d_dirty);
 }
 
 // Error flags raised by kernels of earlier executes (an interpolator tile load

@@ -33,7 +33,8 @@ struct Plan {
     cudaStream_t st = nullptr;
     int device = 0, nsm = 148;
 
-    // set by setpts
+    // set by setpts (geometry stage, then binning stage)
+    bool geom_ready = false;
     bool ready = false;
     long long nrow = 0;
     int nchan = 0;
@@ -98,6 +99,17 @@ int plan_create(int type, int nx, int ny, double psx, double psy, double eps, do
                 const Options &opt, Plan **out);
 int plan_setpts(Plan *p, long long nrow, int nchan, const double *du, const double *dv,
                 const double *dw, int stride, const double *h_freq);
+// plan_setpts in two stages: the geometry (w range, sizes, correction tables,
+// grid buffers and FFT plans, on the plan's stream; synchronises once), then
+// tiles, binning and records on stream st.  With st not the plan's stream, st
+// must wait for the plan's stream first, and the plan's stream must wait for st
+// before anything executes.
+int plan_setpts_geometry(Plan *p, long long nrow, int nchan, const double *du, const double *dv,
+                         const double *dw, int stride, const double *h_freq);
+int plan_setpts_bin(Plan *p, cudaStream_t st);
+// dirty2ms grid preparation (corrections, per-plane screens, transforms) on
+// the plan's stream; needs only the geometry stage.
+int plan_d2m_prologue(Plan *p, const void *d_dirty);
 int plan_execute(Plan *p, void *d_vis, const void *d_wgt, void *d_dirty, int type = 0);
 // The same transform run slab by slab (the one-shot copy / compute pipeline).
 // ms2dirty: before slab k the plan's stream waits for ready[k] (the upload of
@@ -107,9 +119,10 @@ int plan_execute(Plan *p, void *d_vis, const void *d_wgt, void *d_dirty, int typ
 // (its weights) and done[k] is recorded (its rows of d_vis are final).  The
 // events describe the caller's partition of the rows into nev slabs: it must
 // equal the plan's (nev == nslab), or the plan has one slab and waits for /
-// records all of them.  Either array may be null.
+// records all of them.  Either array may be null.  prologue_done: dirty2ms
+// skips the grid preparation (already run by plan_d2m_prologue).
 int plan_execute_slabs(Plan *p, int type, void *d_vis, const void *d_wgt, void *d_dirty,
-                       const cudaEvent_t *ready, const cudaEvent_t *done, int nev);
+                       const cudaEvent_t *ready, const cudaEvent_t *done, int nev, bool prologue_done = false);
 constexpr int MAX_SLABS = 8;
 // first row of slab k of nslab over nrow rows (k = nslab gives nrow)
 inline long long slab_first_row(long long nrow, int nslab, int k) {
