@@ -874,7 +874,8 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned 
                  : "memory");
     return ok != 0;
 }
-// 3-D tiled box load (no multicast) of {x, y, z} (x in elements, x even) into dst.
+// 3-D tiled box load (no multicast) of {x, y, z} (x in 8-byte elements, x * 8
+// a multiple of 16) into dst.
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, unsigned long long *bar, int x, int y,
                                             int z) {
     asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
@@ -913,13 +914,14 @@ k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
         const int oz = g.zpad ? (int)bzi * g.bz - g.hkw : 0;
         const int shift = ox & 1, x_al = ox - shift;
         // interior tiles (no periodic wrap) in one TMA box; the rest with plain loads
-        const bool inner = sizeof(T) == 4 && g.use_tma && x_al >= 0 && x_al + g.tpitch <= g.nf1 && oy >= 0 &&
+        const bool inner = g.use_tma && x_al >= 0 && x_al + g.tpitch <= g.nf1 && oy >= 0 &&
                            oy + g.ty <= g.nf2 && (!g.zpad || (oz >= 0 && oz + g.tz <= g.nf3));
         if (inner) {
             if (threadIdx.x == 0) {
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // earlier reads of the tile
                 mbar_expect_tx(&bar, tile_bytes);
-                tma_load_3d(tile, &tmap, &bar, x_al, oy, oz);
+                // x in 8-byte elements: the cell in FP32, its real part in FP64 (16-byte aligned)
+                tma_load_3d(tile, &tmap, &bar, sizeof(T) == 4 ? x_al : 2 * x_al, oy, oz);
             }
             long long polls = 0;
             bool done = false;

@@ -23,7 +23,7 @@ struct DevGeom {
                                    // (FP64: 1 double atomics, else int64 + int32)
     int tpitch;                    // tile row pitch of the thread-per-visibility kernels: tx + 1 rounded up
                                    // to even (the interpolator's rows start at an even x for TMA)
-    int use_tma;                   // interpolator stages interior tiles with one TMA box load (FP32)
+    int use_tma;                   // interpolator stages interior tiles with one TMA box load
     int no_w;                      // w ignored: one plane, no z taps (window factor 1)
     float wmax3;                   // bound on |kx ky kz| of the tabulated window
     long long nbins;               // bins of all row slabs: nslab * nbins_slab

@@ -550,8 +550,9 @@ retry_tiles:
     dfree(p->d_val_a, st);
     dfree(p->d_bin_last, st);
     // TMA descriptor of the grid for the interpolator's interior tile boxes
-    // ({tpitch, ty, tz} elements of 8 bytes; box edges <= 256, x starts even)
-    if (p->opt.precision && g.tpitch <= 256 && g.ty <= 256 && g.tz <= 256)
+    // ({tpitch, ty, tz} cells in 8-byte elements: one per FP32 cell, two per
+    // FP64 cell; box edges <= 256 elements, x starts 16-byte aligned)
+    if (g.tpitch * (p->opt.precision ? 1 : 2) <= 256 && g.ty <= 256 && g.tz <= 256)
         g.use_tma = encode_grid_map(p) == OK ? 1 : 0;
     mark(p, EV_SET_END);
     p->ready = true;
@@ -582,9 +583,11 @@ static int encode_grid_map(Plan *p) {
     if (!enc) return ERR_UNSUPPORTED;
     const GridParams &gp = p->gp;
     const DevGeom &g = p->dg;
-    cuuint64_t dims[3] = {(cuuint64_t)gp.nf1, (cuuint64_t)gp.nf2, (cuuint64_t)gp.nf3};
-    cuuint64_t strides[2] = {(cuuint64_t)gp.nf1 * 8, (cuuint64_t)gp.nf1 * gp.nf2 * 8};
-    cuuint32_t box[3] = {(cuuint32_t)g.tpitch, (cuuint32_t)g.ty, (cuuint32_t)g.tz};
+    // 8-byte elements: one complex cell in FP32, one component in FP64 (a cell = 2 elements)
+    const int per = p->opt.precision ? 1 : 2;
+    cuuint64_t dims[3] = {(cuuint64_t)gp.nf1 * per, (cuuint64_t)gp.nf2, (cuuint64_t)gp.nf3};
+    cuuint64_t strides[2] = {(cuuint64_t)gp.nf1 * per * 8, (cuuint64_t)gp.nf1 * gp.nf2 * per * 8};
+    cuuint32_t box[3] = {(cuuint32_t)(g.tpitch * per), (cuuint32_t)g.ty, (cuuint32_t)g.tz};
     cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = enc(&p->tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, p->d_grid, dims, strides, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
