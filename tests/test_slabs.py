@@ -109,3 +109,47 @@ def test_slab_count_outside_range_is_rejected():
         st = _lib.lib.curig_ms2dirty(4, 1, 8, 8, 1e-3, 1e-3, freq.ctypes.data, uvw.ctypes.data, ms.ctypes.data,
                                      None, dirty.ctypes.data, 1e-6, 2.0, 1, ctypes.byref(opts))
         assert st == 3
+
+
+@pytest.mark.gpu
+def test_slabs_on_a_caller_stream_and_from_several_threads():
+    """Three-slab one-shot calls on a caller-supplied CUDA stream, and from four
+    host threads at once (each on its per-thread default stream): the same
+    results as one-slab calls made one after another."""
+    import threading
+
+    import torch
+    from curig_b200 import _lib
+    nx = 96
+    psx = 2.0 * np.pi / 180 / nx
+    cases = [_inputs(12007, 2, nx, "fp64", 90 + k) for k in range(4)]
+
+    def run(k, slabs, stream=None):
+        freq, uvw, ms, wgt, img = cases[k]
+        opts = _lib.make_opts(slabs=slabs, stream=stream)
+        d = np.zeros((nx, nx), dtype=np.complex128)
+        v = np.zeros_like(ms)
+        for kind, vis, dirty in ((1, ms, d), (2, v, img)):
+            f = _lib.lib.curig_ms2dirty if kind == 1 else _lib.lib.curig_dirty2ms
+            st = f(ms.shape[0], ms.shape[1], nx, nx, psx, psx, np.ascontiguousarray(freq).ctypes.data,
+                   uvw.ctypes.data, vis.ctypes.data, wgt.ctypes.data, dirty.ctypes.data, 1e-9, 2.0, -1,
+                   ctypes.byref(opts))
+            _lib.check(st, "one-shot")
+        return d, v
+
+    seq = [run(k, 1) for k in range(4)]
+    s = torch.cuda.Stream()
+    d, v = run(0, 3, s.cuda_stream)
+    assert l2err(seq[0][0], d) < 1e-12 and l2err(seq[0][1], v) < 1e-12
+    par = [None] * 4
+
+    def worker(k):
+        par[k] = run(k, 3)
+
+    threads = [threading.Thread(target=worker, args=(k,)) for k in range(4)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    for (d1, v1), (d3, v3) in zip(seq, par):
+        assert l2err(d1, d3) < 1e-12 and l2err(v1, v3) < 1e-12
