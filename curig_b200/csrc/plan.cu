@@ -57,29 +57,44 @@ static int encode_grid_map(Plan *p);
 
 // ------------------------------------------------------------------ cuFFT plan cache
 // Rank-1 batched in-place plans keyed by (device, length, element stride,
-// batch distance, batch, precision, stream, thread).  A cuFFT handle owns one
-// work area, so handles are shared only by plans whose transforms are ordered
-// on one stream: the stream is part of the key, and for the per-thread default
-// stream (one handle value naming each thread's own stream) so is the thread.
+// batch distance, batch, precision, stream, host thread).  Handles are made
+// without a work area of their own (auto-allocation off): every transform pass
+// takes one from the stream-ordered pool on the plan's stream and returns it,
+// so cached handles hold no large buffers and the pool's memory serves all of
+// them.  A handle's stream and work area are per-call state, hence one handle
+// per stream and host thread.
 namespace {
+struct FftEntry {
+    cufftHandle h;
+    size_t work;
+};
 std::mutex g_fft_mu;
-std::map<std::tuple<int, int, int, int, int, int, uintptr_t, std::thread::id>, cufftHandle> g_fft;
+std::map<std::tuple<int, int, int, int, int, int, uintptr_t, std::thread::id>, FftEntry> g_fft;
 }
 
 static int fft_plan1(int dev, int n, int stride, int dist, int batch, int prec, cudaStream_t st,
-                     cufftHandle &out) {
+                     cufftHandle &out, size_t &work) {
     std::lock_guard<std::mutex> lk(g_fft_mu);
-    const std::thread::id tid = st == cudaStreamPerThread ? std::this_thread::get_id() : std::thread::id();
-    auto key = std::make_tuple(dev, n, stride, dist, batch, prec, (uintptr_t)st, tid);
+    auto key = std::make_tuple(dev, n, stride, dist, batch, prec, (uintptr_t)st, std::this_thread::get_id());
     auto it = g_fft.find(key);
-    if (it != g_fft.end()) { out = it->second; return OK; }
+    if (it != g_fft.end()) {
+        out = it->second.h;
+        work = it->second.work;
+        return OK;
+    }
     cufftHandle h;
+    if (cufftCreate(&h) != CUFFT_SUCCESS) return ERR_CUFFT;
     int nn[1] = {n}, emb[1] = {n};
-    if (cufftPlanMany(&h, 1, nn, emb, stride, dist, emb, stride, dist, prec ? CUFFT_C2C : CUFFT_Z2Z, batch) !=
-        CUFFT_SUCCESS)
+    size_t ws = 0;
+    if (cufftSetAutoAllocation(h, 0) != CUFFT_SUCCESS ||
+        cufftMakePlanMany(h, 1, nn, emb, stride, dist, emb, stride, dist, prec ? CUFFT_C2C : CUFFT_Z2Z, batch,
+                          &ws) != CUFFT_SUCCESS) {
+        cufftDestroy(h);
         return ERR_CUFFT;
-    g_fft[key] = h;
+    }
+    g_fft[key] = FftEntry{h, ws};
     out = h;
+    work = ws;
     return OK;
 }
 
@@ -104,19 +119,23 @@ int registry_set_window(int kw, int degree, const double *coef, double eps_reach
     return OK;
 }
 
-const Window *registry_pick_window(double eps) {
+bool registry_pick_window(double eps, Window &out) {
     std::lock_guard<std::mutex> lk(g_win_mu);
     const Window *best = nullptr;
     for (auto &x : g_windows)
         if (x.eps_reached <= eps && (!best || x.kw < best->kw)) best = &x;
-    return best;
+    if (best) out = *best;                       // a copy: the registry may grow meanwhile
+    return best != nullptr;
 }
 
-const Window *registry_get_window(int kw) {
+bool registry_get_window(int kw, Window &out) {
     std::lock_guard<std::mutex> lk(g_win_mu);
     for (auto &x : g_windows)
-        if (x.kw == kw) return &x;
-    return nullptr;
+        if (x.kw == kw) {
+            out = x;
+            return true;
+        }
+    return false;
 }
 
 void registry_clear() {
@@ -348,10 +367,8 @@ int plan_setpts_geometry(Plan *p, long long nrow, int nchan, const double *du, c
     int kw_override = 0;
     p->win = Window();
     if (p->opt.window == 1) {
-        const Window *lw = registry_pick_window(p->eps);
-        if (!lw) return ERR_WINDOW;
-        p->win = *lw;
-        kw_override = lw->kw;
+        if (!registry_pick_window(p->eps, p->win)) return ERR_WINDOW;
+        kw_override = p->win.kw;
     }
     GridRequest req;
     req.grid_x = p->opt.grid_x;
@@ -401,11 +418,15 @@ int plan_setpts_geometry(Plan *p, long long nrow, int nchan, const double *du, c
     p->fft_by = (int)std::max(1LL, std::min(nyrows, (1LL << 28) / gp.nf2));
     p->fft_by_rest = (int)(nyrows % p->fft_by);
     const int pr = p->opt.precision;
-    if (fft_plan1(p->device, gp.nf1, 1, gp.nf1, p->fft_bx, pr, p->st, p->fft_hx)) return ERR_CUFFT;
-    if (p->fft_bx_rest && fft_plan1(p->device, gp.nf1, 1, gp.nf1, p->fft_bx_rest, pr, p->st, p->fft_hx_rest))
+    p->fft_hx_rest = p->fft_hy_rest = 0;
+    p->fft_wx = p->fft_wx_rest = p->fft_wy = p->fft_wy_rest = 0;
+    if (fft_plan1(p->device, gp.nf1, 1, gp.nf1, p->fft_bx, pr, p->st, p->fft_hx, p->fft_wx)) return ERR_CUFFT;
+    if (p->fft_bx_rest &&
+        fft_plan1(p->device, gp.nf1, 1, gp.nf1, p->fft_bx_rest, pr, p->st, p->fft_hx_rest, p->fft_wx_rest))
         return ERR_CUFFT;
-    if (fft_plan1(p->device, gp.nf2, 1, gp.nf2, p->fft_by, pr, p->st, p->fft_hy)) return ERR_CUFFT;
-    if (p->fft_by_rest && fft_plan1(p->device, gp.nf2, 1, gp.nf2, p->fft_by_rest, pr, p->st, p->fft_hy_rest))
+    if (fft_plan1(p->device, gp.nf2, 1, gp.nf2, p->fft_by, pr, p->st, p->fft_hy, p->fft_wy)) return ERR_CUFFT;
+    if (p->fft_by_rest &&
+        fft_plan1(p->device, gp.nf2, 1, gp.nf2, p->fft_by_rest, pr, p->st, p->fft_hy_rest, p->fft_wy_rest))
         return ERR_CUFFT;
     p->geom_ready = true;
     return OK;
@@ -608,16 +629,23 @@ static int fft_exec(Plan *p, cufftHandle h, void *base, long long offset, int di
     return r == CUFFT_SUCCESS ? OK : ERR_CUFFT;
 }
 
-// Batched contiguous row transforms of length n over nrows rows of buf.
-static int fft_rows(Plan *p, void *buf, long long nrows, int n, cufftHandle h, int b, cufftHandle h_rest,
-                    int b_rest, int dir) {
-    for (long long r = 0; r < nrows;) {
+// Batched contiguous row transforms of length n over nrows rows of buf, with
+// one work area from the stream-ordered pool for the pass.
+static int fft_rows(Plan *p, void *buf, long long nrows, int n, cufftHandle h, size_t wh, int b,
+                    cufftHandle h_rest, size_t wr, int b_rest, int dir) {
+    const size_t ws = std::max(wh, h_rest ? wr : (size_t)0);
+    void *work = nullptr;
+    if (ws) CU_TRY(cudaMallocAsync(&work, ws, p->st));
+    int s = OK;
+    if (cufftSetWorkArea(h, work) != CUFFT_SUCCESS || (h_rest && cufftSetWorkArea(h_rest, work) != CUFFT_SUCCESS))
+        s = ERR_CUFFT;
+    for (long long r = 0; s == OK && r < nrows;) {
         const bool full = nrows - r >= b;
-        int s = fft_exec(p, full ? h : h_rest, buf, r * n, dir);
-        if (s) return s;
+        s = fft_exec(p, full ? h : h_rest, buf, r * n, dir);
         r += full ? b : b_rest;
     }
-    return OK;
+    if (work) cudaFreeAsync(work, p->st);
+    return s;
 }
 
 // 2-D transform of every plane (cuft.cu:127-143) restricted to what the image
@@ -631,15 +659,19 @@ static int plane_fft(Plan *p, int dir, bool m2d) {
     const long long nx_rows = (long long)gp.nf2 * gp.nf3, ny_rows = (long long)p->ny * gp.nf3;
     int s;
     if (m2d) {
-        if ((s = fft_rows(p, p->d_grid, nx_rows, gp.nf1, p->fft_hx, p->fft_bx, p->fft_hx_rest, p->fft_bx_rest, dir)))
+        if ((s = fft_rows(p, p->d_grid, nx_rows, gp.nf1, p->fft_hx, p->fft_wx, p->fft_bx, p->fft_hx_rest, p->fft_wx_rest,
+                      p->fft_bx_rest, dir)))
             return s;
         launch_cols_to_t<T>(p->ny, gp.nf1, gp.nf2, gp.nf3, p->d_grid, p->d_tgrid, p->st);
-        return fft_rows(p, p->d_tgrid, ny_rows, gp.nf2, p->fft_hy, p->fft_by, p->fft_hy_rest, p->fft_by_rest, dir);
+        return fft_rows(p, p->d_tgrid, ny_rows, gp.nf2, p->fft_hy, p->fft_wy, p->fft_by, p->fft_hy_rest, p->fft_wy_rest,
+                      p->fft_by_rest, dir);
     }
-    if ((s = fft_rows(p, p->d_tgrid, ny_rows, gp.nf2, p->fft_hy, p->fft_by, p->fft_hy_rest, p->fft_by_rest, dir)))
+    if ((s = fft_rows(p, p->d_tgrid, ny_rows, gp.nf2, p->fft_hy, p->fft_wy, p->fft_by, p->fft_hy_rest, p->fft_wy_rest,
+                      p->fft_by_rest, dir)))
         return s;
     launch_t_to_grid<T>(p->ny, gp.nf1, gp.nf2, gp.nf3, p->d_tgrid, p->d_grid, p->st);
-    return fft_rows(p, p->d_grid, nx_rows, gp.nf1, p->fft_hx, p->fft_bx, p->fft_hx_rest, p->fft_bx_rest, dir);
+    return fft_rows(p, p->d_grid, nx_rows, gp.nf1, p->fft_hx, p->fft_wx, p->fft_bx, p->fft_hx_rest, p->fft_wx_rest,
+                      p->fft_bx_rest, dir);
 }
 
 template <typename T>

@@ -70,6 +70,7 @@ struct Plan {
 
     // x transforms on grid rows, y transforms on rows of the column-transposed planes
     cufftHandle fft_hx = 0, fft_hx_rest = 0, fft_hy = 0, fft_hy_rest = 0;
+    size_t fft_wx = 0, fft_wx_rest = 0, fft_wy = 0, fft_wy_rest = 0;      // work-area bytes
     int fft_bx = 0, fft_bx_rest = 0, fft_by = 0, fft_by_rest = 0;         // rows per call
 
     // learned-window tables per width (coefficients [kw][deg+1]); empty -> ES only
@@ -185,8 +186,8 @@ int plan_device_status(Plan *p);
 // global learned-window registry (set through the C ABI)
 int registry_set_window(int kw, int degree, const double *coef, double eps_reached);
 // smallest registered width whose reached error is <= eps (nullptr: none)
-const Window *registry_pick_window(double eps);
-const Window *registry_get_window(int kw);
+bool registry_pick_window(double eps, Window &out);   // narrowest window reaching eps
+bool registry_get_window(int kw, Window &out);
 void registry_clear();
 
 }  // namespace curig
