@@ -9,3 +9,11 @@ plan API.  Importing raises RuntimeError when the library is not built.
 from .curagridder import dirty2vis, vis2dirty  # noqa: F401
 from .cursl import dirty2ms, ms2dirty  # noqa: F401
 from .plan import DIRTY2MS, MS2DIRTY, GridderPlan  # noqa: F401
+
+
+def release_memory() -> None:
+    """Return the device memory the library keeps for its next calls (the
+    current device's stream-ordered pool) to the driver.  Call it when no
+    call or plan of the library is executing on the device."""
+    from . import _lib
+    _lib.check(_lib.lib.curig_release_memory(), "release_memory")

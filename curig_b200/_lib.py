@@ -90,6 +90,8 @@ lib.curig_clear_windows.argtypes = []
 lib.curig_clear_windows.restype = None
 lib.curig_last_error.argtypes = []
 lib.curig_last_error.restype = ctypes.c_char_p
+lib.curig_release_memory.argtypes = []
+lib.curig_release_memory.restype = c_int
 lib.curig_grid_params.argtypes = [c_int, c_int, c_double, c_double, c_double, c_double, c_double,
                                   c_double, ctypes.POINTER(c_int), ctypes.POINTER(c_double)]
 lib.curig_grid_params.restype = c_int

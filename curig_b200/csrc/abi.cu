@@ -45,6 +45,15 @@ extern "C" void curig_default_opts(curig_opts *o) {
 
 extern "C" const char *curig_last_error(void) { return g_last_error.c_str(); }
 
+extern "C" int curig_release_memory(void) {
+    int dev = 0;
+    cudaMemPool_t pool;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess ||
+        cudaMemPoolTrimTo(pool, 0) != cudaSuccess)
+        return fail(ERR_CUDA, "memory pool trim failed");
+    return OK;
+}
+
 // One call with host buffers: allocate, copy in, plan, execute, copy out, free
 // (the reference's ms2dirty_exec / dirty2ms_exec life cycle, cugridder.cu:330-582),
 // pipelined over row slabs.  A copy stream uploads uvw first (set points needs

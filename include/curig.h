@@ -215,6 +215,14 @@ int curig_nufft_destroy(curig_nufft plan);
 /* Last error text of this thread (static storage, empty if none). */
 const char *curig_last_error(void);
 
+/* Device memory: calls and plans allocate from the current device's default
+ * stream-ordered pool, which keeps freed memory for the next call (no
+ * cudaMalloc per call).  This returns the pool's unused memory to the driver,
+ * e.g. before another library needs it.  Call it when no call or plan of this
+ * library is executing on the device.  No counterpart in the reference, which
+ * allocates and frees with cudaMalloc / cudaFree in every call. */
+int curig_release_memory(void);
+
 #ifdef __cplusplus
 }
 #endif

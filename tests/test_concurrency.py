@@ -69,3 +69,19 @@ def test_one_shot_calls_from_several_threads():
         t.join()
     for a, b in zip(seq, par):
         assert l2err(a, b) < 1e-12
+
+
+@pytest.mark.gpu
+def test_release_memory_between_calls():
+    """The pool keeps freed memory for the next call; releasing it between
+    calls returns it to the driver and the next call allocates it again."""
+    import torch
+    import curig_b200 as C
+    nx = ny = 96
+    psx = 2.0 * np.pi / 180 / nx
+    freq, uvw, ms, wgt = disk_inputs(8000, 1, nx, 2.0, max_pix=40, wmax=300, seed=50)
+    a = C.ms2dirty(uvw, freq, ms, wgt, nx, ny, psx, psx, 0, 0, 1e-9, True)
+    torch.cuda.synchronize()
+    C.release_memory()
+    b = C.ms2dirty(uvw, freq, ms, wgt, nx, ny, psx, psx, 0, 0, 1e-9, True)
+    assert l2err(a, b) < 1e-12
