@@ -60,6 +60,8 @@ def args_():
     ap.add_argument("--bin", type=int, default=0, help="bin edge in cells (0 automatic)")
     ap.add_argument("--smem", type=int, default=0, help="shared-memory budget per tile CTA (bytes)")
     ap.add_argument("--sub", type=int, default=0, help="visibilities per tile chunk (0 automatic)")
+    ap.add_argument("--slabs", type=int, default=0,
+                    help="row slabs of the one-shot calls timed as e2e (0 automatic, 1..8)")
     ap.add_argument("--error-table", action="store_true",
                     help="print errors per epsilon and precision form (FP64 DFT, FP64 GPU) and exit")
     return ap.parse_args()
@@ -509,7 +511,7 @@ def main():
         h_vout = torch.empty_like(h_vis).pin_memory()
         fr = np.ascontiguousarray(freq, dtype=np.float64)
         opts = _lib.make_opts(1 if a.precision == "fp32" else 0, 1 if window == "learned" else 0,
-                              a.bin, a.sub, a.smem, stream.cuda_stream, a.accumulate)
+                              a.bin, a.sub, a.smem, stream.cuda_stream, a.accumulate, slabs=a.slabs)
 
         def e2e_step():
             s1 = _lib.lib.curig_ms2dirty(a.nrow, a.nchan, a.npix, a.npix, psx, psx, fr.ctypes.data,
@@ -543,7 +545,8 @@ def main():
         bo = h_dirty.numel() * h_dirty.element_size() + h_vout.numel() * h_vout.element_size()
         e2e = {"value": M * world / (ems / 1e3), "unit": "vis/s", "h2d_bytes_per_step": int(bi),
                "d2h_bytes_per_step": int(bo), "ms_per_step": round(ems, 3), "steps": ke,
-               "api": "curig_ms2dirty + curig_dirty2ms (C ABI, pinned host buffers)"}
+               "api": "curig_ms2dirty + curig_dirty2ms (C ABI, pinned host buffers)",
+               "slabs": a.slabs or "automatic"}
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
