@@ -27,6 +27,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -98,12 +99,12 @@ class Clocks:
 
     def __init__(self, index):
         self.index = index
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        fd, self.path = tempfile.mkstemp(prefix="curig_clocks_", suffix=".csv")
+        os.close(fd)
         self.p = None
 
     def __enter__(self):
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
             self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
                                        "--format=csv,noheader,nounits", "-lms", "100"],
@@ -126,6 +127,11 @@ class Clocks:
             rows = [l.split(",") for l in open(self.path).read().strip().splitlines() if l.strip()]
         except Exception:
             return None
+        finally:
+            try:
+                os.unlink(self.path)
+            except OSError:
+                pass
         if not rows:
             return None
         sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]

@@ -118,6 +118,8 @@ lib.curig_nufft_execute.restype = c_int
 lib.curig_nufft_destroy.argtypes = [c_void_p]
 lib.curig_nufft_destroy.restype = c_int
 lib.curig_default_opts.restype = None
+lib.curig_test_tile_wait.argtypes = [c_int64, c_int]
+lib.curig_test_tile_wait.restype = None
 
 ERRORS = {
     1: "generic error", 2: "bad upsampling factor", 3: "invalid argument", 4: "CUDA error",

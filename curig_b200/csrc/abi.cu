@@ -51,6 +51,7 @@ extern "C" int curig_release_memory(void) {
     if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess ||
         cudaMemPoolTrimTo(pool, 0) != cudaSuccess)
         return fail(ERR_CUDA, "memory pool trim failed");
+    fft_cache_trim();
     return OK;
 }
 
@@ -357,6 +358,8 @@ extern "C" int curig_plan_timings(curig_plan h, double *out, int n) {
 }
 
 extern "C" int64_t curig_launch_count(void) { return launch_count(); }
+
+extern "C" void curig_test_tile_wait(int64_t polls, int noissue) { set_tile_wait(polls, noissue); }
 
 extern "C" int curig_destroy(curig_plan h) {
     if (!h) return OK;

@@ -882,7 +882,6 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
                  ::"r"(smem_addr(dst)), "l"(map), "r"(smem_addr(bar)), "r"(x), "r"(y), "r"(z)
                  : "memory");
 }
-constexpr long long TMA_WAIT_LIMIT = 1LL << 26;   // try_wait polls (seconds): then the error flag
 
 template <typename T, int KW>
 __global__ void __launch_bounds__(interp_threads<T>(), sizeof(T) == 4 ? 3 : 2)
@@ -921,11 +920,11 @@ k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // earlier reads of the tile
                 mbar_expect_tx(&bar, tile_bytes);
                 // x in 8-byte elements: the cell in FP32, its real part in FP64 (16-byte aligned)
-                tma_load_3d(tile, &tmap, &bar, sizeof(T) == 4 ? x_al : 2 * x_al, oy, oz);
+                if (!g.tma_test_noissue) tma_load_3d(tile, &tmap, &bar, sizeof(T) == 4 ? x_al : 2 * x_al, oy, oz);
             }
             long long polls = 0;
             bool done = false;
-            while (!(done = mbar_try_wait(&bar, parity)) && ++polls < TMA_WAIT_LIMIT) {
+            while (!(done = mbar_try_wait(&bar, parity)) && ++polls < g.tma_polls) {
             }
             parity ^= 1u;
             if (__syncthreads_or(!done)) {          // the load never completed: flag it and stop

@@ -24,6 +24,8 @@ struct DevGeom {
     int tpitch;                    // tile row pitch of the thread-per-visibility kernels: tx + 1 rounded up
                                    // to even (the interpolator's rows start at an even x for TMA)
     int use_tma;                   // interpolator stages interior tiles with one TMA box load
+    long long tma_polls;           // polls of a tile load's barrier before the load counts as lost
+    int tma_test_noissue;          // test only: arm the barrier but issue no load (the wait runs out)
     int no_w;                      // w ignored: one plane, no z taps (window factor 1)
     float wmax3;                   // bound on |kx ky kz| of the tabulated window
     long long nbins;               // bins of all row slabs: nslab * nbins_slab

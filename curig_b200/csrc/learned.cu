@@ -16,8 +16,10 @@
 
 #include "../../include/curig.h"
 
+#include <atomic>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 namespace curig {
@@ -381,17 +383,33 @@ namespace curig {
 constexpr size_t WSCRATCH_BYTES = 64 * 1024;
 static __device__ __align__(256) unsigned char g_window_scratch[WSCRATCH_BYTES];
 
+// Device address of g_window_scratch on the current device, looked up once per
+// device (std::call_once: threads making their first call on one device at the
+// same time wait for a single lookup).  A failed lookup is retried on the next
+// call.  The cached address belongs to the device's current context: after
+// cudaDeviceReset the module is loaded again and this cache is stale, so a
+// process that resets a device must not call this entry point afterwards.
+constexpr int MAX_DEVICES = 64;
+static std::once_flag g_scratch_once[MAX_DEVICES];
+static std::atomic<void *> g_scratch_addr[MAX_DEVICES];
+static std::mutex g_scratch_retry;
+
 static void *window_scratch_ptr(int &status) {
-    static void *addr[64] = {nullptr};
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) { status = ERR_CUDA; return nullptr; }
-    if (!addr[dev]) {
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) { status = ERR_CUDA; return nullptr; }
+    std::call_once(g_scratch_once[dev], [dev] {
         void *p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_window_scratch) != cudaSuccess || !p) { status = ERR_CUDA; return nullptr; }
-        addr[dev] = p;
+        if (cudaGetSymbolAddress(&p, g_window_scratch) == cudaSuccess) g_scratch_addr[dev].store(p);
+    });
+    void *p = g_scratch_addr[dev].load();
+    if (!p) {                                     // the first lookup failed: try again, serialised
+        std::lock_guard<std::mutex> lk(g_scratch_retry);
+        if (!g_scratch_addr[dev].load() && cudaGetSymbolAddress(&p, g_window_scratch) == cudaSuccess)
+            g_scratch_addr[dev].store(p);
+        p = g_scratch_addr[dev].load();
     }
-    status = OK;
-    return addr[dev];
+    status = p ? OK : ERR_CUDA;
+    return p;
 }
 
 }  // namespace curig

@@ -62,22 +62,32 @@ static int encode_grid_map(Plan *p);
 // takes one from the stream-ordered pool on the plan's stream and returns it,
 // so cached handles hold no large buffers and the pool's memory serves all of
 // them.  A handle's stream and work area are per-call state, hence one handle
-// per stream and host thread.
+// per stream and host thread.  Plans hold references to the handles they use;
+// released handles stay cached for the next plan of the same shape, at most
+// FFT_KEEP of them (least recently released destroyed first), and
+// fft_cache_trim (called by curig_release_memory) destroys all of them.
 namespace {
 struct FftEntry {
     cufftHandle h;
     size_t work;
+    int refs;
+    unsigned long long released;   // release tick, for the least-recently-released eviction
 };
+using FftKey = std::tuple<int, int, int, int, int, int, uintptr_t, std::thread::id>;
 std::mutex g_fft_mu;
-std::map<std::tuple<int, int, int, int, int, int, uintptr_t, std::thread::id>, FftEntry> g_fft;
+std::map<FftKey, FftEntry> g_fft;
+unsigned long long g_fft_tick = 0;
+constexpr int FFT_KEEP = 16;
 }
 
-static int fft_plan1(int dev, int n, int stride, int dist, int batch, int prec, cudaStream_t st,
-                     cufftHandle &out, size_t &work) {
+static int fft_plan1(Plan *p, int n, int stride, int dist, int batch, int prec, cufftHandle &out, size_t &work) {
     std::lock_guard<std::mutex> lk(g_fft_mu);
-    auto key = std::make_tuple(dev, n, stride, dist, batch, prec, (uintptr_t)st, std::this_thread::get_id());
+    FftKey key = std::make_tuple(p->device, n, stride, dist, batch, prec, (uintptr_t)p->st,
+                                 std::this_thread::get_id());
     auto it = g_fft.find(key);
     if (it != g_fft.end()) {
+        ++it->second.refs;
+        p->fft_keys.push_back(key);
         out = it->second.h;
         work = it->second.work;
         return OK;
@@ -92,10 +102,53 @@ static int fft_plan1(int dev, int n, int stride, int dist, int batch, int prec, 
         cufftDestroy(h);
         return ERR_CUFFT;
     }
-    g_fft[key] = FftEntry{h, ws};
+    g_fft[key] = FftEntry{h, ws, 1, 0};
+    p->fft_keys.push_back(key);
     out = h;
     work = ws;
     return OK;
+}
+
+// Drop the plan's references; keep at most FFT_KEEP unreferenced handles.
+static void fft_release(Plan *p) {
+    std::lock_guard<std::mutex> lk(g_fft_mu);
+    for (const FftKey &k : p->fft_keys) {
+        auto it = g_fft.find(k);
+        if (it != g_fft.end() && it->second.refs > 0 && --it->second.refs == 0) it->second.released = ++g_fft_tick;
+    }
+    p->fft_keys.clear();
+    for (;;) {
+        int idle = 0;
+        auto oldest = g_fft.end();
+        for (auto it = g_fft.begin(); it != g_fft.end(); ++it)
+            if (it->second.refs == 0) {
+                ++idle;
+                if (oldest == g_fft.end() || it->second.released < oldest->second.released) oldest = it;
+            }
+        if (idle <= FFT_KEEP) break;
+        cufftDestroy(oldest->second.h);
+        g_fft.erase(oldest);
+    }
+}
+
+int fft_cache_trim() {
+    std::lock_guard<std::mutex> lk(g_fft_mu);
+    int n = 0;
+    for (auto it = g_fft.begin(); it != g_fft.end();) {
+        if (it->second.refs == 0) {
+            cufftDestroy(it->second.h);
+            it = g_fft.erase(it);
+            ++n;
+        } else {
+            ++it;
+        }
+    }
+    return n;
+}
+
+int fft_cache_size() {
+    std::lock_guard<std::mutex> lk(g_fft_mu);
+    return (int)g_fft.size();
 }
 
 // ------------------------------------------------------------------ learned-window registry
@@ -178,6 +231,20 @@ int plan_timings(Plan *p, double *out, int n) {
     return OK;
 }
 
+// ------------------------------------------------------------------ tile-load wait
+// Polls of the interpolator's tile-load barrier before it gives up (about a
+// second at the default); a test can shorten it and suppress the load so that
+// the wait runs out on purpose (nothing is in flight when the CTA leaves).
+namespace {
+std::atomic<long long> g_tma_polls{DEFAULT_TMA_POLLS};
+std::atomic<int> g_tma_noissue{0};
+}
+
+void set_tile_wait(long long polls, int noissue) {
+    g_tma_polls.store(polls > 0 ? polls : DEFAULT_TMA_POLLS);
+    g_tma_noissue.store(noissue ? 1 : 0);
+}
+
 // ------------------------------------------------------------------ plan
 int plan_create(int type, int nx, int ny, double psx, double psy, double eps, double sigma, int sign,
                 const Options &opt, Plan **out) {
@@ -219,6 +286,8 @@ void plan_release_points(Plan *p) {
     dfree(p->d_val_a, st); dfree(p->d_idx, st); dfree(p->d_err, st); dfree(p->d_keys, st);
     dfree(p->d_rec, st); dfree(p->d_ph, st); dfree(p->d_cs, st); dfree(p->d_grid, st); dfree(p->d_tmp, st);
     dfree(p->d_tgrid, st);
+    fft_release(p);
+    p->fft_hx = p->fft_hx_rest = p->fft_hy = p->fft_hy_rest = 0;
     p->ready = false;
     p->geom_ready = false;
 }
@@ -420,13 +489,13 @@ int plan_setpts_geometry(Plan *p, long long nrow, int nchan, const double *du, c
     const int pr = p->opt.precision;
     p->fft_hx_rest = p->fft_hy_rest = 0;
     p->fft_wx = p->fft_wx_rest = p->fft_wy = p->fft_wy_rest = 0;
-    if (fft_plan1(p->device, gp.nf1, 1, gp.nf1, p->fft_bx, pr, p->st, p->fft_hx, p->fft_wx)) return ERR_CUFFT;
+    if (fft_plan1(p, gp.nf1, 1, gp.nf1, p->fft_bx, pr, p->fft_hx, p->fft_wx)) return ERR_CUFFT;
     if (p->fft_bx_rest &&
-        fft_plan1(p->device, gp.nf1, 1, gp.nf1, p->fft_bx_rest, pr, p->st, p->fft_hx_rest, p->fft_wx_rest))
+        fft_plan1(p, gp.nf1, 1, gp.nf1, p->fft_bx_rest, pr, p->fft_hx_rest, p->fft_wx_rest))
         return ERR_CUFFT;
-    if (fft_plan1(p->device, gp.nf2, 1, gp.nf2, p->fft_by, pr, p->st, p->fft_hy, p->fft_wy)) return ERR_CUFFT;
+    if (fft_plan1(p, gp.nf2, 1, gp.nf2, p->fft_by, pr, p->fft_hy, p->fft_wy)) return ERR_CUFFT;
     if (p->fft_by_rest &&
-        fft_plan1(p->device, gp.nf2, 1, gp.nf2, p->fft_by_rest, pr, p->st, p->fft_hy_rest, p->fft_wy_rest))
+        fft_plan1(p, gp.nf2, 1, gp.nf2, p->fft_by_rest, pr, p->fft_hy_rest, p->fft_wy_rest))
         return ERR_CUFFT;
     p->geom_ready = true;
     return OK;
@@ -465,6 +534,8 @@ retry_tiles:
     g.tx = tg.tx; g.ty = tg.ty; g.tz = tg.tz; g.zpad = tg.zpad; g.sub = tg.sub;
     g.tpitch = (tg.tx + 2) & ~1;
     g.use_tma = 0;                          // set once the grid's TMA descriptor exists
+    g.tma_polls = g_tma_polls.load();
+    g.tma_test_noissue = g_tma_noissue.load();
     // row slabs (tile kernels only): bins of slab k are k * nbins_slab + bin
     int nslab = std::max(1, std::min(p->opt.slabs, MAX_SLABS));
     if (g.kw > TAB_KW || nrow < nslab || (long long)nslab * tg.nbins() > INT_MAX / 2) nslab = 1;

@@ -4,7 +4,11 @@
 #include "curig_internal.h"
 #include "kernels.cuh"
 
+#include <cstdint>
 #include <string>
+#include <thread>
+#include <tuple>
+#include <vector>
 
 namespace curig {
 
@@ -72,6 +76,9 @@ struct Plan {
     cufftHandle fft_hx = 0, fft_hx_rest = 0, fft_hy = 0, fft_hy_rest = 0;
     size_t fft_wx = 0, fft_wx_rest = 0, fft_wy = 0, fft_wy_rest = 0;      // work-area bytes
     int fft_bx = 0, fft_bx_rest = 0, fft_by = 0, fft_by_rest = 0;         // rows per call
+
+    // cuFFT cache entries this plan holds a reference to (released with its points)
+    std::vector<std::tuple<int, int, int, int, int, int, uintptr_t, std::thread::id>> fft_keys;
 
     // learned-window tables per width (coefficients [kw][deg+1]); empty -> ES only
     std::vector<Window> learned;
@@ -182,6 +189,14 @@ void launch_psi_grid(int n, int nq, const double *qx, const double *qg, double *
 void launch_nupts_uvw(long long m, const double *x, const double *y, double s, double *uvw, cudaStream_t st);
 
 int plan_device_status(Plan *p);
+// Bound on the polls of the interpolator's tile-load wait for plans whose
+// points are set afterwards (polls <= 0: the default); noissue != 0 makes the
+// tile loads not happen, for tests of the timeout path.
+constexpr long long DEFAULT_TMA_POLLS = 1LL << 26;
+void set_tile_wait(long long polls, int noissue);
+// destroy the cached cuFFT handles no plan holds (returns how many); number cached
+int fft_cache_trim();
+int fft_cache_size();
 
 // global learned-window registry (set through the C ABI)
 int registry_set_window(int kw, int degree, const double *coef, double eps_reached);

@@ -11,7 +11,7 @@ window="learned" uses the narrowest registered width whose error reaches the
 requested epsilon, and windows are registered only through this module.
 
 Trained parameters for sigma = 2 ship in curig_b200/windows/learned_sigma2.json
-(written by curig_b200/windows/train_windows.py on a B200).
+(written by oracle/train_windows.py on a B200).
 """
 from __future__ import annotations
 

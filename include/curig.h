@@ -161,8 +161,10 @@ int curig_window_table(int W, double sigma, const float *params, int degree, dou
  * device memory is reserved up front by another framework's pool, or their
  * pipeline forbids allocation after initialisation).  Its scratch lives in one
  * 64 KiB file-scope device array that every GPU loading the library holds until
- * exit; the array's device address is looked up on the first call with a
- * device current, so make that first call before any stream capture.  Calls
+ * exit; the array's device address is looked up once per device, on the first
+ * call with that device current, so make that first call before any stream
+ * capture (and do not call it again on a device after cudaDeviceReset, which
+ * reloads the module at a new address).  Calls
  * share the array: calls that overlap on the GPU race.  W above 12 is rejected
  * (status 3).  params, loss and grad are host pointers.  No counterpart in the
  * reference. */
@@ -196,6 +198,15 @@ void curig_set_timing(int on);
 int curig_plan_timings(curig_plan plan, double *out, int n);
 int64_t curig_launch_count(void);
 
+/* Test hook for the interpolator's bounded wait on its TMA tile loads: plans
+ * whose points are set after this call poll a load's barrier at most `polls`
+ * times (<= 0: the default, about a second) before raising the error that the
+ * one-shot calls report as status 4 ("a tile load did not complete (timed
+ * out)").  noissue != 0 arms the barrier without issuing the load, so the wait
+ * runs out with nothing in flight; (0, 0) restores normal operation.  No
+ * counterpart in the reference, which has no bounded waits. */
+void curig_test_tile_wait(int64_t polls, int noissue);
+
 /* Generic NUFFT, types 1 (points -> modes) and 2 (modes -> points) in one or two
  * dimensions, on the w-free gridder (same kernel-width, grid-size and correction
  * rules as the gridder; takes the place of the reference's cunufft_setting /
@@ -218,9 +229,12 @@ const char *curig_last_error(void);
 /* Device memory: calls and plans allocate from the current device's default
  * stream-ordered pool, which keeps freed memory for the next call (no
  * cudaMalloc per call).  This returns the pool's unused memory to the driver,
- * e.g. before another library needs it.  Call it when no call or plan of this
- * library is executing on the device.  No counterpart in the reference, which
- * allocates and frees with cudaMalloc / cudaFree in every call. */
+ * e.g. before another library needs it, and destroys the cached cuFFT
+ * handles that no live plan holds (at most 16 such handles are kept between
+ * calls; the rest are destroyed when released).  Call it when no call or plan
+ * of this library is executing on the device.  No counterpart in the
+ * reference, which allocates and frees with cudaMalloc / cudaFree in every
+ * call. */
 int curig_release_memory(void);
 
 #ifdef __cplusplus

@@ -4,7 +4,9 @@
 oracle/_build/liboracle_dft.so, and -- when the reference sources are present
 in this container -- the reference library itself into oracle/_ref/ via
 oracle/Makefile.ref.  Both outputs are git-ignored; they travel to GPU boxes
-with the working tree.
+with the working tree.  The reference source tree is taken from the
+CURIG_REFERENCE environment variable (default: the read-only checkout this
+recipe was written against).
 """
 from __future__ import annotations
 
@@ -14,7 +16,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 BUILD = os.path.join(HERE, "_build")
-REF_SRC = "/root/reference"
+REF_SRC = os.environ.get("CURIG_REFERENCE", "/root/reference")
 
 
 def build_dft(force: bool = False) -> str:

@@ -1,6 +1,6 @@
 """Train the learned windows on the GPU and record their measured accuracy.
 
-    python curig_b200/windows/train_windows.py [out.json] [--iters N]
+    python oracle/train_windows.py [out.json] [--iters N]
 
 For each support width W (sigma = 2) the MLP window is trained by the
 library's own kernels (curig_train_window), tabulated, and its error measured
@@ -9,6 +9,8 @@ with w-stacking against the exact FP64 DFT (oracle/dft.c, used here only as the
 checker).  The ES window of the same width is measured on the same problem.
 The output JSON holds the trained parameters and eps_reached (the measured
 learned error) per width; curig_b200.learned.load_default_windows() reads it.
+The recipe lives beside the oracle, not in the package: the package never
+imports the oracle.
 """
 from __future__ import annotations
 
@@ -20,7 +22,7 @@ import time
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-ROOT = os.path.dirname(os.path.dirname(HERE))
+ROOT = os.path.dirname(HERE)
 sys.path.insert(0, ROOT)
 
 

@@ -75,3 +75,47 @@ def disk_inputs(nrow, nchan, nx, fov_deg, f0=1.0e9, fmax=None, max_pix=120.0, wm
     ms = rng.standard_normal((nrow, nchan)) + 1j * rng.standard_normal((nrow, nchan))
     wgt = (1.0 - rng.random((nrow, nchan))) * 0.5 + 0.5
     return freq, uvw, ms, wgt
+
+
+def gaussian_uv_inputs(nrow, nchan=16, npix=4096, fov_deg=3.0, seed=0, fmin=0.9e9, fmax=1.1e9, wmax=1000.0):
+    """The 4096^2 configuration's visibilities, drawn with numpy (the same
+    values on every machine with this numpy): channels linear in
+    [fmin, fmax]; (u, v) from an isotropic Gaussian of sigma = 0.3 R, draws
+    beyond R drawn again, R * fov / lambda_min = 0.47 npix pixels; w uniform
+    in +-wmax metres; complex-normal visibilities [nrow][nchan]; weights
+    uniform in (0.5, 1]."""
+    rng = np.random.default_rng(seed)
+    freq = np.linspace(fmin, fmax, nchan) if nchan > 1 else np.array([1.0e9])
+    R = 0.47 * npix * (SPEEDOFLIGHT / freq.max()) / (fov_deg * np.pi / 180)
+    uv = rng.standard_normal((nrow, 2)) * (0.3 * R)
+    for _ in range(64):
+        bad = np.flatnonzero((uv * uv).sum(1) > R * R)
+        if bad.size == 0:
+            break
+        uv[bad] = rng.standard_normal((bad.size, 2)) * (0.3 * R)
+    w = rng.uniform(-wmax, wmax, (nrow, 1))
+    uvw = np.ascontiguousarray(np.concatenate([uv, w], 1))
+    vis = np.empty((nrow, nchan), dtype=np.complex128)
+    vis.real = rng.standard_normal((nrow, nchan))
+    vis.imag = rng.standard_normal((nrow, nchan))
+    wgt = 1.0 - 0.5 * rng.random((nrow, nchan))
+    return freq, uvw, vis, wgt
+
+
+def gaussian_image(npix, seed=1):
+    """Complex-normal dirty image [npix][npix] (numpy, seeded)."""
+    rng = np.random.default_rng(seed)
+    img = np.empty((npix, npix), dtype=np.complex128)
+    img.real = rng.standard_normal((npix, npix))
+    img.imag = rng.standard_normal((npix, npix))
+    return img
+
+
+def input_checksum(*arrays):
+    """Order-sensitive checksum of the inputs (detects a change of generator)."""
+    s = 0.0
+    for a in arrays:
+        f = np.ascontiguousarray(a).view(np.float64).reshape(-1)
+        k = np.arange(1, f.size + 1, dtype=np.float64) % 997.0
+        s += float(np.dot(f, k))
+    return s

@@ -1,7 +1,7 @@
 """Generate golden vectors from the reference's own Python truth functions.
 
 Run here (the reference tree is only needed at generation time):
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <reference source tree>
 
 The reference's test modules import its ctypes library at module level and run
 tests on import, so the truth functions are taken out of the source with
@@ -88,4 +88,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) < 2 and not os.environ.get("CURIG_REFERENCE"):
+        sys.exit("usage: make_golden.py <reference source tree> (or set CURIG_REFERENCE)")
+    main(sys.argv[1] if len(sys.argv) > 1 else os.environ["CURIG_REFERENCE"])

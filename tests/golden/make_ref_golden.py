@@ -8,7 +8,7 @@ _1 forms) on seeded inputs, and writes reflib_*.npz (inputs + outputs) to the
 directory given on the command line.  The files are then committed under
 tests/golden/ and pin both the oracle's NUFFT restatement and the product.
 
-    python tests/golden/make_ref_golden.py gpurun_out/golden
+    python tests/golden/make_ref_golden.py <output directory>
 """
 from __future__ import annotations
 
@@ -91,4 +91,6 @@ def main(outdir):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "golden"))
+    if len(sys.argv) < 2:
+        sys.exit("usage: make_ref_golden.py <output directory>")
+    main(sys.argv[1])

@@ -128,3 +128,21 @@ def test_oracle_nufft_matches_reference_library(path):
     v = nufft.dirty2ms(g["uvw"], g["freq"], g["dirty"], wgt, *args)
     assert l2err(g["ms2dirty"], d) < 1e-11
     assert l2err(g["dirty2ms"], v) < 1e-11
+
+
+@pytest.mark.parametrize("nchan,sign,use_wgt", [(1, -1, True), (3, 1, False), (4, -1, True)])
+def test_torch_dft_matches_c_oracle(nchan, sign, use_wgt):
+    """oracle/dft_torch.py (the size-scale checker) against oracle/dft.c, on the CPU."""
+    from oracle import dft_torch
+    freq, uvw, ms, dirty, wgt = wst_inputs(150, nchan, 48, 40, 10.0, wgt=use_wgt)
+    psx, psy = 10 * np.pi / 180 / 48, 10 * np.pi / 180 / 40
+    rng = np.random.default_rng(1)
+    pix = rng.integers(0, 48 * 40, 300)
+    ref = dft.ms2dirty_dft(uvw, freq, ms, wgt, 48, 40, psx, psy, sign, pix=pix)
+    got = dft_torch.ms2dirty_dft(uvw, freq, ms, wgt, 48, 40, psx, psy, sign, pix, chunk=64)
+    assert l2err(ref, got) < 1e-12
+    d = dirty + 1j * rng.standard_normal(dirty.shape)
+    idx = rng.integers(0, 150 * nchan, 200)
+    ref = dft.dirty2ms_dft(uvw, freq, d, wgt, psx, psy, sign, idx=idx)
+    got = dft_torch.dirty2ms_dft(uvw, freq, d, wgt, psx, psy, sign, idx, chunk=500)
+    assert l2err(ref, got) < 1e-12

@@ -31,6 +31,37 @@ def test_static_scratch_entry_matches_allocating_entry():
         assert np.linalg.norm(g - g_ref) <= 1e-5 * np.linalg.norm(g_ref)
 
 
+def _pool_reserved():
+    """Bytes the device's default stream-ordered pool holds (cudaMallocAsync's source)."""
+    import torch
+    from cuda.bindings import runtime as rt
+    err, pool = rt.cudaDeviceGetDefaultMemPool(torch.cuda.current_device())
+    assert err == rt.cudaError_t.cudaSuccess
+    err, v = rt.cudaMemPoolGetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrReservedMemCurrent)
+    assert err == rt.cudaError_t.cudaSuccess
+    return int(v)
+
+
+def test_static_scratch_entry_allocates_no_device_memory():
+    """After one warm-up call (which loads the module and its static array),
+    repeated calls change neither the device's free memory (a cudaMalloc takes
+    at least a 2 MiB page) nor the default pool's reservation (cudaMallocAsync)."""
+    import torch
+    from curig_b200 import _lib, learned
+    lib = _lib.lib
+    p = learned.init_params(3)
+    assert _static(lib, 6, p)[0] == 0
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    pool0 = _pool_reserved()
+    for W in (6, 5, 8):
+        assert _static(lib, W, p)[0] == 0, lib.curig_last_error()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert _pool_reserved() == pool0
+    assert free1 >= free0 - (1 << 20), (free0, free1)
+
+
 def test_static_scratch_entry_rejects_oversize():
     from curig_b200 import _lib, learned
     p = learned.init_params(0)
