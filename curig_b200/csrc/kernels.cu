@@ -15,8 +15,6 @@
 #include "kernels.cuh"
 #include "plan.h"
 
-#include <cub/cub.cuh>
-
 namespace curig {
 
 template <typename T> using C = typename cplx_t<T>::type;
@@ -83,17 +81,25 @@ __device__ __forceinline__ double w_eff(const DevGeom &g, const double *__restri
 }
 
 // Periodic wrap into [0, nf), start cell ceil(g - kw/2), offset u = start-g+kw/2
-// in [0,1), bin index and start relative to the bin's tile origin.
-__device__ __forceinline__ void axis_loc(double gc, int nf, int B, int nb, int hkw, int kw, int &bin,
-                                         int &lstart, double &u) {
-    double gw = gc - (double)nf * floor(gc / (double)nf);
-    if (gw >= (double)nf) gw -= (double)nf;
-    if (gw < 0.0) gw = 0.0;
+// in [0,1), bin index and start relative to the bin's tile origin.  Points
+// already inside [0, nf) (all of them unless |u| pixsize reaches 1/2) skip the
+// wrap's division; the bin index is floor(gw / B) from a multiply by 1/B,
+// corrected by exact integer comparisons.
+__device__ __forceinline__ void axis_loc(double gc, int nf, int B, double invB, int nb, int hkw, int kw,
+                                         int &bin, int &lstart, double &u) {
+    double gw = gc;
+    if (!(gc >= 0.0 && gc < (double)nf)) {
+        gw = gc - (double)nf * floor(gc / (double)nf);
+        if (gw >= (double)nf) gw -= (double)nf;
+        if (gw < 0.0) gw = 0.0;
+    }
     double sd = ceil(gw - 0.5 * kw);
     u = (sd - gw) + 0.5 * kw;
     if (u < 0.0) u = 0.0;
     if (u >= 1.0) u = 0.99999999999999989;
-    bin = (int)(gw / (double)B);
+    bin = (int)(gw * invB);
+    if ((double)(bin + 1) * B <= gw) ++bin;
+    else if ((double)bin * B > gw) --bin;
     if (bin >= nb) bin = nb - 1;
     lstart = (int)sd - (bin * B - hkw);
 }
@@ -106,14 +112,14 @@ struct VisLoc {
 
 __device__ __forceinline__ int locate(const DevGeom &g, double gx, double gy, double gz, VisLoc &L) {
     int bxi, byi, bzi;
-    axis_loc(gx, g.nf1, g.bx, g.nbx, g.hkw, g.kw, bxi, L.lx, L.ux);
-    axis_loc(gy, g.nf2, g.by, g.nby, g.hkw, g.kw, byi, L.ly, L.uy);
+    axis_loc(gx, g.nf1, g.bx, g.ibx, g.nbx, g.hkw, g.kw, bxi, L.lx, L.ux);
+    axis_loc(gy, g.nf2, g.by, g.iby, g.nby, g.hkw, g.kw, byi, L.ly, L.uy);
     if (g.no_w) {                                  // one plane, no z taps
         L.lz = 0;
         L.uz = 0.0;
         bzi = 0;
     } else if (g.zpad) {
-        axis_loc(gz, g.nf3, g.bz, g.nbz, g.hkw, g.kw, bzi, L.lz, L.uz);
+        axis_loc(gz, g.nf3, g.bz, g.ibz, g.nbz, g.hkw, g.kw, bzi, L.lz, L.uz);
     } else {
         double sd = ceil(gz - 0.5 * g.kw);
         double u = (sd - gz) + 0.5 * g.kw;
@@ -156,59 +162,190 @@ __global__ void k_wrange(const double *__restrict__ w, int stride, long long nro
     }
 }
 
-// ------------------------------------------------------------------ binning
+// ------------------------------------------------------------------ binning (counting sort)
 // Sort key of one visibility: bin id in the high bits, then the residue mod 32
 // of its start cell's index in the tile (the shared-memory bank of its first
-// tap); the radix sort is stable, so equal keys keep input order.  With row
-// slabs the bin id is slab * nbins_slab + bin (slab = row * nslab / nrow), so
-// each slab's visibilities are contiguous in sorted order.  0xffffffff marks a
-// visibility that could not be placed.
-__global__ void k_bin_keys(DevGeom g, const double *__restrict__ uu, const double *__restrict__ vv,
-                           const double *__restrict__ ww, const double *__restrict__ foc,
-                           unsigned *__restrict__ keys, int *__restrict__ vals, int *err) {
+// tap).  With row slabs the bin id is slab * nbins_slab + bin (slab = row *
+// nslab / nrow), so each slab's visibilities are contiguous in sorted order.
+// BAD_KEY marks a visibility that could not be placed.
+//
+// The sort is a counting sort over the key values (at most 2^31 of them):
+// k_bin_count counts every key, an exclusive scan turns the counts into each
+// key's first sorted position, and k_bin_scatter claims positions with atomics
+// and writes the input index there.  Sorted order is bin-major and, inside a
+// bin, residue-major; the order of visibilities that share a key is whatever
+// order their atomics ran in (nothing downstream depends on it beyond the last
+// bits of FP32 sums, whose flush order is free anyway).  Lanes of a warp with
+// equal keys (neighbouring channels of one row often share a cell) are merged
+// with __match_any_sync into one atomic.
+constexpr unsigned BAD_KEY = 0xffffffffu;
+
+__device__ __forceinline__ unsigned vis_key(const DevGeom &g, const double *__restrict__ uu,
+                                            const double *__restrict__ vv, const double *__restrict__ ww,
+                                            const double *__restrict__ foc, long long j, int &e) {
+    const long long row = j / g.nchan;
+    const int ch = (int)(j - row * g.nchan);
+    double gx, gy, gz;
+    VisLoc L;
+    e = vis_grid(g, uu, vv, ww, row, foc[ch], gx, gy, gz) ? locate(g, gx, gy, gz, L) : EF_NONFINITE;
+    if (e) return BAD_KEY;
+    const unsigned cell = g.cbits ? (unsigned)((L.lz * g.ty + L.ly) * g.tpitch + L.lx) & 31u : 0u;
+    const long long slab = g.nslab > 1 ? row * g.nslab / g.nrow : 0;
+    return ((unsigned)(slab * g.nbins_slab + L.bin) << g.cbits) | cell;
+}
+
+// keys[j] for every visibility (input order) and count[key] += 1.
+__global__ void k_bin_count(DevGeom g, const double *__restrict__ uu, const double *__restrict__ vv,
+                            const double *__restrict__ ww, const double *__restrict__ foc,
+                            unsigned *__restrict__ keys, int *__restrict__ count, int *err) {
     const long long M = g.nrow * g.nchan;
-    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < M;
-         j += (long long)gridDim.x * blockDim.x) {
-        long long row = j / g.nchan;
-        int ch = (int)(j - row * g.nchan);
-        double gx, gy, gz;
-        VisLoc L;
-        int e = vis_grid(g, uu, vv, ww, row, foc[ch], gx, gy, gz) ? locate(g, gx, gy, gz, L)
-                                                                  : EF_NONFINITE;
-        unsigned key = 0xffffffffu;
-        if (e) {
-            atomicOr(err, e);
-        } else {
-            unsigned cell = g.cbits ? (unsigned)((L.lz * g.ty + L.ly) * g.tpitch + L.lx) & 31u : 0u;
-            const long long slab = g.nslab > 1 ? row * g.nslab / g.nrow : 0;
-            key = ((unsigned)(slab * g.nbins_slab + L.bin) << g.cbits) | cell;
+    const int lane = threadIdx.x & 31;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    int bad = 0;
+    // warp-uniform loop: every lane takes part in the match below
+    for (long long j0 = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); j0 < M; j0 += stride) {
+        const long long j = j0 + lane;
+        unsigned key = BAD_KEY;
+        if (j < M) {
+            int e;
+            key = vis_key(g, uu, vv, ww, foc, j, e);
+            bad |= e;
+            keys[j] = key;
         }
-        keys[j] = key;
-        vals[j] = (int)j;
+        const unsigned peers = __match_any_sync(0xffffffffu, key);
+        if (key != BAD_KEY && lane == __ffs(peers) - 1) atomicAdd(count + key, __popc(peers));
+    }
+    if (bad) atomicOr(err, bad);
+}
+
+// idx[position] = j: position = first position of key[j] + the rank claimed.
+// start[] (the exclusive scan of the counts) is consumed: it ends as each
+// key's one-past-last position.
+__global__ void k_bin_scatter(long long M, const unsigned *__restrict__ keys, int *__restrict__ start,
+                              int *__restrict__ idx) {
+    const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long j0 = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); j0 < M; j0 += stride) {
+        const long long j = j0 + lane;
+        const unsigned key = j < M ? keys[j] : BAD_KEY;
+        const unsigned peers = __match_any_sync(0xffffffffu, key);
+        const int leader = __ffs(peers) - 1;
+        int base = 0;
+        if (key != BAD_KEY && lane == leader) base = atomicAdd(start + key, __popc(peers));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (key != BAD_KEY) idx[base + __popc(peers & below)] = (int)j;
     }
 }
 
-// first / one-past-last sorted position of every non-empty bin
-__global__ void k_bin_bounds(const unsigned *__restrict__ keys, long long M, int cbits,
-                             int *__restrict__ first, int *__restrict__ last) {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < M;
-         i += (long long)gridDim.x * blockDim.x) {
-        unsigned k = keys[i];
-        if (k == 0xffffffffu) continue;
-        unsigned b = k >> cbits;
-        if (i == 0 || (keys[i - 1] >> cbits) != b || keys[i - 1] == 0xffffffffu) first[b] = (int)i;
-        if (i == M - 1 || keys[i + 1] == 0xffffffffu || (keys[i + 1] >> cbits) != b) last[b] = (int)i + 1;
-    }
-}
-
-__global__ void k_nsub(const int *__restrict__ first, const int *__restrict__ last, int *__restrict__ count,
-                       int *__restrict__ nsub, long long nb, int sub) {
+// Per bin, from the scanned key counts: first sorted position, count and the
+// number of sub-problems (chunks of at most `sub` visibilities).
+__global__ void k_bins_from_keys(const int *__restrict__ kstart, const int *__restrict__ total, long long nb,
+                                 int cbits, int sub, int *__restrict__ bin_start, int *__restrict__ bin_count,
+                                 int *__restrict__ nsub) {
     for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < nb;
          b += (long long)gridDim.x * blockDim.x) {
-        int c = last[b] - first[b];
-        count[b] = c;
-        nsub[b] = (c + sub - 1) / sub;
+        const int s = kstart[b << cbits];
+        const int e = b + 1 < nb ? kstart[(b + 1) << cbits] : *total;
+        bin_start[b] = s;
+        bin_count[b] = e - s;
+        nsub[b] = (e - s + sub - 1) / sub;
     }
+}
+
+// ------------------------------------------------------------------ scan
+// Prefix sums of int32 arrays (n < 2^31 summing below 2^31): per-block sums,
+// one block scanning the block sums, then each block's items scanned with its
+// offset.  SCAN_T threads x SCAN_I consecutive items per block, staged in
+// shared memory so that global loads and stores are coalesced.
+constexpr int SCAN_T = 512, SCAN_I = 8, SCAN_B = SCAN_T * SCAN_I;
+
+// Exclusive scan over the block (all SCAN_T threads call it, wsum has 32
+// entries); tot = the block's total.
+__device__ __forceinline__ int block_exclusive(int v, int *wsum, int &tot) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        int s = lane < SCAN_T / 32 ? wsum[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        wsum[lane] = s;
+    }
+    __syncthreads();
+    const int r = (warp ? wsum[warp - 1] : 0) + x - v;
+    tot = wsum[SCAN_T / 32 - 1];
+    __syncthreads();                     // wsum may be reused by the caller
+    return r;
+}
+
+__global__ void __launch_bounds__(SCAN_T) k_scan_sums(const int *__restrict__ in, long long n, int *__restrict__ bsum) {
+    const long long b0 = (long long)blockIdx.x * SCAN_B;
+    int s = 0;
+    for (int k = threadIdx.x; k < SCAN_B; k += SCAN_T)
+        if (b0 + k < n) s += in[b0 + k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    __shared__ int ws[32];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int t = 0;
+        for (int w = 0; w < SCAN_T / 32; ++w) t += ws[w];
+        bsum[blockIdx.x] = t;
+    }
+}
+
+// One block: exclusive scan of the nblk block sums in place; *total = their sum.
+__global__ void __launch_bounds__(SCAN_T) k_scan_top(int *__restrict__ bsum, long long nblk, int *__restrict__ total) {
+    __shared__ int ws[32];
+    int carry = 0;
+    for (long long c0 = 0; c0 < nblk; c0 += SCAN_T) {
+        const long long i = c0 + threadIdx.x;
+        const int v = i < nblk ? bsum[i] : 0;
+        int tot;
+        const int ex = block_exclusive(v, ws, tot);
+        if (i < nblk) bsum[i] = carry + ex;
+        carry += tot;
+    }
+    if (threadIdx.x == 0) *total = carry;
+}
+
+__global__ void __launch_bounds__(SCAN_T) k_scan_apply(const int *__restrict__ in, long long n,
+                                                       const int *__restrict__ boff, int *__restrict__ out,
+                                                       int inclusive) {
+    __shared__ int buf[SCAN_B + SCAN_B / 32];          // one pad word per 32: fewer bank conflicts
+    __shared__ int ws[32];
+    const long long b0 = (long long)blockIdx.x * SCAN_B;
+    auto at = [](int k) { return k + (k >> 5); };
+    for (int k = threadIdx.x; k < SCAN_B; k += SCAN_T) buf[at(k)] = b0 + k < n ? in[b0 + k] : 0;
+    __syncthreads();
+    int loc[SCAN_I], s = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_I; ++i) {
+        loc[i] = buf[at(threadIdx.x * SCAN_I + i)];
+        s += loc[i];
+    }
+    int tot;
+    int run = boff[blockIdx.x] + block_exclusive(s, ws, tot);
+#pragma unroll
+    for (int i = 0; i < SCAN_I; ++i) {
+        const int v = loc[i];
+        buf[at(threadIdx.x * SCAN_I + i)] = inclusive ? run + v : run;
+        run += v;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < SCAN_B; k += SCAN_T)
+        if (b0 + k < n) out[b0 + k] = buf[at(k)];
 }
 
 // Per sorted visibility: fractional offsets + packed start cell, and the
@@ -1232,46 +1369,35 @@ void launch_wrange(const double *w, int stride, long long nrow, unsigned long lo
     k_wrange<<<grid_for(nrow), NTHREADS, 0, st>>>(w, stride, nrow, keys, err);
 }
 
-void launch_bin_keys(const DevGeom &g, const double *u, const double *v, const double *w, const double *foc,
-                     unsigned *keys, int *vals, int *err, cudaStream_t st) {
+void launch_bin_count(const DevGeom &g, const double *u, const double *v, const double *w, const double *foc,
+                      unsigned *keys, int *count, int *err, cudaStream_t st) {
     count_launch();
-    k_bin_keys<<<grid_for(g.nrow * g.nchan), NTHREADS, 0, st>>>(g, u, v, w, foc, keys, vals, err);
+    k_bin_count<<<grid_for(g.nrow * g.nchan), NTHREADS, 0, st>>>(g, u, v, w, foc, keys, count, err);
 }
 
-size_t sort_temp_bytes(long long M, int end_bit) {
-    size_t b = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, b, (const unsigned *)nullptr, (unsigned *)nullptr,
-                                    (const int *)nullptr, (int *)nullptr, (int)M, 0, end_bit);
-    return b;
-}
-
-int sort_pairs(void *tmp, size_t tmpb, const unsigned *kin, unsigned *kout, const int *vin, int *vout,
-               long long M, int end_bit, cudaStream_t st) {
-    count_launch(2 * ((end_bit + 7) / 8) + 1);      // upsweep/histogram + one pass per digit (approx.)
-    return cub::DeviceRadixSort::SortPairs(tmp, tmpb, kin, kout, vin, vout, (int)M, 0, end_bit, st) ==
-                   cudaSuccess ? 0 : ERR_CUDA;
-}
-
-void launch_bin_bounds(const unsigned *keys, long long M, int cbits, int *first, int *last, cudaStream_t st) {
+void launch_bin_scatter(long long M, const unsigned *keys, int *start, int *idx, cudaStream_t st) {
     count_launch();
-    k_bin_bounds<<<grid_for(M), NTHREADS, 0, st>>>(keys, M, cbits, first, last);
+    k_bin_scatter<<<grid_for(M), NTHREADS, 0, st>>>(M, keys, start, idx);
 }
 
-void launch_nsub(const int *first, const int *last, int *count, int *nsub, long long nb, int sub,
-                 cudaStream_t st) {
+void launch_bins_from_keys(const int *kstart, const int *total, long long nb, int cbits, int sub, int *bin_start,
+                           int *bin_count, int *nsub, cudaStream_t st) {
     count_launch();
-    k_nsub<<<grid_for(nb), NTHREADS, 0, st>>>(first, last, count, nsub, nb, sub);
+    k_bins_from_keys<<<grid_for(nb), NTHREADS, 0, st>>>(kstart, total, nb, cbits, sub, bin_start, bin_count, nsub);
 }
 
-size_t scan_temp_bytes(long long n) {
-    size_t b = 0;
-    cub::DeviceScan::InclusiveSum(nullptr, b, (const int *)nullptr, (int *)nullptr, (int)n);
-    return b;
-}
+long long scan_temp_ints(long long n) { return (n + SCAN_B - 1) / SCAN_B + 1; }
 
-int scan_inclusive(void *tmp, size_t tmpb, const int *in, int *out, long long n, cudaStream_t st) {
-    count_launch(2);   // CUB scan: init + scan kernels
-    return cub::DeviceScan::InclusiveSum(tmp, tmpb, in, out, (int)n, st) == cudaSuccess ? 0 : ERR_CUDA;
+void scan_ints(const int *in, int *out, long long n, bool inclusive, int *tmp, cudaStream_t st) {
+    const long long nblk = (n + SCAN_B - 1) / SCAN_B;
+    if (nblk == 0) {
+        cudaMemsetAsync(tmp + 1, 0, sizeof(int), st);
+        return;
+    }
+    count_launch(3);
+    k_scan_sums<<<(unsigned)nblk, SCAN_T, 0, st>>>(in, n, tmp + 1);
+    k_scan_top<<<1, SCAN_T, 0, st>>>(tmp + 1, nblk, tmp);
+    k_scan_apply<<<(unsigned)nblk, SCAN_T, 0, st>>>(in, n, tmp + 1, out, inclusive ? 1 : 0);
 }
 
 template <typename T>

@@ -16,6 +16,7 @@ struct DevGeom {
     int nf1, nf2, nf3;
     int kw, hkw;                   // kernel width, floor(kw/2)
     int bx, by, bz, nbx, nby, nbz;
+    double ibx, iby, ibz;          // 1 / bx, 1 / by, 1 / bz
     int tx, ty, tz, zpad;
     int sub;                       // visibilities per sub-problem
     int cbits;                     // bits of the in-tile start cell in the sort key (0: bin only)

@@ -281,10 +281,10 @@ int plan_create(int type, int nx, int ny, double psx, double psy, double eps, do
 void plan_release_points(Plan *p) {
     cudaStream_t st = p->st;
     dfree(p->d_foc, st); dfree(p->d_quad, st); dfree(p->d_psi1, st); dfree(p->d_psi2, st);
-    dfree(p->d_wcoef, st); dfree(p->d_bin_count, st); dfree(p->d_bin_start, st); dfree(p->d_bin_last, st);
-    dfree(p->d_nsub, st); dfree(p->d_sub_end, st); dfree(p->d_key_a, st); dfree(p->d_key_b, st);
-    dfree(p->d_val_a, st); dfree(p->d_idx, st); dfree(p->d_err, st); dfree(p->d_keys, st);
-    dfree(p->d_rec, st); dfree(p->d_ph, st); dfree(p->d_cs, st); dfree(p->d_grid, st); dfree(p->d_tmp, st);
+    dfree(p->d_wcoef, st); dfree(p->d_bin_count, st); dfree(p->d_bin_start, st);
+    dfree(p->d_nsub, st); dfree(p->d_sub_end, st); dfree(p->d_keys_in, st); dfree(p->d_kcount, st);
+    dfree(p->d_idx, st); dfree(p->d_err, st); dfree(p->d_keys, st); dfree(p->d_scan, st);
+    dfree(p->d_rec, st); dfree(p->d_ph, st); dfree(p->d_cs, st); dfree(p->d_grid, st);
     dfree(p->d_tgrid, st);
     fft_release(p);
     p->fft_hx = p->fft_hx_rest = p->fft_hy = p->fft_hy_rest = 0;
@@ -531,6 +531,7 @@ retry_tiles:
     g.nf1 = gp.nf1; g.nf2 = gp.nf2; g.nf3 = gp.nf3;
     g.kw = gp.kp.kw; g.hkw = gp.kp.kw / 2;
     g.bx = tg.bx; g.by = tg.by; g.bz = tg.bz; g.nbx = tg.nbx; g.nby = tg.nby; g.nbz = tg.nbz;
+    g.ibx = 1.0 / tg.bx; g.iby = 1.0 / tg.by; g.ibz = tg.bz > 0 ? 1.0 / tg.bz : 0.0;
     g.tx = tg.tx; g.ty = tg.ty; g.tz = tg.tz; g.zpad = tg.zpad; g.sub = tg.sub;
     g.tpitch = (tg.tx + 2) & ~1;
     g.use_tma = 0;                          // set once the grid's TMA descriptor exists
@@ -581,35 +582,31 @@ retry_tiles:
     g.psx = gp.pixsize_x; g.psy = gp.pixsize_y; g.i_center = gp.i_center; g.gamma = gp.gamma;
     g.o_center = gp.o_center; g.sign = (double)gp.sign;
 
-    // binning: key per visibility (bin, start-cell residue), radix sort, bin bounds,
-    //    sub-problem scan, records in bin order (replaces the transpose and the
-    //    unsorted point order of the reference)
+    // binning: key per visibility (bin, start-cell residue) and its count, a
+    //    scan of the counts, per-bin bounds and sub-problems, the scatter of the
+    //    input indices into bin order, then records in bin order (replaces the
+    //    transpose and the unsorted point order of the reference)
     const long long nb = g.nbins;
     int binbits = 1;
     while ((1LL << binbits) < nb) ++binbits;
     int cbits = binbits + 5 <= 31 ? 5 : 0;               // start-cell bank residue; bin-only keys beyond
     if (binbits > 31) return ERR_UNSUPPORTED;
     g.cbits = cbits;
-    const int end_bit = binbits + cbits;
-    CU_TRY(dalloc(&p->d_key_a, M * sizeof(unsigned), st));
-    CU_TRY(dalloc(&p->d_key_b, M * sizeof(unsigned), st));
-    CU_TRY(dalloc(&p->d_val_a, M * sizeof(int), st));
+    const long long nkeys = nb << cbits;
+    CU_TRY(dalloc(&p->d_keys_in, M * sizeof(unsigned), st));
+    CU_TRY(dalloc(&p->d_kcount, nkeys * sizeof(int), st));
     CU_TRY(dalloc(&p->d_idx, M * sizeof(int), st));
     CU_TRY(dalloc(&p->d_bin_start, nb * sizeof(int), st));
-    CU_TRY(dalloc(&p->d_bin_last, nb * sizeof(int), st));
     CU_TRY(dalloc(&p->d_bin_count, nb * sizeof(int), st));
     CU_TRY(dalloc(&p->d_nsub, nb * sizeof(int), st));
     CU_TRY(dalloc(&p->d_sub_end, nb * sizeof(int), st));
-    p->tmp_bytes = std::max(sort_temp_bytes(M, end_bit), scan_temp_bytes(nb));
-    CU_TRY(dalloc(&p->d_tmp, p->tmp_bytes, st));
-    launch_bin_keys(g, du, dv, dw, p->d_foc, p->d_key_a, p->d_val_a, p->d_err, st);
-    if (sort_pairs(p->d_tmp, p->tmp_bytes, p->d_key_a, p->d_key_b, p->d_val_a, p->d_idx, M, end_bit, st))
-        return ERR_CUDA;
-    CU_TRY(cudaMemsetAsync(p->d_bin_start, 0, nb * sizeof(int), st));
-    CU_TRY(cudaMemsetAsync(p->d_bin_last, 0, nb * sizeof(int), st));
-    launch_bin_bounds(p->d_key_b, M, cbits, p->d_bin_start, p->d_bin_last, st);
-    launch_nsub(p->d_bin_start, p->d_bin_last, p->d_bin_count, p->d_nsub, nb, g.sub, st);
-    if (scan_inclusive(p->d_tmp, p->tmp_bytes, p->d_nsub, p->d_sub_end, nb, st)) return ERR_CUDA;
+    CU_TRY(dalloc(&p->d_scan, std::max(scan_temp_ints(nkeys), scan_temp_ints(nb)) * sizeof(int), st));
+    CU_TRY(cudaMemsetAsync(p->d_kcount, 0, nkeys * sizeof(int), st));
+    launch_bin_count(g, du, dv, dw, p->d_foc, p->d_keys_in, p->d_kcount, p->d_err, st);
+    scan_ints(p->d_kcount, p->d_kcount, nkeys, false, p->d_scan, st);          // in place: first position per key
+    launch_bins_from_keys(p->d_kcount, p->d_scan, nb, cbits, g.sub, p->d_bin_start, p->d_bin_count, p->d_nsub, st);
+    launch_bin_scatter(M, p->d_keys_in, p->d_kcount, p->d_idx, st);
+    scan_ints(p->d_nsub, p->d_sub_end, nb, true, p->d_scan, st);
     p->slab_sub_end.assign(nslab, 0);               // last sub-problem end of every slab
     for (int k = 0; k < nslab; ++k)
         CU_TRY(cudaMemcpyAsync(&p->slab_sub_end[k], p->d_sub_end + (k + 1) * g.nbins_slab - 1, sizeof(int),
@@ -623,9 +620,9 @@ retry_tiles:
             force_slabs = true;
             herr = 0;
             CU_TRY(cudaMemsetAsync(p->d_err, 0, sizeof(int), st));
-            dfree(p->d_key_a, st); dfree(p->d_key_b, st); dfree(p->d_val_a, st); dfree(p->d_idx, st);
-            dfree(p->d_bin_start, st); dfree(p->d_bin_last, st); dfree(p->d_bin_count, st);
-            dfree(p->d_nsub, st); dfree(p->d_sub_end, st); dfree(p->d_tmp, st);
+            dfree(p->d_keys_in, st); dfree(p->d_kcount, st); dfree(p->d_idx, st);
+            dfree(p->d_bin_start, st); dfree(p->d_bin_count, st);
+            dfree(p->d_nsub, st); dfree(p->d_sub_end, st); dfree(p->d_scan, st);
             goto retry_tiles;
         }
         return ERR_GENERIC;
@@ -637,10 +634,9 @@ retry_tiles:
         launch_records<float>(g, du, dv, dw, p->d_foc, p->d_idx, M, p->d_rec, p->d_ph, st);
     else
         launch_records<double>(g, du, dv, dw, p->d_foc, p->d_idx, M, p->d_rec, p->d_ph, st);
-    dfree(p->d_key_a, st);
-    dfree(p->d_key_b, st);
-    dfree(p->d_val_a, st);
-    dfree(p->d_bin_last, st);
+    dfree(p->d_keys_in, st);
+    dfree(p->d_kcount, st);
+    dfree(p->d_scan, st);
     // TMA descriptor of the grid for the interpolator's interior tile boxes
     // ({tpitch, ty, tz} cells in 8-byte elements: one per FP32 cell, two per
     // FP64 cell; box edges <= 256 elements, x starts 16-byte aligned)

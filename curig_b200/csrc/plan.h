@@ -61,16 +61,16 @@ struct Plan {
 
     // device buffers owned by the plan
     double *d_foc = nullptr, *d_quad = nullptr, *d_psi1 = nullptr, *d_psi2 = nullptr, *d_wcoef = nullptr;
-    int *d_bin_count = nullptr, *d_bin_start = nullptr, *d_bin_last = nullptr, *d_nsub = nullptr,
-        *d_sub_end = nullptr;
-    unsigned *d_key_a = nullptr, *d_key_b = nullptr;   // sort keys (unsorted / sorted)
-    int *d_val_a = nullptr, *d_idx = nullptr;           // input index (unsorted / sorted = bin order)
+    int *d_bin_count = nullptr, *d_bin_start = nullptr, *d_nsub = nullptr, *d_sub_end = nullptr;
+    unsigned *d_keys_in = nullptr;                      // sort key per visibility (input order)
+    int *d_kcount = nullptr;                            // count / first position per key value
+    int *d_idx = nullptr;                               // input index per sorted position (bin order)
     int *d_err = nullptr;
     unsigned long long *d_keys = nullptr;
-    void *d_rec = nullptr, *d_ph = nullptr, *d_cs = nullptr, *d_grid = nullptr, *d_tmp = nullptr;
+    int *d_scan = nullptr;                              // scan temporaries (total, block sums)
+    void *d_rec = nullptr, *d_ph = nullptr, *d_cs = nullptr, *d_grid = nullptr;
     void *d_tgrid = nullptr;           // image columns of every plane, transposed: [nf3][ny][nf2]
     CUtensorMap tmap{};                // TMA descriptor of d_grid for the interpolator's tile boxes (FP32)
-    size_t tmp_bytes = 0;
 
     // x transforms on grid rows, y transforms on rows of the column-transposed planes
     cufftHandle fft_hx = 0, fft_hx_rest = 0, fft_hy = 0, fft_hy_rest = 0;
@@ -142,16 +142,16 @@ void plan_release_points(Plan *p);
 // launchers (kernels.cu)
 void launch_wrange(const double *w, int stride, long long nrow, unsigned long long *keys, int *err,
                    cudaStream_t st);
-void launch_bin_keys(const DevGeom &g, const double *u, const double *v, const double *w, const double *foc,
-                     unsigned *keys, int *vals, int *err, cudaStream_t st);
-size_t sort_temp_bytes(long long M, int end_bit);
-int sort_pairs(void *tmp, size_t tmpb, const unsigned *kin, unsigned *kout, const int *vin, int *vout,
-               long long M, int end_bit, cudaStream_t st);
-void launch_bin_bounds(const unsigned *keys, long long M, int cbits, int *first, int *last, cudaStream_t st);
-void launch_nsub(const int *first, const int *last, int *count, int *nsub, long long nb, int sub,
-                 cudaStream_t st);
-size_t scan_temp_bytes(long long n);
-int scan_inclusive(void *tmp, size_t tmpb, const int *in, int *out, long long n, cudaStream_t st);
+// binning: a counting sort over (bin, residue) keys (kernels.cu)
+void launch_bin_count(const DevGeom &g, const double *u, const double *v, const double *w, const double *foc,
+                      unsigned *keys, int *count, int *err, cudaStream_t st);
+void launch_bin_scatter(long long M, const unsigned *keys, int *start, int *idx, cudaStream_t st);
+void launch_bins_from_keys(const int *kstart, const int *total, long long nb, int cbits, int sub, int *bin_start,
+                           int *bin_count, int *nsub, cudaStream_t st);
+// Prefix sum of n int32 values (exclusive or inclusive); tmp holds
+// scan_temp_ints(n) ints, tmp[0] receives the total.
+long long scan_temp_ints(long long n);
+void scan_ints(const int *in, int *out, long long n, bool inclusive, int *tmp, cudaStream_t st);
 size_t tile_smem_bytes(const TileGeom &tg, int esize, int kw, int wdeg);
 template <typename T>
 void launch_records(const DevGeom &g, const double *u, const double *v, const double *w, const double *foc,
