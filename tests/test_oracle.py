@@ -111,7 +111,9 @@ def test_oracle_multichannel_is_sum_of_channels():
 
 
 def _reflib_files():
-    return sorted(glob.glob(os.path.join(GOLDEN, "reflib_*.npz")))
+    # single-call fixtures (inputs stored); the 4096^2 ones are in test_configs_at_size.py
+    return sorted(p for p in glob.glob(os.path.join(GOLDEN, "reflib_*.npz"))
+                  if not os.path.basename(p).startswith("reflib_cfg2_"))
 
 
 @pytest.mark.parametrize("path", _reflib_files(), ids=os.path.basename)
