@@ -54,7 +54,9 @@ def args_():
     ap.add_argument("--window", default="auto", choices=["auto", "es", "learned"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--no-arms", action="store_true", help="skip the ES comparison arms")
+    ap.add_argument("--no-arms", action="store_true", help="skip the comparison arms (ES, FP64, exact FP32)")
+    ap.add_argument("--no-refgpu", action="store_true",
+                    help="skip timing the reference's own GPU library (oracle/_ref) beside this one")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--accumulate", type=int, default=0, help="tile accumulation: 0 automatic, 1 float atomics, 2 one-word int32 fixed point, 3 two-word (exact); FP64: 1 double atomics, else exact int64 + int32")
@@ -66,6 +68,27 @@ def args_():
     ap.add_argument("--error-table", action="store_true",
                     help="print errors per epsilon and precision form (FP64 DFT, FP64 GPU) and exit")
     return ap.parse_args()
+
+
+def bench_config(a, world):
+    """The workload description both arms print (a function of the arguments only)."""
+    acc = {0: "automatic", 1: "float atomics", 2: "one-word int32 fixed point",
+           3: "two-word int32 fixed point (exact)"}.get(a.accumulate, str(a.accumulate))
+    return {"workload": f"ms2dirty+dirty2ms, {a.nrow} rows x {a.nchan} ch ({a.nrow * a.nchan} vis), "
+                        f"{a.npix}^2, fov {a.fov} deg, eps {a.eps}, sigma 2",
+            "window": a.window, "precision": a.precision, "accumulate": acc,
+            "l2": "inputs (>= 1.9 GB per step) larger than L2; no flush needed",
+            "parallelism": f"dp{world} (visibility shards, all-reduce of dirty)" if world > 1 else "single GPU"}
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
 
 
 def workload(torch, nrow, nchan, npix, fov, seed, device):
@@ -174,9 +197,113 @@ def cpu_baseline(uvw_h, freq, vis_h, wgt_h, npix, fov, target_s):
     rate = nrow_s * nchan * npx / t                          # pixel * vis / s
     vis_per_s = rate / (2.0 * npix * npix)                   # ms2dirty + dirty2ms over the full image
     return {"value": vis_per_s, "unit": "vis/s", "cores": os.cpu_count(), "kind": "port",
+            "cpu_model": cpu_model(),
             "sample": f"{nrow_s * nchan} vis x {npx} pixels of the {npix}^2 image, FP64 DFT "
                       f"(oracle/dft.c, OpenMP), {t:.1f} s; extrapolated to ms2dirty+dirty2ms over "
-                      f"all pixels", "pixel_vis_per_s": rate}
+                      f"all pixels", "pixel_vis_per_s": rate, "sample_seconds": t}
+
+
+def numpy_explicit_baseline(uvw_h, freq, vis_h, npix, fov, target_s):
+    """The reference's own CPU path as it runs: its numpy explicit gridder and
+    degridder (restated in oracle/explicit_numpy.py), one process, whole-image
+    array operations per visibility, on the full npix^2 image for a few
+    visibilities; vis/s of ms2dirty + dirty2ms over the full image."""
+    from oracle import explicit_numpy as X
+    psx = fov * np.pi / 180 / npix
+    img = np.zeros((npix, npix))
+    n, t = 1, 0.0
+    while True:
+        t0 = time.perf_counter()
+        X.explicit_gridder(uvw_h[:n], freq[:1], vis_h[:n, :1], npix, npix, psx, psx)
+        X.explicit_degridder(uvw_h[:n], freq[:1], img, psx, psx, -1)
+        t = time.perf_counter() - t0
+        if t >= target_s or n >= 64:
+            break
+        n = max(n + 1, int(n * min(8.0, 1.2 * target_s / max(t, 1e-3))))
+    return {"value": n / t, "unit": "vis/s", "cores": 1, "kind": "port",
+            "sample": f"{n} vis, ms2dirty + dirty2ms each over the full {npix}^2 image (numpy, "
+                      f"one process), {t:.1f} s", "sample_seconds": t}
+
+
+def _bind_reference_abi(path):
+    """ms2dirty_2 / dirty2ms_2 of a libcurafft.so with plain pointer arguments
+    (include/cugridder.h:13-20 of the reference)."""
+    import ctypes
+    lib = ctypes.CDLL(path)
+    P, ci, cd = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    for name in ("ms2dirty_2", "dirty2ms_2"):
+        f = getattr(lib, name)
+        f.argtypes = [ci, ci, ci, cd, cd, P, P, P, P, cd, cd, ci]
+        f.restype = ci
+    return lib
+
+
+def reference_gpu(torch, uvw, freq, vis, wgt, npix, fov, eps):
+    """The reference's own GPU library on the same B200, beside this library's
+    reference ABI: libcurafft.so built for sm_100a from the reference's sources
+    (oracle/Makefile.ref, flag-only changes) into oracle/_ref/, called through
+    its stock one-shot ABI (ms2dirty_2 / dirty2ms_2: FP64, host buffers, one
+    frequency per call, src/astro/cugridder.cu:587-612) once per channel, as its
+    Python package does (python/curagridder/curagridder.py:92 passes freq[0]).
+    Each call is one 1e7-row single-channel FP64 transform with its own copies.
+    The same 2 x nchan calls then go through this library's reference ABI.
+    Wall time of the calls alone; the host-side channel sum is not timed.
+    The outputs of the two libraries are compared over the whole image and
+    all visibilities."""
+    path = os.path.join(ROOT, "oracle", "_ref", "libcurafft_ref.so")
+    if not os.path.exists(path):
+        return {"unavailable": "oracle/_ref/libcurafft_ref.so not built (needs the reference sources)"}
+    from curig_b200 import _lib
+    ref, mine = _bind_reference_abi(path), _bind_reference_abi(_lib.LIB_PATH)
+    nrow, nchan = vis.shape
+    fovd = float(fov)
+    h_uvw = uvw.to(torch.float64).contiguous().cpu().pin_memory()
+    vis_ch = [vis[:, c].to(torch.complex128).contiguous().cpu().pin_memory() for c in range(nchan)]
+    wgt_ch = [wgt[:, c].to(torch.float64).contiguous().cpu().pin_memory() for c in range(nchan)]
+    img = torch.complex(torch.randn((npix, npix), dtype=torch.float64),
+                        torch.randn((npix, npix), dtype=torch.float64)).pin_memory()
+    out = torch.empty((npix, npix), dtype=torch.complex128).pin_memory()
+    vout = torch.empty(nrow, dtype=torch.complex128).pin_memory()
+
+    def step(lib, keep_vis):
+        """One step of 2 x nchan reference-ABI calls: (seconds in the calls,
+        dirty image summed over channels, per-channel visibilities if kept)."""
+        t = 0.0
+        acc = torch.zeros((npix, npix), dtype=torch.complex128)
+        kept = []
+        for c in range(nchan):
+            t0 = time.perf_counter()
+            s1 = lib.ms2dirty_2(nrow, npix, npix, fovd, float(freq[c]), h_uvw.data_ptr(), vis_ch[c].data_ptr(),
+                                wgt_ch[c].data_ptr(), out.data_ptr(), eps, 2.0, -1)
+            t += time.perf_counter() - t0
+            acc += out
+            t0 = time.perf_counter()
+            s2 = lib.dirty2ms_2(nrow, npix, npix, fovd, float(freq[c]), h_uvw.data_ptr(), vout.data_ptr(),
+                                wgt_ch[c].data_ptr(), img.data_ptr(), eps, 2.0, -1)
+            t += time.perf_counter() - t0
+            if s1 or s2:
+                raise RuntimeError(f"reference ABI status {s1} / {s2}")
+            if keep_vis:
+                kept.append(vout.clone())
+        return t, acc, kept
+
+    # warm-up: one channel through each library (context, module loading)
+    for lib in (ref, mine):
+        lib.ms2dirty_2(nrow, npix, npix, fovd, float(freq[0]), h_uvw.data_ptr(), vis_ch[0].data_ptr(),
+                       wgt_ch[0].data_ptr(), out.data_ptr(), eps, 2.0, -1)
+    t_ref, d_ref, v_ref = step(ref, True)
+    t_mine, d_mine, v_mine = step(mine, True)
+    num_v = sum(float(torch.sum(torch.abs(x - y) ** 2)) for x, y in zip(v_mine, v_ref))
+    den_v = sum(float(torch.sum(torch.abs(y) ** 2)) for y in v_ref)
+    M = nrow * nchan
+    return {"value": M / t_ref, "unit": "vis/s", "ms_per_step": round(1e3 * t_ref, 1),
+            "this_library_same_calls": {"value": M / t_mine, "ms_per_step": round(1e3 * t_mine, 1)},
+            "speedup_same_calls": round(t_ref / t_mine, 2),
+            "rel_diff_ms2dirty": float(torch.linalg.vector_norm(d_mine - d_ref) / torch.linalg.vector_norm(d_ref)),
+            "rel_diff_dirty2ms": float(np.sqrt(num_v / den_v)),
+            "calls": f"{nchan} x ms2dirty_2 + {nchan} x dirty2ms_2, {nrow} rows each, FP64, eps {eps}, "
+                     f"pinned host buffers, wall time of the calls",
+            "library": "reference libcurafft.so built for sm_100a from its sources (flag-only changes)"}
 
 
 def es_width_for(eps):
@@ -380,16 +507,24 @@ def main():
     # every arm accumulates like the headline (automatic mode resolved at its epsilon)
     acc_mode = a.accumulate or (2 if a.eps >= 1e-5 else 3)
 
-    def time_arm(win, eps, steps, warmup, with_clocks=False):
-        plan = GridderPlan(1, a.npix, a.npix, psx, psx, eps, 2.0, -1, precision=a.precision, window=win,
-                           stream=stream, bin_xy=a.bin, sub=a.sub, smem_budget=a.smem, accumulate=acc_mode)
+    def time_arm(win, eps, steps, warmup, with_clocks=False, precision=None, accumulate=None):
+        prec = precision or a.precision
+        if prec == a.precision:
+            v_, w_, d_, o_ = vis, wgt, dirty, vout
+        else:                                            # another precision: its own copies
+            c_ = torch.complex64 if prec == "fp32" else torch.complex128
+            v_, w_ = vis.to(c_), wgt.to(torch.float32 if prec == "fp32" else torch.float64)
+            d_, o_ = torch.empty((a.npix, a.npix), dtype=c_, device=dev), torch.empty_like(v_)
+        plan = GridderPlan(1, a.npix, a.npix, psx, psx, eps, 2.0, -1, precision=prec, window=win,
+                           stream=stream, bin_xy=a.bin, sub=a.sub, smem_budget=a.smem,
+                           accumulate=acc_mode if accumulate is None else accumulate)
 
         def step():
             plan.setpts(uvw, freq)
-            plan.execute_dir(1, vis, wgt, dirty)
+            plan.execute_dir(1, v_, w_, d_)
             if world > 1:
-                torch.distributed.all_reduce(dirty)
-            plan.execute_dir(2, vout, wgt, dirty)
+                torch.distributed.all_reduce(d_)
+            plan.execute_dir(2, o_, w_, d_)
 
         for _ in range(warmup):
             step()
@@ -446,6 +581,19 @@ def main():
                                      "rule": "kw = ceil(-log10(eps/10)) (conv_interp_invoker.cu:84)"}
         if table:
             arms["learned_measured_error_256"] = table[info["kw"]]["eps_reached"]
+    if world == 1 and not a.no_arms:
+        # the exact (compensated) FP32 tile form at the headline epsilon and window
+        if a.precision == "fp32" and acc_mode != 3:
+            r = time_arm(window, a.eps, max(2, a.steps // 2), 2, accumulate=3)
+            arms["fp32_two_word_exact"] = {"value": r["value"], "ms_per_step": round(r["ms"], 3),
+                                           "kw": r["info"]["kw"], "window": window,
+                                           "accumulate": "two-word int32 fixed point (exact)"}
+        # the reference's arithmetic: FP64, ES window at the reference's width rule
+        r = time_arm("es", a.eps, max(2, a.steps // 2), 2, precision="fp64", accumulate=0)
+        arms["fp64_es_reference_rule"] = {"value": r["value"], "ms_per_step": round(r["ms"], 3),
+                                          "kw": r["info"]["kw"], "window": "es",
+                                          "accumulate": "int64 + int32 fixed point (exact)"}
+        torch.cuda.empty_cache()
 
     # batch of 8 independent problems through the autograd pair (single process)
     batch8 = None
@@ -559,6 +707,16 @@ def main():
         n = max(1, 20000 // a.nchan)
         cpu = cpu_baseline(uvw[:n].cpu().numpy(), freq, vis[:n].cpu().numpy().astype(np.complex128),
                            wgt[:n].cpu().numpy().astype(np.float64), a.npix, a.fov, a.cpu_seconds)
+        cpu["numpy_explicit"] = numpy_explicit_baseline(uvw[:64].cpu().numpy(), freq,
+                                                        vis[:64].cpu().numpy().astype(np.complex128),
+                                                        a.npix, a.fov, min(a.cpu_seconds, 8.0))
+
+    refgpu = None
+    if rank == 0 and world == 1 and not a.no_refgpu:
+        try:
+            refgpu = reference_gpu(torch, uvw, freq, vis, wgt, a.npix, a.fov, a.eps)
+        except Exception as exc:  # pragma: no cover
+            refgpu = {"error": str(exc)}
 
     if rank == 0:
         out = {
@@ -566,14 +724,13 @@ def main():
             "warmup": a.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32" if a.precision == "fp32" else "f64",
             "data": "synthetic (seeded Gaussian uv density, uniform w, complex-normal vis; generated on device)",
-            "config": {"workload": f"ms2dirty+dirty2ms, {a.nrow} rows x {a.nchan} ch "
-                                   f"({a.nrow * a.nchan} vis), {a.npix}^2, fov {a.fov} deg, "
-                                   f"eps {a.eps}, sigma 2", "window": window,
-                       "precision": a.precision, "kw": info["kw"], "nf": [info["nf1"], info["nf2"], info["nf3"]],
-                       "bin_xy": info["bin_xy"], "accumulate": ({1: "float atomics", 2: "one-word int32 fixed point", 3: "two-word int32 fixed point (exact)"}[acc_mode] if a.precision == "fp32" else
-                                      "double atomics" if acc_mode == 1 else "int64 + int32 fixed point (exact)"),
-                       "l2": "inputs (>= 1.9 GB per step) larger than L2; no flush needed",
-                       "parallelism": f"dp{world} (visibility shards, all-reduce of dirty)" if world > 1 else "single GPU"},
+            "config": bench_config(a, world),
+            "plan": {"window": window, "kw": info["kw"], "nf": [info["nf1"], info["nf2"], info["nf3"]],
+                     "bin_xy": info["bin_xy"],
+                     "accumulate": ({1: "float atomics", 2: "one-word int32 fixed point",
+                                     3: "two-word int32 fixed point (exact)"}[acc_mode] if a.precision == "fp32" else
+                                    "double atomics" if acc_mode == 1 else "int64 + int32 fixed point (exact)")},
+            "reference_gpu": refgpu,
             "e2e": e2e, "gpu_launches": int(head["launches"]), "clocks": head["clocks"],
             "roofline": roof, "cpu_baseline": cpu, "arms": arms, "batch8_autograd": batch8,
             "accuracy_vs_dft": acc,
@@ -585,7 +742,12 @@ def main():
 
 
 def reference_arm(a, rank, world):
-    """CPU explicit DFT of the reference (oracle/dft.c port) on the host cores."""
+    """The reference's CPU path for this transform on the host cores: its
+    explicit FP64 DFT (python/curagridder/test_wst.py:15-32,
+    explicit_test.py:32-54), as the C/OpenMP port oracle/dft.c on all host
+    threads.  One step = one bounded sample of the workload (ms_per_step is the
+    sample's measured duration); value = the vis/s that rate gives for
+    ms2dirty + dirty2ms over the full workload (extrapolated_ms_per_step)."""
     if rank != 0:
         return
     rng = np.random.default_rng(a.seed)
@@ -603,14 +765,17 @@ def reference_arm(a, rank, world):
         cpu_baseline(uvw, freq, vis, wgt, a.npix, a.fov, per / 4)
     vals = [cpu_baseline(uvw, freq, vis, wgt, a.npix, a.fov, per) for _ in range(a.steps)]
     v = float(np.median([x["value"] for x in vals]))
+    sample_ms = float(np.mean([x["sample_seconds"] for x in vals])) * 1e3
     cb = dict(vals[-1])
     cb["value"] = v
     out = {"impl": "reference", "metric": METRIC, "value": v, "unit": "vis/s", "n_gpus": world,
-           "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * (a.nrow * a.nchan) / v,
+           "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(sample_ms, 1),
+           "extrapolated_ms_per_step": 1e3 * (a.nrow * a.nchan) / v,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic (seeded Gaussian uv density, uniform w, complex-normal vis)",
-           "config": {"workload": f"ms2dirty+dirty2ms, {a.nrow} rows x {a.nchan} ch, {a.npix}^2, "
-                                  f"fov {a.fov} deg, eps {a.eps}", "path": "explicit FP64 DFT on host cores"},
+           "config": bench_config(a, world),
+           "path": "explicit FP64 DFT on host cores (the reference's CPU path; C/OpenMP port)",
+           "step": "one bounded sample of the workload, timed; value extrapolated to the full workload",
            "cpu_baseline": cb,
            "e2e": {"value": v, "unit": "vis/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)

@@ -218,23 +218,25 @@ __global__ void k_bin_count(DevGeom g, const double *__restrict__ uu, const doub
     if (bad) atomicOr(err, bad);
 }
 
-// idx[position] = j: position = first position of key[j] + the rank claimed.
-// start[] (the exclusive scan of the counts) is consumed: it ends as each
-// key's one-past-last position.
-__global__ void k_bin_scatter(long long M, const unsigned *__restrict__ keys, int *__restrict__ start,
-                              int *__restrict__ idx) {
+// Coarse placement: tmp[position] = j with position = the first position of
+// j's bin + a rank claimed on the bin's cursor (bcur starts at bin_start).
+// With one cursor per bin (not per key) the partly written sectors of tmp stay
+// in L2 while the pass runs; k_records then orders each bin by residue.
+__global__ void k_bin_scatter(long long M, const unsigned *__restrict__ keys, int cbits, int *__restrict__ bcur,
+                              int *__restrict__ tmp) {
     const int lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long j0 = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); j0 < M; j0 += stride) {
         const long long j = j0 + lane;
         const unsigned key = j < M ? keys[j] : BAD_KEY;
-        const unsigned peers = __match_any_sync(0xffffffffu, key);
+        const unsigned bin = key == BAD_KEY ? BAD_KEY : key >> cbits;
+        const unsigned peers = __match_any_sync(0xffffffffu, bin);
         const int leader = __ffs(peers) - 1;
         int base = 0;
-        if (key != BAD_KEY && lane == leader) base = atomicAdd(start + key, __popc(peers));
+        if (bin != BAD_KEY && lane == leader) base = atomicAdd(bcur + bin, __popc(peers));
         base = __shfl_sync(0xffffffffu, base, leader);
-        if (key != BAD_KEY) idx[base + __popc(peers & below)] = (int)j;
+        if (bin != BAD_KEY) tmp[base + __popc(peers & below)] = (int)j;
     }
 }
 
@@ -242,12 +244,13 @@ __global__ void k_bin_scatter(long long M, const unsigned *__restrict__ keys, in
 // number of sub-problems (chunks of at most `sub` visibilities).
 __global__ void k_bins_from_keys(const int *__restrict__ kstart, const int *__restrict__ total, long long nb,
                                  int cbits, int sub, int *__restrict__ bin_start, int *__restrict__ bin_count,
-                                 int *__restrict__ nsub) {
+                                 int *__restrict__ nsub, int *__restrict__ bcur) {
     for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < nb;
          b += (long long)gridDim.x * blockDim.x) {
         const int s = kstart[b << cbits];
         const int e = b + 1 < nb ? kstart[(b + 1) << cbits] : *total;
         bin_start[b] = s;
+        bcur[b] = s;
         bin_count[b] = e - s;
         nsub[b] = (e - s + sub - 1) / sub;
     }
@@ -348,32 +351,56 @@ __global__ void __launch_bounds__(SCAN_T) k_scan_apply(const int *__restrict__ i
         if (b0 + k < n) out[b0 + k] = buf[at(k)];
 }
 
-// Per sorted visibility: fractional offsets + packed start cell, and the
-// w-shift phase e^{i o_c w} (cuft.cu:19-39), computed in FP64.
+// Records in sorted order: the visibilities of each bin (tmp, from
+// k_bin_scatter) are placed at their final position inside the bin's
+// segment, by residue: position = a rank claimed on the cursor of their key
+// (kcur = the exclusive scan of the key counts).  Per position: fractional
+// offsets + packed start cell, the w-shift phase e^{i o_c w} (cuft.cu:19-39,
+// FP64) and the input index.
 template <typename T>
 __global__ void k_records(DevGeom g, const double *__restrict__ uu, const double *__restrict__ vv,
                           const double *__restrict__ ww, const double *__restrict__ foc,
-                          const int *__restrict__ idx, long long M, R<T> *__restrict__ rec,
-                          C<T> *__restrict__ ph) {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < M;
-         i += (long long)gridDim.x * blockDim.x) {
-        int j = idx[i];
-        int row = j / g.nchan;
-        int ch = j - row * g.nchan;
-        double gx, gy, gz;
+                          const int *__restrict__ tmp, long long M, int *__restrict__ kcur, R<T> *__restrict__ rec,
+                          C<T> *__restrict__ ph, int *__restrict__ idx) {
+    const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i0 = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); i0 < M; i0 += stride) {
+        const long long i = i0 + lane;
+        unsigned key = BAD_KEY;
+        int j = 0;
         VisLoc L;
-        vis_grid(g, uu, vv, ww, row, foc[ch], gx, gy, gz);
-        locate(g, gx, gy, gz, L);
+        long long row = 0;
+        int ch = 0;
+        if (i < M) {
+            j = tmp[i];
+            row = j / g.nchan;
+            ch = (int)(j - row * g.nchan);
+            double gx, gy, gz;
+            vis_grid(g, uu, vv, ww, row, foc[ch], gx, gy, gz);
+            locate(g, gx, gy, gz, L);
+            const unsigned cell = g.cbits ? (unsigned)((L.lz * g.ty + L.ly) * g.tpitch + L.lx) & 31u : 0u;
+            const long long slab = g.nslab > 1 ? row * g.nslab / g.nrow : 0;
+            key = ((unsigned)(slab * g.nbins_slab + L.bin) << g.cbits) | cell;
+        }
+        const unsigned peers = __match_any_sync(0xffffffffu, key);
+        const int leader = __ffs(peers) - 1;
+        int base = 0;
+        if (key != BAD_KEY && lane == leader) base = atomicAdd(kcur + key, __popc(peers));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (key == BAD_KEY) continue;
+        const int p = base + __popc(peers & below);
         R<T> r;
         r.x = (T)L.ux;
         r.y = (T)L.uy;
         r.z = (T)L.uz;
         if constexpr (sizeof(T) == 4) r.w = pack_cell_f(L.lx, L.ly, L.lz);
         else r.w = pack_cell_d(L.lx, L.ly, L.lz);
-        rec[i] = r;
-        double s, c;
-        sincos(g.o_center * w_eff(g, ww, row, foc[ch]), &s, &c);
-        ph[i] = C<T>{(T)c, (T)s};
+        rec[p] = r;
+        double sn, cs;
+        sincos(g.o_center * w_eff(g, ww, row, foc[ch]), &sn, &cs);
+        ph[p] = C<T>{(T)cs, (T)sn};
+        idx[p] = j;
     }
 }
 
@@ -1375,15 +1402,16 @@ void launch_bin_count(const DevGeom &g, const double *u, const double *v, const 
     k_bin_count<<<grid_for(g.nrow * g.nchan), NTHREADS, 0, st>>>(g, u, v, w, foc, keys, count, err);
 }
 
-void launch_bin_scatter(long long M, const unsigned *keys, int *start, int *idx, cudaStream_t st) {
+void launch_bin_scatter(long long M, const unsigned *keys, int cbits, int *bcur, int *tmp, cudaStream_t st) {
     count_launch();
-    k_bin_scatter<<<grid_for(M), NTHREADS, 0, st>>>(M, keys, start, idx);
+    k_bin_scatter<<<grid_for(M), NTHREADS, 0, st>>>(M, keys, cbits, bcur, tmp);
 }
 
 void launch_bins_from_keys(const int *kstart, const int *total, long long nb, int cbits, int sub, int *bin_start,
-                           int *bin_count, int *nsub, cudaStream_t st) {
+                           int *bin_count, int *nsub, int *bcur, cudaStream_t st) {
     count_launch();
-    k_bins_from_keys<<<grid_for(nb), NTHREADS, 0, st>>>(kstart, total, nb, cbits, sub, bin_start, bin_count, nsub);
+    k_bins_from_keys<<<grid_for(nb), NTHREADS, 0, st>>>(kstart, total, nb, cbits, sub, bin_start, bin_count, nsub,
+                                                        bcur);
 }
 
 long long scan_temp_ints(long long n) { return (n + SCAN_B - 1) / SCAN_B + 1; }
@@ -1402,10 +1430,10 @@ void scan_ints(const int *in, int *out, long long n, bool inclusive, int *tmp, c
 
 template <typename T>
 void launch_records(const DevGeom &g, const double *u, const double *v, const double *w, const double *foc,
-                    const int *idx, long long M, void *rec, void *ph, cudaStream_t st) {
+                    const int *tmp, long long M, int *kcur, void *rec, void *ph, int *idx, cudaStream_t st) {
     count_launch();
-    k_records<T><<<grid_for(M), NTHREADS, 0, st>>>(g, u, v, w, foc, idx, M, reinterpret_cast<R<T> *>(rec),
-                                                   reinterpret_cast<C<T> *>(ph));
+    k_records<T><<<grid_for(M), NTHREADS, 0, st>>>(g, u, v, w, foc, tmp, M, kcur, reinterpret_cast<R<T> *>(rec),
+                                                   reinterpret_cast<C<T> *>(ph), idx);
 }
 
 template <typename T>
@@ -1597,8 +1625,8 @@ void launch_zero_tpad(int nx, int ny, int nf2, int nf3, void *t, cudaStream_t st
 
 #define CURIG_INSTANTIATE(T)                                                                          \
     template void launch_records<T>(const DevGeom &, const double *, const double *, const double *,  \
-                                    const double *, const int *, long long, void *, void *,           \
-                                    cudaStream_t);                                                    \
+                                    const double *, const int *, long long, int *, void *, void *,    \
+                                    int *, cudaStream_t);                                             \
     template void launch_vis_prep<T>(long long, const int *, const void *, const void *, const void *,\
                                      void *, cudaStream_t);                                           \
     template void launch_vis_out<T>(long long, const int *, const void *, const void *, const void *, \

@@ -284,6 +284,7 @@ void plan_release_points(Plan *p) {
     dfree(p->d_wcoef, st); dfree(p->d_bin_count, st); dfree(p->d_bin_start, st);
     dfree(p->d_nsub, st); dfree(p->d_sub_end, st); dfree(p->d_keys_in, st); dfree(p->d_kcount, st);
     dfree(p->d_idx, st); dfree(p->d_err, st); dfree(p->d_keys, st); dfree(p->d_scan, st);
+    dfree(p->d_tmp, st); dfree(p->d_bcur, st);
     dfree(p->d_rec, st); dfree(p->d_ph, st); dfree(p->d_cs, st); dfree(p->d_grid, st);
     dfree(p->d_tgrid, st);
     fft_release(p);
@@ -595,7 +596,8 @@ retry_tiles:
     const long long nkeys = nb << cbits;
     CU_TRY(dalloc(&p->d_keys_in, M * sizeof(unsigned), st));
     CU_TRY(dalloc(&p->d_kcount, nkeys * sizeof(int), st));
-    CU_TRY(dalloc(&p->d_idx, M * sizeof(int), st));
+    CU_TRY(dalloc(&p->d_tmp, M * sizeof(int), st));
+    CU_TRY(dalloc(&p->d_bcur, nb * sizeof(int), st));
     CU_TRY(dalloc(&p->d_bin_start, nb * sizeof(int), st));
     CU_TRY(dalloc(&p->d_bin_count, nb * sizeof(int), st));
     CU_TRY(dalloc(&p->d_nsub, nb * sizeof(int), st));
@@ -604,8 +606,9 @@ retry_tiles:
     CU_TRY(cudaMemsetAsync(p->d_kcount, 0, nkeys * sizeof(int), st));
     launch_bin_count(g, du, dv, dw, p->d_foc, p->d_keys_in, p->d_kcount, p->d_err, st);
     scan_ints(p->d_kcount, p->d_kcount, nkeys, false, p->d_scan, st);          // in place: first position per key
-    launch_bins_from_keys(p->d_kcount, p->d_scan, nb, cbits, g.sub, p->d_bin_start, p->d_bin_count, p->d_nsub, st);
-    launch_bin_scatter(M, p->d_keys_in, p->d_kcount, p->d_idx, st);
+    launch_bins_from_keys(p->d_kcount, p->d_scan, nb, cbits, g.sub, p->d_bin_start, p->d_bin_count, p->d_nsub,
+                          p->d_bcur, st);
+    launch_bin_scatter(M, p->d_keys_in, cbits, p->d_bcur, p->d_tmp, st);
     scan_ints(p->d_nsub, p->d_sub_end, nb, true, p->d_scan, st);
     p->slab_sub_end.assign(nslab, 0);               // last sub-problem end of every slab
     for (int k = 0; k < nslab; ++k)
@@ -620,7 +623,7 @@ retry_tiles:
             force_slabs = true;
             herr = 0;
             CU_TRY(cudaMemsetAsync(p->d_err, 0, sizeof(int), st));
-            dfree(p->d_keys_in, st); dfree(p->d_kcount, st); dfree(p->d_idx, st);
+            dfree(p->d_keys_in, st); dfree(p->d_kcount, st); dfree(p->d_tmp, st); dfree(p->d_bcur, st);
             dfree(p->d_bin_start, st); dfree(p->d_bin_count, st);
             dfree(p->d_nsub, st); dfree(p->d_sub_end, st); dfree(p->d_scan, st);
             goto retry_tiles;
@@ -630,13 +633,18 @@ retry_tiles:
     CU_TRY(dalloc(&p->d_rec, M * 4 * (size_t)esize, st));
     CU_TRY(dalloc(&p->d_ph, M * 2 * (size_t)esize, st));
     CU_TRY(dalloc(&p->d_cs, M * 2 * (size_t)esize, st));
+    CU_TRY(dalloc(&p->d_idx, M * sizeof(int), st));
+    // each bin's visibilities (tmp) placed by residue; the key cursors start at
+    // the scanned key counts
     if (p->opt.precision)
-        launch_records<float>(g, du, dv, dw, p->d_foc, p->d_idx, M, p->d_rec, p->d_ph, st);
+        launch_records<float>(g, du, dv, dw, p->d_foc, p->d_tmp, M, p->d_kcount, p->d_rec, p->d_ph, p->d_idx, st);
     else
-        launch_records<double>(g, du, dv, dw, p->d_foc, p->d_idx, M, p->d_rec, p->d_ph, st);
+        launch_records<double>(g, du, dv, dw, p->d_foc, p->d_tmp, M, p->d_kcount, p->d_rec, p->d_ph, p->d_idx, st);
     dfree(p->d_keys_in, st);
     dfree(p->d_kcount, st);
     dfree(p->d_scan, st);
+    dfree(p->d_tmp, st);
+    dfree(p->d_bcur, st);
     // TMA descriptor of the grid for the interpolator's interior tile boxes
     // ({tpitch, ty, tz} cells in 8-byte elements: one per FP32 cell, two per
     // FP64 cell; box edges <= 256 elements, x starts 16-byte aligned)

@@ -64,6 +64,7 @@ struct Plan {
     int *d_bin_count = nullptr, *d_bin_start = nullptr, *d_nsub = nullptr, *d_sub_end = nullptr;
     unsigned *d_keys_in = nullptr;                      // sort key per visibility (input order)
     int *d_kcount = nullptr;                            // count / first position per key value
+    int *d_bcur = nullptr, *d_tmp = nullptr;            // bin cursors; input index per position, bin order
     int *d_idx = nullptr;                               // input index per sorted position (bin order)
     int *d_err = nullptr;
     unsigned long long *d_keys = nullptr;
@@ -145,9 +146,9 @@ void launch_wrange(const double *w, int stride, long long nrow, unsigned long lo
 // binning: a counting sort over (bin, residue) keys (kernels.cu)
 void launch_bin_count(const DevGeom &g, const double *u, const double *v, const double *w, const double *foc,
                       unsigned *keys, int *count, int *err, cudaStream_t st);
-void launch_bin_scatter(long long M, const unsigned *keys, int *start, int *idx, cudaStream_t st);
+void launch_bin_scatter(long long M, const unsigned *keys, int cbits, int *bcur, int *tmp, cudaStream_t st);
 void launch_bins_from_keys(const int *kstart, const int *total, long long nb, int cbits, int sub, int *bin_start,
-                           int *bin_count, int *nsub, cudaStream_t st);
+                           int *bin_count, int *nsub, int *bcur, cudaStream_t st);
 // Prefix sum of n int32 values (exclusive or inclusive); tmp holds
 // scan_temp_ints(n) ints, tmp[0] receives the total.
 long long scan_temp_ints(long long n);
@@ -155,7 +156,7 @@ void scan_ints(const int *in, int *out, long long n, bool inclusive, int *tmp, c
 size_t tile_smem_bytes(const TileGeom &tg, int esize, int kw, int wdeg);
 template <typename T>
 void launch_records(const DevGeom &g, const double *u, const double *v, const double *w, const double *foc,
-                    const int *idx, long long M, void *rec, void *ph, cudaStream_t st);
+                    const int *tmp, long long M, int *kcur, void *rec, void *ph, int *idx, cudaStream_t st);
 template <typename T>
 void launch_vis_prep(long long M, const int *idx, const void *ph, const void *vis, const void *wgt, void *cs,
                      cudaStream_t st);

@@ -148,3 +148,20 @@ def test_torch_dft_matches_c_oracle(nchan, sign, use_wgt):
     ref = dft.dirty2ms_dft(uvw, freq, d, wgt, psx, psy, sign, idx=idx)
     got = dft_torch.dirty2ms_dft(uvw, freq, d, wgt, psx, psy, sign, idx, chunk=500)
     assert l2err(ref, got) < 1e-12
+
+
+@pytest.mark.parametrize("path", _golden_files()[1:], ids=os.path.basename)
+def test_numpy_explicit_path_matches_reference_truth(path):
+    """oracle/explicit_numpy.py (the reference's CPU path as bench.py times it)
+    against the reference's own explicit_gridder / explicit_degridder outputs."""
+    from oracle import explicit_numpy as X
+    g = np.load(path)
+    uvw, freq, ms = g["uvw"], g["freq"], g["ms"]
+    wgt = g["wgt"] if g["wgt"].size else None
+    nx, ny = g["gridder_sign_m1"].shape
+    msw = ms * wgt if wgt is not None else ms
+    xps, yps = float(g["xpixsize"]), float(g["ypixsize"])
+    assert l2err(g["gridder_sign_m1"], X.explicit_gridder(uvw, freq, msw, nx, ny, xps, yps)) < 1e-12
+    if "degridder_sign_m1" in g:
+        got = X.explicit_degridder(uvw, freq, g["dirty"], xps, yps, -1)
+        assert l2err(g["degridder_sign_m1"], got) < 1e-12
