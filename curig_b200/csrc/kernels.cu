@@ -2,7 +2,7 @@
 //
 // Replaces, on the ms2dirty / dirty2ms path of the reference:
 //   get_effective_coordinate + rescaling + pre_stage_1/2 + transpose
-//       (precomp.cu:48-79, utils.cu:56-154, cuft.cu:19-92)  -> k_bin_keys + radix sort + k_records / k_vis_prep
+//       (precomp.cu:48-79, utils.cu:56-154, cuft.cu:19-92)  -> k_bin_count + counting sort + k_records / k_vis_stage + k_vis_place
 //   conv_3d_nputsdriven (conv.cu:144-228)                  -> k_spread_t / k_spread (tile-binned)
 //   interp_3d_nputsdriven (interp.cu:143-227)              -> k_interp_t / k_interp (tile-staged)
 //   w_term_dft + deconv_2d + w_term_deconv + div_n_lm
@@ -218,12 +218,12 @@ __global__ void k_bin_count(DevGeom g, const double *__restrict__ uu, const doub
     if (bad) atomicOr(err, bad);
 }
 
-// Coarse placement: tmp[position] = j with position = the first position of
+// Coarse placement: tmp[q] = j and slot[j] = q with q = the first position of
 // j's bin + a rank claimed on the bin's cursor (bcur starts at bin_start).
 // With one cursor per bin (not per key) the partly written sectors of tmp stay
 // in L2 while the pass runs; k_records then orders each bin by residue.
 __global__ void k_bin_scatter(long long M, const unsigned *__restrict__ keys, int cbits, int *__restrict__ bcur,
-                              int *__restrict__ tmp) {
+                              int *__restrict__ tmp, int *__restrict__ slot) {
     const int lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
     const long long stride = (long long)gridDim.x * blockDim.x;
@@ -236,7 +236,11 @@ __global__ void k_bin_scatter(long long M, const unsigned *__restrict__ keys, in
         int base = 0;
         if (bin != BAD_KEY && lane == leader) base = atomicAdd(bcur + bin, __popc(peers));
         base = __shfl_sync(0xffffffffu, base, leader);
-        if (bin != BAD_KEY) tmp[base + __popc(peers & below)] = (int)j;
+        if (bin != BAD_KEY) {
+            const int q = base + __popc(peers & below);
+            tmp[q] = (int)j;
+            slot[j] = q;                 // the visibility's place in bin order (coalesced)
+        }
     }
 }
 
@@ -356,12 +360,12 @@ __global__ void __launch_bounds__(SCAN_T) k_scan_apply(const int *__restrict__ i
 // segment, by residue: position = a rank claimed on the cursor of their key
 // (kcur = the exclusive scan of the key counts).  Per position: fractional
 // offsets + packed start cell, the w-shift phase e^{i o_c w} (cuft.cu:19-39,
-// FP64) and the input index.
+// FP64) and the input index; per bin-order place q its final position qpos[q].
 template <typename T>
 __global__ void k_records(DevGeom g, const double *__restrict__ uu, const double *__restrict__ vv,
                           const double *__restrict__ ww, const double *__restrict__ foc,
                           const int *__restrict__ tmp, long long M, int *__restrict__ kcur, R<T> *__restrict__ rec,
-                          C<T> *__restrict__ ph, int *__restrict__ idx) {
+                          C<T> *__restrict__ ph, int *__restrict__ idx, int *__restrict__ qpos) {
     const int lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
     const long long stride = (long long)gridDim.x * blockDim.x;
@@ -401,19 +405,42 @@ __global__ void k_records(DevGeom g, const double *__restrict__ uu, const double
         sincos(g.o_center * w_eff(g, ww, row, foc[ch]), &sn, &cs);
         ph[p] = C<T>{(T)cs, (T)sn};
         idx[p] = j;
+        qpos[i] = p;                     // bin order -> final position (same bin segment)
     }
 }
 
-// c = vis * wgt * e^{i o_c w} gathered into bin order (ra_exec.cu:98-104).
+// c = vis * wgt * e^{i o_c w} in sorted order (ra_exec.cu:98-104), as a
+// permutation in two passes with local writes instead of one random gather:
+// k_vis_stage reads the caller's visibilities and weights in input order and
+// writes vis * wgt to each visibility's place in bin order (slot[j]; the
+// places of one bin fill in L2 while the pass runs); k_vis_place moves every
+// value inside its bin's segment to its final, residue-sorted position and
+// applies the w-shift phase there (reads and writes within one bin's segment).
 template <typename T>
-__global__ void k_vis_prep(long long M, const int *__restrict__ idx, const C<T> *__restrict__ ph,
-                           const C<T> *__restrict__ vis, const T *__restrict__ wgt, C<T> *__restrict__ cs) {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < M;
-         i += (long long)gridDim.x * blockDim.x) {
-        int j = idx[i];
-        C<T> v = vis[j], e = ph[i];
-        T wt = wgt ? wgt[j] : (T)1;
-        cs[i] = C<T>{(v.x * e.x - v.y * e.y) * wt, (v.x * e.y + v.y * e.x) * wt};
+__global__ void k_vis_stage(long long j0, long long n, const int *__restrict__ slot, const C<T> *__restrict__ vis,
+                            const T *__restrict__ wgt, C<T> *__restrict__ stage) {
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+         k += (long long)gridDim.x * blockDim.x) {
+        const long long j = j0 + k;
+        C<T> v = vis[j];
+        if (wgt) {
+            const T wt = wgt[j];
+            v.x *= wt;
+            v.y *= wt;
+        }
+        stage[slot[j]] = v;
+    }
+}
+
+template <typename T>
+__global__ void k_vis_place(long long q0, long long n, const int *__restrict__ qpos, const C<T> *__restrict__ stage,
+                            const C<T> *__restrict__ ph, C<T> *__restrict__ cs) {
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+         k += (long long)gridDim.x * blockDim.x) {
+        const long long q = q0 + k;
+        const int p = qpos[q];
+        const C<T> v = stage[q], e = ph[p];
+        cs[p] = C<T>{v.x * e.x - v.y * e.y, v.x * e.y + v.y * e.x};
     }
 }
 
@@ -1402,9 +1429,10 @@ void launch_bin_count(const DevGeom &g, const double *u, const double *v, const 
     k_bin_count<<<grid_for(g.nrow * g.nchan), NTHREADS, 0, st>>>(g, u, v, w, foc, keys, count, err);
 }
 
-void launch_bin_scatter(long long M, const unsigned *keys, int cbits, int *bcur, int *tmp, cudaStream_t st) {
+void launch_bin_scatter(long long M, const unsigned *keys, int cbits, int *bcur, int *tmp, int *slot,
+                        cudaStream_t st) {
     count_launch();
-    k_bin_scatter<<<grid_for(M), NTHREADS, 0, st>>>(M, keys, cbits, bcur, tmp);
+    k_bin_scatter<<<grid_for(M), NTHREADS, 0, st>>>(M, keys, cbits, bcur, tmp, slot);
 }
 
 void launch_bins_from_keys(const int *kstart, const int *total, long long nb, int cbits, int sub, int *bin_start,
@@ -1430,19 +1458,22 @@ void scan_ints(const int *in, int *out, long long n, bool inclusive, int *tmp, c
 
 template <typename T>
 void launch_records(const DevGeom &g, const double *u, const double *v, const double *w, const double *foc,
-                    const int *tmp, long long M, int *kcur, void *rec, void *ph, int *idx, cudaStream_t st) {
+                    const int *tmp, long long M, int *kcur, void *rec, void *ph, int *idx, int *qpos,
+                    cudaStream_t st) {
     count_launch();
     k_records<T><<<grid_for(M), NTHREADS, 0, st>>>(g, u, v, w, foc, tmp, M, kcur, reinterpret_cast<R<T> *>(rec),
-                                                   reinterpret_cast<C<T> *>(ph), idx);
+                                                   reinterpret_cast<C<T> *>(ph), idx, qpos);
 }
 
 template <typename T>
-void launch_vis_prep(long long M, const int *idx, const void *ph, const void *vis, const void *wgt, void *cs,
-                     cudaStream_t st) {
-    count_launch();
-    k_vis_prep<T><<<grid_for(M), NTHREADS, 0, st>>>(M, idx, reinterpret_cast<const C<T> *>(ph),
-                                                    reinterpret_cast<const C<T> *>(vis),
-                                                    reinterpret_cast<const T *>(wgt), reinterpret_cast<C<T> *>(cs));
+void launch_vis_prep(long long j0, long long n, const int *slot, const int *qpos, const void *ph, const void *vis,
+                     const void *wgt, void *stage, void *cs, cudaStream_t st) {
+    if (n <= 0) return;
+    count_launch(2);
+    k_vis_stage<T><<<grid_for(n), NTHREADS, 0, st>>>(j0, n, slot, reinterpret_cast<const C<T> *>(vis),
+                                                     reinterpret_cast<const T *>(wgt), reinterpret_cast<C<T> *>(stage));
+    k_vis_place<T><<<grid_for(n), NTHREADS, 0, st>>>(j0, n, qpos, reinterpret_cast<const C<T> *>(stage),
+                                                     reinterpret_cast<const C<T> *>(ph), reinterpret_cast<C<T> *>(cs));
 }
 
 template <typename T>
@@ -1626,9 +1657,9 @@ void launch_zero_tpad(int nx, int ny, int nf2, int nf3, void *t, cudaStream_t st
 #define CURIG_INSTANTIATE(T)                                                                          \
     template void launch_records<T>(const DevGeom &, const double *, const double *, const double *,  \
                                     const double *, const int *, long long, int *, void *, void *,    \
-                                    int *, cudaStream_t);                                             \
-    template void launch_vis_prep<T>(long long, const int *, const void *, const void *, const void *,\
-                                     void *, cudaStream_t);                                           \
+                                    int *, int *, cudaStream_t);                                      \
+    template void launch_vis_prep<T>(long long, long long, const int *, const int *, const void *,     \
+                                     const void *, const void *, void *, void *, cudaStream_t);       \
     template void launch_vis_out<T>(long long, const int *, const void *, const void *, const void *, \
                                     void *, cudaStream_t);                                            \
     template int launch_spread<T>(const DevGeom &, size_t, const int *, const int *, const int *,     \

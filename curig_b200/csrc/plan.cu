@@ -597,6 +597,7 @@ retry_tiles:
     CU_TRY(dalloc(&p->d_keys_in, M * sizeof(unsigned), st));
     CU_TRY(dalloc(&p->d_kcount, nkeys * sizeof(int), st));
     CU_TRY(dalloc(&p->d_tmp, M * sizeof(int), st));
+    CU_TRY(dalloc(&p->d_slot, M * sizeof(int), st));
     CU_TRY(dalloc(&p->d_bcur, nb * sizeof(int), st));
     CU_TRY(dalloc(&p->d_bin_start, nb * sizeof(int), st));
     CU_TRY(dalloc(&p->d_bin_count, nb * sizeof(int), st));
@@ -608,7 +609,7 @@ retry_tiles:
     scan_ints(p->d_kcount, p->d_kcount, nkeys, false, p->d_scan, st);          // in place: first position per key
     launch_bins_from_keys(p->d_kcount, p->d_scan, nb, cbits, g.sub, p->d_bin_start, p->d_bin_count, p->d_nsub,
                           p->d_bcur, st);
-    launch_bin_scatter(M, p->d_keys_in, cbits, p->d_bcur, p->d_tmp, st);
+    launch_bin_scatter(M, p->d_keys_in, cbits, p->d_bcur, p->d_tmp, p->d_slot, st);
     scan_ints(p->d_nsub, p->d_sub_end, nb, true, p->d_scan, st);
     p->slab_sub_end.assign(nslab, 0);               // last sub-problem end of every slab
     for (int k = 0; k < nslab; ++k)
@@ -624,6 +625,7 @@ retry_tiles:
             herr = 0;
             CU_TRY(cudaMemsetAsync(p->d_err, 0, sizeof(int), st));
             dfree(p->d_keys_in, st); dfree(p->d_kcount, st); dfree(p->d_tmp, st); dfree(p->d_bcur, st);
+            dfree(p->d_slot, st);
             dfree(p->d_bin_start, st); dfree(p->d_bin_count, st);
             dfree(p->d_nsub, st); dfree(p->d_sub_end, st); dfree(p->d_scan, st);
             goto retry_tiles;
@@ -633,13 +635,17 @@ retry_tiles:
     CU_TRY(dalloc(&p->d_rec, M * 4 * (size_t)esize, st));
     CU_TRY(dalloc(&p->d_ph, M * 2 * (size_t)esize, st));
     CU_TRY(dalloc(&p->d_cs, M * 2 * (size_t)esize, st));
+    CU_TRY(dalloc(&p->d_stage, M * 2 * (size_t)esize, st));
     CU_TRY(dalloc(&p->d_idx, M * sizeof(int), st));
+    CU_TRY(dalloc(&p->d_qpos, M * sizeof(int), st));
     // each bin's visibilities (tmp) placed by residue; the key cursors start at
     // the scanned key counts
     if (p->opt.precision)
-        launch_records<float>(g, du, dv, dw, p->d_foc, p->d_tmp, M, p->d_kcount, p->d_rec, p->d_ph, p->d_idx, st);
+        launch_records<float>(g, du, dv, dw, p->d_foc, p->d_tmp, M, p->d_kcount, p->d_rec, p->d_ph, p->d_idx,
+                              p->d_qpos, st);
     else
-        launch_records<double>(g, du, dv, dw, p->d_foc, p->d_tmp, M, p->d_kcount, p->d_rec, p->d_ph, p->d_idx, st);
+        launch_records<double>(g, du, dv, dw, p->d_foc, p->d_tmp, M, p->d_kcount, p->d_rec, p->d_ph, p->d_idx,
+                               p->d_qpos, st);
     dfree(p->d_keys_in, st);
     dfree(p->d_kcount, st);
     dfree(p->d_scan, st);
@@ -759,7 +765,7 @@ static int execute_t(Plan *p, int type, void *d_vis, const void *d_wgt, void *d_
     int s;
     if (type == 1) {
         mark(p, EV_M2D_BEGIN);
-        launch_vis_prep<T>(M, p->d_idx, p->d_ph, d_vis, d_wgt, p->d_cs, st);
+        launch_vis_prep<T>(0, M, p->d_slot, p->d_qpos, p->d_ph, d_vis, d_wgt, p->d_stage, p->d_cs, st);
         mark(p, EV_M2D_PREP);
         CU_TRY(cudaMemsetAsync(p->d_grid, 0, gbytes, st));
         mark(p, EV_M2D_ZERO);
@@ -835,9 +841,7 @@ static int execute_slabs_t(Plan *p, int type, void *d_vis, const void *d_wgt, vo
         for (int k = 0; k < ns; ++k) {
             CU_TRY(wait_slab(k));
             const long long i0 = p->slab_row[k] * p->nchan, i1 = p->slab_row[k + 1] * p->nchan;
-            if (i1 > i0)
-                launch_vis_prep<T>(i1 - i0, p->d_idx + i0, static_cast<const char *>(p->d_ph) + i0 * 2 * sizeof(T),
-                                   d_vis, d_wgt, static_cast<char *>(p->d_cs) + i0 * 2 * sizeof(T), st);
+            launch_vis_prep<T>(i0, i1 - i0, p->d_slot, p->d_qpos, p->d_ph, d_vis, d_wgt, p->d_stage, p->d_cs, st);
             DevGeom gk;
             if (slab_geom(k, gk) &&
                 (s = launch_spread<T>(gk, p->smem, p->d_bin_start, p->d_bin_count, p->d_sub_end, p->d_rec, p->d_cs,
