@@ -189,7 +189,7 @@ __device__ __forceinline__ unsigned vis_key(const DevGeom &g, const double *__re
     VisLoc L;
     e = vis_grid(g, uu, vv, ww, row, foc[ch], gx, gy, gz) ? locate(g, gx, gy, gz, L) : EF_NONFINITE;
     if (e) return BAD_KEY;
-    const unsigned cell = g.cbits ? (unsigned)((L.lz * g.ty + L.ly) * g.tpitch + L.lx) & 31u : 0u;
+    const unsigned cell = (unsigned)((L.lz * g.ty + L.ly) * g.tpitch + L.lx) & ((1u << g.cbits) - 1u);
     const long long slab = g.nslab > 1 ? row * g.nslab / g.nrow : 0;
     return ((unsigned)(slab * g.nbins_slab + L.bin) << g.cbits) | cell;
 }
@@ -383,7 +383,7 @@ __global__ void k_records(DevGeom g, const double *__restrict__ uu, const double
             double gx, gy, gz;
             vis_grid(g, uu, vv, ww, row, foc[ch], gx, gy, gz);
             locate(g, gx, gy, gz, L);
-            const unsigned cell = g.cbits ? (unsigned)((L.lz * g.ty + L.ly) * g.tpitch + L.lx) & 31u : 0u;
+            const unsigned cell = (unsigned)((L.lz * g.ty + L.ly) * g.tpitch + L.lx) & ((1u << g.cbits) - 1u);
             const long long slab = g.nslab > 1 ? row * g.nslab / g.nrow : 0;
             key = ((unsigned)(slab * g.nbins_slab + L.bin) << g.cbits) | cell;
         }
@@ -977,6 +977,262 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
     }
 }
 
+// ------------------------------------------------------------------ FP32 spreader
+// The FP32 tile kernels order each bin by the residue mod 16 of its start
+// cells (NCLS classes; the sort key's residue) and give every class two lanes
+// of a warp: lane 2k + f takes elements f, f + 2, f + 4, ... of class k.  A
+// tile cell's two words (re, im, or the high and low word of one component)
+// are adjacent, so cell c covers banks 2c and 2c + 1 (mod 32): cells of
+// different classes never share a bank, and the two lanes of one class write
+// their cells' words in opposite order (lane f = 0: first word, then second;
+// f = 1: second, then first), so they never meet in one instruction either.
+// Every atomic instruction is one shared-memory wavefront; a warp step idles
+// the lanes of classes that have run out (steps = the largest class / 2).
+constexpr int NCLS = 16;
+
+// Class boundaries of a chunk whose positions (start + k * stride, k < n) are
+// sorted by class: cls[q] = first k of class q, cls[NCLS] = n.  All threads
+// call it; the caller synchronises before reading cls.
+template <typename RT>
+__device__ __forceinline__ void chunk_classes(const RT *__restrict__ rec, int start, int stride, int n, int txy,
+                                              int tx, int *cls, int nthreads) {
+    auto klass = [&](int k) {
+        const int cb = cell_bits(rec[start + k * stride].w);
+        return ((((cb >> 20) & 0xfff) * txy + ((cb >> 10) & 0x3ff) * tx + (cb & 0x3ff)) & (NCLS - 1));
+    };
+    for (int k = threadIdx.x; k < n; k += nthreads) {
+        const int c = klass(k);
+        const int prev = k ? klass(k - 1) : -1;
+        for (int q = prev + 1; q <= c; ++q) cls[q] = k;
+        if (k == n - 1)
+            for (int q = c + 1; q <= NCLS; ++q) cls[q] = n;
+    }
+}
+
+// Warp steps of the class schedule: the largest class, halved (rounded up).
+__device__ __forceinline__ int class_steps(const int *cls, int n) {
+    int t = 0;
+#pragma unroll
+    for (int q = 0; q < NCLS; ++q) t = max(t, (min(max(cls[q + 1] - cls[q], 0), n) + 1) >> 1);
+    return t;
+}
+
+// First position and size of class q, clamped to the chunk [0, n) (memory
+// safety only: the sort makes the boundaries monotonic).
+__device__ __forceinline__ void class_range(const int *cls, int q, int n, int &c0, int &nk) {
+    c0 = min(max(cls[q], 0), n);
+    nk = min(max(cls[q + 1] - c0, 0), n - c0);
+}
+
+// FP32 tile accumulation (g.smode): 2 one-word int32 fixed point [re, im] per
+// cell; 0 exact two-word int32 fixed point, plane A [re high, re low] and plane
+// B [im high, im low] per cell; 1 float atomics [re, im] per cell.  Scale,
+// overflow bound and chunk statistics as in k_spread_t.
+template <int KW>
+__global__ void __launch_bounds__(TTHREADS, 2)
+k_spread_f32(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__ bin_count,
+             const int *__restrict__ sub_end, const float4 *__restrict__ rec, const float2 *__restrict__ cs,
+             float2 *__restrict__ grid, const WinTab<float> tab) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ float redbuf[TWARPS];
+    __shared__ int cls[NCLS + 1];
+    const int ntile = g.tpitch * g.ty * g.tz;           // cells; tile [tz][ty][tpitch], columns >= tx stay 0
+    const int mode = g.smode;
+    const bool two = mode == 0, one = mode == 2, fixed = mode != 1;
+    int *wA = reinterpret_cast<int *>(smem);            // [ntile][2]
+    int *wB = wA + 2 * ntile;                           // two-word: [ntile][2]
+    const int nwords = (two ? 4 : 2) * ntile;
+    float *colsum = reinterpret_cast<float *>(wA + nwords);   // one word: per start column sum|c|
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int total = g.sub_hi ? g.sub_hi : sub_end[g.nbins - 1];
+    const int tx = g.tpitch, txy = g.tpitch * g.ty;
+    const int klass = lane >> 1, f = lane & 1;
+    for (int s = g.sub_lo + blockIdx.x; s < total; s += gridDim.x) {
+        long long b;
+        int start, stride, n;
+        sub_range(g, bin_start, bin_count, sub_end, s, b, start, stride, n);
+        const long long bl = b % g.nbins_slab;
+        const long long bxi = bl % g.nbx, byi = (bl / g.nbx) % g.nby, bzi = bl / ((long long)g.nbx * g.nby);
+        const int ox = (int)bxi * g.bx - g.hkw, oy = (int)byi * g.by - g.hkw;
+        const int oz = g.zpad ? (int)bzi * g.bz - g.hkw : 0;
+        const int shift = ox & 1, x_al = ox - shift;
+        float4 *tv = reinterpret_cast<float4 *>(smem);
+        for (int e = threadIdx.x; e < nwords / 4; e += TTHREADS) tv[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (one)
+            for (int e = threadIdx.x; e < txy; e += TTHREADS) colsum[e] = 0.f;
+        __syncthreads();
+        // chunk statistics: largest component of c, one word: start-column sums
+        float m = 0.f;
+        if (fixed)
+            for (int k = threadIdx.x; k < n; k += TTHREADS) {
+                const int i = start + k * stride;
+                const float2 c = cs[i];
+                const float mc = fmaxf(fabsf(c.x), fabsf(c.y));
+                m = fmaxf(m, mc);
+                if (one) {
+                    const int cb = cell_bits(rec[i].w);
+                    atomicAdd(colsum + ((cb >> 10) & 0x3ff) * tx + (cb & 0x3ff), mc);
+                }
+            }
+        chunk_classes(rec, start, stride, n, txy, tx, cls, TTHREADS);
+        float q = 1.f;
+        double qinv = 1.0;
+        if (fixed) {
+            for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+            if (lane == 0) redbuf[warp] = m;
+            __syncthreads();
+            m = 0.f;
+#pragma unroll
+            for (int w = 0; w < TWARPS; ++w) m = fmaxf(m, redbuf[w]);
+            int k;
+            if (two) {
+                int e = m > 0.f ? ilogb(m) + 1 : 0;       // 2^(e-1) <= m < 2^e
+                k = FIX_BITS - e;
+            } else {
+                float bmax = 0.f;                         // largest kw x kw box sum of the start columns
+                for (int e = threadIdx.x; e < txy; e += TTHREADS) {
+                    const int x = e % tx, y = e / tx;
+                    float a = 0.f;
+                    for (int yy = max(0, y - KW + 1); yy <= y; ++yy)
+                        for (int xx = max(0, x - KW + 1); xx <= x; ++xx) a += colsum[yy * tx + xx];
+                    bmax = fmaxf(bmax, a);
+                }
+                for (int o = 16; o > 0; o >>= 1) bmax = fmaxf(bmax, __shfl_xor_sync(0xffffffffu, bmax, o));
+                __syncthreads();                          // every thread has read redbuf
+                if (lane == 0) redbuf[warp] = bmax;
+                __syncthreads();
+                float bb = 0.f;
+#pragma unroll
+                for (int w = 0; w < TWARPS; ++w) bb = fmaxf(bb, redbuf[w]);
+                const int em = m > 0.f ? ilogb(m * g.wmax3) + 1 : 0;
+                const int es = bb > 0.f ? ilogb(bb * g.wmax3) + 1 : 0;
+                k = min(22 - em, 30 - es);
+            }
+            k = min(k, 120);
+            q = (float)ldexp(1.0, k);
+            qinv = ldexp(1.0, -k);
+        }
+        __syncthreads();
+        // class schedule: lane 2k + f, element 2t + f of class k at step t;
+        // chunks of few steps split each visibility's w-planes into S parts
+        const int T = class_steps(cls, n);
+        int c0, nk;
+        class_range(cls, klass, n, c0, nk);
+        const int KZ = g.no_w ? 1 : KW;
+        const int S = max(1, min(KZ, TWARPS / max(T, 1)));
+        for (int u = warp; u < T * S; u += TWARPS) {
+            const int t = u / S, part = u - t * S;
+            const int e = 2 * t + f;
+            if (e >= nk) continue;
+            const int i = start + (c0 + e) * stride;
+            const int dz0 = part * KZ / S, dz1 = (part + 1) * KZ / S;
+            const float4 r = rec[i];
+            float2 c = cs[i];
+            float kx[KW], ky[KW];
+#pragma unroll
+            for (int d = 0; d < KW; ++d) {
+                kx[d] = win_tap<float>(g, tab, r.x, d);
+                ky[d] = win_tap<float>(g, tab, r.y, d);
+            }
+            const int cb = cell_bits(r.w);
+            const int cell = ((cb >> 20) & 0xfff) * txy + ((cb >> 10) & 0x3ff) * tx + (cb & 0x3ff) + shift;
+            const int p0 = 2 * cell + f, p1 = 2 * cell + 1 - f;   // this lane's first / second word
+            c.x *= q;
+            c.y *= q;
+#pragma unroll 1
+            for (int dz = dz0; dz < dz1; ++dz) {
+                const float kz = g.no_w ? 1.f : win_tap<float>(g, tab, r.z, dz);
+                const float cr = c.x * kz, ci = c.y * kz;
+                const int oz = 2 * dz * txy;
+#pragma unroll
+                for (int dy = 0; dy < KW; ++dy) {
+                    const float ar = cr * ky[dy], ai = ci * ky[dy];
+                    const int o = oz + 2 * dy * tx;
+                    if (one) {
+                        const float a0 = f ? ai : ar, a1 = f ? ar : ai;
+                        int *r0 = wA + p0 + o, *r1 = wA + p1 + o;
+#pragma unroll
+                        for (int dx = 0; dx < KW; ++dx) {
+                            atomicAdd(r0 + 2 * dx, round_fix(a0, kx[dx]));
+                            atomicAdd(r1 + 2 * dx, round_fix(a1, kx[dx]));
+                        }
+                    } else if (two) {
+                        int *a0 = wA + p0 + o, *a1 = wA + p1 + o, *b0 = wB + p0 + o, *b1 = wB + p1 + o;
+#pragma unroll
+                        for (int dx = 0; dx < KW; ++dx) {
+                            int hr, lr, hi, li;
+                            split_fix(ar * kx[dx], hr, lr);
+                            split_fix(ai * kx[dx], hi, li);
+                            atomicAdd(a0 + 2 * dx, f ? lr : hr);
+                            atomicAdd(a1 + 2 * dx, f ? hr : lr);
+                            atomicAdd(b0 + 2 * dx, f ? li : hi);
+                            atomicAdd(b1 + 2 * dx, f ? hi : li);
+                        }
+                    } else {
+                        const float a0 = f ? ai : ar, a1 = f ? ar : ai;
+                        float *r0 = reinterpret_cast<float *>(wA) + p0 + o, *r1 = reinterpret_cast<float *>(wA) + p1 + o;
+#pragma unroll
+                        for (int dx = 0; dx < KW; ++dx) {
+                            atomicAdd(r0 + 2 * dx, a0 * kx[dx]);
+                            atomicAdd(r1 + 2 * dx, a1 * kx[dx]);
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        // Flush: cell pairs in memory order (one 16-byte shared load per pair
+        // and plane); non-wrapping tiles add a pair with one 16-byte vector
+        // reduction (grid column x_al + 2k is even), wrapping tiles cell by cell.
+        {
+            const float qf = (float)qinv, qf18 = (float)(qinv * 262144.0);
+            const bool xin = x_al >= 0 && x_al + tx <= g.nf1;
+            const int ty = g.ty, npair = ntile >> 1, hp = tx >> 1;
+            const int q0 = TTHREADS / hp;
+            const int sx = TTHREADS - q0 * hp, sy = q0 % ty, sz = q0 / ty;
+            int xp = threadIdx.x % hp, yz = threadIdx.x / hp;
+            int y = yz % ty, z = yz / ty;
+            for (int pr = threadIdx.x; pr < npair; pr += TTHREADS) {
+                float2 v0, v1;
+                if (one) {
+                    const int4 a = reinterpret_cast<const int4 *>(wA)[pr];
+                    v0 = make_float2(__int2float_rn(a.x) * qf, __int2float_rn(a.y) * qf);
+                    v1 = make_float2(__int2float_rn(a.z) * qf, __int2float_rn(a.w) * qf);
+                } else if (two) {
+                    const int4 a = reinterpret_cast<const int4 *>(wA)[pr], bq = reinterpret_cast<const int4 *>(wB)[pr];
+                    v0 = make_float2(fmaf(__int2float_rn(a.x), qf18, __int2float_rn(a.y) * qf),
+                                     fmaf(__int2float_rn(bq.x), qf18, __int2float_rn(bq.y) * qf));
+                    v1 = make_float2(fmaf(__int2float_rn(a.z), qf18, __int2float_rn(a.w) * qf),
+                                     fmaf(__int2float_rn(bq.z), qf18, __int2float_rn(bq.w) * qf));
+                } else {
+                    const float4 a = reinterpret_cast<const float4 *>(wA)[pr];
+                    v0 = make_float2(a.x, a.y);
+                    v1 = make_float2(a.z, a.w);
+                }
+                const bool nz0 = v0.x != 0.f || v0.y != 0.f, nz1 = v1.x != 0.f || v1.y != 0.f;
+                if (nz0 || nz1) {
+                    const int gy = wrap3(oy + y, g.nf2);
+                    const int gz = g.zpad ? wrap3(oz + z, g.nf3) : z;
+                    float2 *grow = grid + ((long long)gz * g.nf2 + gy) * g.nf1;
+                    const int col = 2 * xp;
+                    if (xin) {
+                        red_add_v4(reinterpret_cast<float *>(grow + x_al + col), v0.x, v0.y, v1.x, v1.y);
+                    } else {
+                        if (nz0) atomic_add_c(grow + wrap3(x_al + col, g.nf1), v0);
+                        if (nz1) atomic_add_c(grow + wrap3(x_al + col + 1, g.nf1), v1);
+                    }
+                }
+                xp += sx;
+                if (xp >= hp) { xp -= hp; ++y; }
+                y += sy;
+                z += sz;
+                if (y >= ty) { y -= ty; ++z; }
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // vis[idx[i]] = value * wgt * e^{-i o_c w} (ra_exec.cu:56-89; the weight
 // multiplies, utils.cu:189): the scatter of dirty2ms back to input order.
 template <typename T>
@@ -1083,6 +1339,7 @@ k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ C<T> partial[IT];      // per (column, part, lane) sums of split visibilities
     __shared__ unsigned long long bar;      // TMA completion barrier
+    __shared__ int cls[NCLS + 1];           // FP32: class boundaries of the chunk
     C<T> *tile = reinterpret_cast<C<T> *>(smem);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int total = g.sub_hi ? g.sub_hi : sub_end[g.nbins - 1];   // sub-problem window [sub_lo, total)
@@ -1106,6 +1363,8 @@ k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
         // interior tiles (no periodic wrap) in one TMA box; the rest with plain loads
         const bool inner = g.use_tma && x_al >= 0 && x_al + g.tpitch <= g.nf1 && oy >= 0 &&
                            oy + g.ty <= g.nf2 && (!g.zpad || (oz >= 0 && oz + g.tz <= g.nf3));
+        // FP32 class schedule (the classes are read while the tile loads)
+        if constexpr (sizeof(T) == 4) chunk_classes(rec, start, stride, n, txy, tx, cls, IT);
         if (inner) {
             if (threadIdx.x == 0) {
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // earlier reads of the tile
@@ -1126,14 +1385,29 @@ k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
             load_tile<T, IW>(g, grid, tile, x_al, oy, oz, warp, lane);
             __syncthreads();
         }
-        // same lane / position map and w-plane split as k_spread_t
-        const int L = (n + 31) >> 5;
+        // lane / position map and w-plane split of the spreader: FP32 the class
+        // schedule (two lanes per class: a warp's 8-byte loads take the minimum
+        // two wavefronts), FP64 the 32 x L matrix of residue-sorted positions
         const int KZ = g.no_w ? 1 : KW;
+        int L, c0 = 0, nk = 0;
+        if constexpr (sizeof(T) == 4) {
+            L = class_steps(cls, n);
+            class_range(cls, lane >> 1, n, c0, nk);
+        } else {
+            L = (n + 31) >> 5;
+        }
         const int S = max(1, min(KZ, IW / max(L, 1)));
         for (int u = warp; u < L * S; u += IW) {
             const int k = u / S, part = u - k * S;
-            const int m = lane * L + k;
-            if (m >= n) continue;
+            int m;
+            if constexpr (sizeof(T) == 4) {
+                const int e = 2 * k + (lane & 1);
+                if (e >= nk) continue;
+                m = c0 + e;
+            } else {
+                m = lane * L + k;
+                if (m >= n) continue;
+            }
             const int i = start + m * stride;
             const int dz0 = part * KZ / S, dz1 = (part + 1) * KZ / S;
             R<T> r = rec[i];
@@ -1175,7 +1449,18 @@ k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
         if (S > 1) {                                   // L * S <= IW: one pass
             __syncthreads();
             for (int m = threadIdx.x; m < n; m += IT) {
-                const int ln = m / L, k = m - ln * L;
+                int ln, k;
+                if constexpr (sizeof(T) == 4) {          // the lane and step that held position m
+                    int q = 0;
+                    while (q < NCLS - 1 && cls[q + 1] <= m) ++q;
+                    const int e = m - cls[q];
+                    if (e < 0 || (e >> 1) >= L) continue;   // (unreachable for sorted chunks)
+                    ln = 2 * q + (e & 1);
+                    k = e >> 1;
+                } else {
+                    ln = m / L;
+                    k = m - ln * L;
+                }
                 C<T> v = partial[(k * S) * 32 + ln];
                 for (int p = 1; p < S; ++p) {
                     C<T> w = partial[(k * S + p) * 32 + ln];
@@ -1522,7 +1807,14 @@ static int launch_spread_kw(const DevGeom &g, size_t smem, const int *bs, const 
                             const void *rec, void *cs, void *grid, const double *wc, const double *ht,
                             const VisIO &io, long long M, int nsm, cudaStream_t st) {
     int blocks = 0, s;
-    if constexpr (KW > 0) {
+    if constexpr (KW > 0 && sizeof(T) == 4) {
+        auto kern = k_spread_f32<KW>;
+        if ((s = launch_persistent(kern, smem, nsm, blocks, TTHREADS))) return s;
+        count_launch();
+        kern<<<blocks, TTHREADS, smem, st>>>(g, bs, bc, se, reinterpret_cast<const float4 *>(rec),
+                                             reinterpret_cast<const float2 *>(cs), reinterpret_cast<float2 *>(grid),
+                                             make_tab<float>(g, ht));
+    } else if constexpr (KW > 0) {
         auto kern = k_spread_t<T, KW>;
         if ((s = launch_persistent(kern, smem, nsm, blocks, TTHREADS))) return s;
         count_launch();

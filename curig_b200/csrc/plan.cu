@@ -590,8 +590,11 @@ retry_tiles:
     const long long nb = g.nbins;
     int binbits = 1;
     while ((1LL << binbits) < nb) ++binbits;
-    int cbits = binbits + 5 <= 31 ? 5 : 0;               // start-cell bank residue; bin-only keys beyond
-    if (binbits > 31) return ERR_UNSUPPORTED;
+    // start-cell residue in the key: mod 16 for the FP32 tile kernels (their
+    // class schedule needs it), mod 32 for the FP64 ones (bin-only keys beyond 31 bits)
+    const bool f32tile = esize == 4 && g.kw <= TAB_KW;
+    int cbits = f32tile ? 4 : (binbits + 5 <= 31 ? 5 : 0);
+    if (binbits > 31 || binbits + cbits > 31) return ERR_UNSUPPORTED;
     g.cbits = cbits;
     const long long nkeys = nb << cbits;
     CU_TRY(dalloc(&p->d_keys_in, M * sizeof(unsigned), st));
