@@ -284,7 +284,8 @@ void plan_release_points(Plan *p) {
     dfree(p->d_wcoef, st); dfree(p->d_bin_count, st); dfree(p->d_bin_start, st);
     dfree(p->d_nsub, st); dfree(p->d_sub_end, st); dfree(p->d_keys_in, st); dfree(p->d_kcount, st);
     dfree(p->d_idx, st); dfree(p->d_err, st); dfree(p->d_keys, st); dfree(p->d_scan, st);
-    dfree(p->d_tmp, st); dfree(p->d_bcur, st);
+    dfree(p->d_tmp, st); dfree(p->d_bcur, st); dfree(p->d_slot, st); dfree(p->d_qpos, st); dfree(p->d_stage, st);
+    dfree(p->d_dslot, st); dfree(p->d_jlist, st);
     dfree(p->d_rec, st); dfree(p->d_ph, st); dfree(p->d_cs, st); dfree(p->d_grid, st);
     dfree(p->d_tgrid, st);
     fft_release(p);
@@ -649,6 +650,21 @@ retry_tiles:
     else
         launch_records<double>(g, du, dv, dw, p->d_foc, p->d_tmp, M, p->d_kcount, p->d_rec, p->d_ph, p->d_idx,
                                p->d_qpos, st);
+    // dirty2ms output staging: windows of 2^18 input indices inside each row slab
+    {
+        long long maxslab = 0;
+        for (int k = 0; k < nslab; ++k) maxslab = std::max(maxslab, (p->slab_row[k + 1] - p->slab_row[k]) * nchan);
+        const long long bmax = (maxslab + (1LL << 18) - 1) >> 18;
+        const long long ncur = (long long)nslab * bmax;
+        CU_TRY(dalloc(&p->d_dslot, M * sizeof(int), st));
+        CU_TRY(dalloc(&p->d_jlist, M * sizeof(int), st));
+        if (ncur > nb) {                                // cursors: the bin cursors' buffer when it is large enough
+            dfree(p->d_bcur, st);
+            CU_TRY(dalloc(&p->d_bcur, ncur * sizeof(int), st));
+        }
+        CU_TRY(cudaMemsetAsync(p->d_bcur, 0, ncur * sizeof(int), st));
+        launch_out_maps(M, p->d_idx, nrow, nchan, nslab, (int)bmax, p->d_bcur, p->d_dslot, p->d_jlist, st);
+    }
     dfree(p->d_keys_in, st);
     dfree(p->d_kcount, st);
     dfree(p->d_scan, st);
@@ -772,10 +788,8 @@ static int execute_t(Plan *p, int type, void *d_vis, const void *d_wgt, void *d_
         mark(p, EV_M2D_PREP);
         CU_TRY(cudaMemsetAsync(p->d_grid, 0, gbytes, st));
         mark(p, EV_M2D_ZERO);
-        const VisIO io{p->d_idx, p->d_ph, d_wgt, d_vis};
         s = launch_spread<T>(g, p->smem, p->d_bin_start, p->d_bin_count, p->d_sub_end, p->d_rec, p->d_cs,
-                             p->d_grid, p->d_wcoef, p->htab.empty() ? nullptr : p->htab.data(), io, M, p->nsm,
-                             st);
+                             p->d_grid, p->d_wcoef, p->htab.empty() ? nullptr : p->htab.data(), p->nsm, st);
         if (s) return s;
         mark(p, EV_M2D_SPREAD);
         s = plane_fft<T>(p, CUFFT_INVERSE, true);    // +1, cuft.cu:127-143
@@ -791,13 +805,13 @@ static int execute_t(Plan *p, int type, void *d_vis, const void *d_wgt, void *d_
         s = plane_fft<T>(p, CUFFT_FORWARD, false);   // -1
         if (s) return s;
         mark(p, EV_D2M_FFT);
-        const VisIO io{p->d_idx, p->d_ph, d_wgt, d_vis};
         s = launch_interp<T>(g, p->smem_interp, p->d_bin_start, p->d_bin_count, p->d_sub_end, p->d_rec, p->d_grid,
-                             p->d_cs, p->d_wcoef, p->htab.empty() ? nullptr : p->htab.data(), io, M, &p->tmap,
-                             p->d_err, p->nsm, st);
+                             p->d_cs, p->d_wcoef, p->htab.empty() ? nullptr : p->htab.data(), &p->tmap, p->d_err,
+                             p->nsm, st);
         if (s) return s;
         mark(p, EV_D2M_INTERP);
-        mark(p, EV_D2M_END);                     // the scatter runs inside the interpolator
+        launch_vis_out<T>(0, M, p->d_dslot, p->d_jlist, p->d_cs, p->d_ph, d_wgt, p->d_stage, d_vis, st);
+        mark(p, EV_D2M_END);
     }
     CU_TRY(cudaGetLastError());
     return OK;
@@ -835,7 +849,6 @@ static int execute_slabs_t(Plan *p, int type, void *d_vis, const void *d_wgt, vo
         gk.sub_hi = p->slab_sub_end[k];
         return gk.sub_hi > gk.sub_lo;
     };
-    const VisIO io{p->d_idx, p->d_ph, d_wgt, d_vis};
     const double *ht = p->htab.empty() ? nullptr : p->htab.data();
     int s;
     if (type == 1) {
@@ -848,7 +861,7 @@ static int execute_slabs_t(Plan *p, int type, void *d_vis, const void *d_wgt, vo
             DevGeom gk;
             if (slab_geom(k, gk) &&
                 (s = launch_spread<T>(gk, p->smem, p->d_bin_start, p->d_bin_count, p->d_sub_end, p->d_rec, p->d_cs,
-                                      p->d_grid, p->d_wcoef, ht, io, p->nrow * p->nchan, p->nsm, st)))
+                                      p->d_grid, p->d_wcoef, ht, p->nsm, st)))
                 return s;
         }
         if ((s = plane_fft<T>(p, CUFFT_INVERSE, true))) return s;
@@ -864,9 +877,10 @@ static int execute_slabs_t(Plan *p, int type, void *d_vis, const void *d_wgt, vo
             DevGeom gk;
             if (slab_geom(k, gk) &&
                 (s = launch_interp<T>(gk, p->smem_interp, p->d_bin_start, p->d_bin_count, p->d_sub_end, p->d_rec,
-                                      p->d_grid, p->d_cs, p->d_wcoef, ht, io, p->nrow * p->nchan, &p->tmap,
-                                      p->d_err, p->nsm, st)))
+                                      p->d_grid, p->d_cs, p->d_wcoef, ht, &p->tmap, p->d_err, p->nsm, st)))
                 return s;
+            const long long i0 = p->slab_row[k] * p->nchan, i1 = p->slab_row[k + 1] * p->nchan;
+            launch_vis_out<T>(i0, i1 - i0, p->d_dslot, p->d_jlist, p->d_cs, p->d_ph, d_wgt, p->d_stage, d_vis, st);
             CU_TRY(done_slab(k));
         }
     }

@@ -68,7 +68,9 @@ struct Plan {
     int *d_idx = nullptr;                               // input index per sorted position (bin order)
     int *d_slot = nullptr;                              // bin-order place of each input visibility
     int *d_qpos = nullptr;                              // final sorted position of each bin-order place
-    void *d_stage = nullptr;                            // visibilities in bin order (ms2dirty staging)
+    void *d_stage = nullptr;                            // visibilities in bin / staging order (both directions)
+    int *d_dslot = nullptr;                             // dirty2ms: staging place of each sorted position
+    int *d_jlist = nullptr;                             // dirty2ms: input index of each staging place
     int *d_err = nullptr;
     unsigned long long *d_keys = nullptr;
     int *d_scan = nullptr;                              // scan temporaries (total, block sums)
@@ -168,22 +170,23 @@ void launch_records(const DevGeom &g, const double *u, const double *v, const do
 template <typename T>
 void launch_vis_prep(long long j0, long long n, const int *slot, const int *qpos, const void *ph, const void *vis,
                      const void *wgt, void *stage, void *cs, cudaStream_t st);
+// dirty2ms output: staging places of the sorted positions (set points), then
+// vis[j] = os[p] * conj(ph[p]) * wgt[j] for the sorted positions [p0, p0 + n)
+// of a row slab (whose staging places fill the same range).
+void launch_out_maps(long long M, const int *idx, long long nrow, int nchan, int nslab, int bmax, int *ocur,
+                     int *dslot, int *jlist, cudaStream_t st);
 template <typename T>
-void launch_vis_out(long long M, const int *idx, const void *ph, const void *os, const void *wgt, void *vis,
-                    cudaStream_t st);
-// Tile kernels.  launch_spread spreads cs (vis * wgt * phase in bin order,
-// written by k_vis_prep); launch_interp interpolates and scatters
-// wgt * conj(phase) * value to io.vis — inside the tile kernel for widths up to
-// 12 (the random writes overlap the shared-memory work), through os and
-// k_vis_out for the generic wider kernel.
+void launch_vis_out(long long p0, long long n, const int *dslot, const int *jlist, const void *os, const void *ph,
+                    const void *wgt, void *stage, void *vis, cudaStream_t st);
+// Tile kernels: launch_spread spreads cs (vis * wgt * phase in sorted order);
+// launch_interp writes the interpolated values to os in sorted order.
 template <typename T>
 int launch_spread(const DevGeom &g, size_t smem, const int *bs, const int *bc, const int *se,
-                  const void *rec, void *cs, void *grid, const double *wc, const double *ht, VisIO io,
-                  long long M, int nsm, cudaStream_t st);
+                  const void *rec, void *cs, void *grid, const double *wc, const double *ht, int nsm, cudaStream_t st);
 template <typename T>
 int launch_interp(const DevGeom &g, size_t smem, const int *bs, const int *bc, const int *se,
-                  const void *rec, const void *grid, void *os, const double *wc, const double *ht, VisIO io,
-                  long long M, const CUtensorMap *tmap, int *err, int nsm, cudaStream_t st);
+                  const void *rec, const void *grid, void *os, const double *wc, const double *ht,
+                  const CUtensorMap *tmap, int *err, int nsm, cudaStream_t st);
 template <typename T>
 void launch_correct_m2d(const DevCorr &cc, const void *grid, void *dirty, cudaStream_t st);
 template <typename T>
