@@ -2,7 +2,7 @@
 //
 // Replaces, on the ms2dirty / dirty2ms path of the reference:
 //   get_effective_coordinate + rescaling + pre_stage_1/2 + transpose
-//       (precomp.cu:48-79, utils.cu:56-154, cuft.cu:19-92)  -> k_bin_count + counting sort + k_records / k_vis_stage + k_vis_place
+//       (precomp.cu:48-79, utils.cu:56-154, cuft.cu:19-92)  -> k_bin_keys + radix sort + k_records / k_vis_prep
 //   conv_3d_nputsdriven (conv.cu:144-228)                  -> k_spread_t / k_spread (tile-binned)
 //   interp_3d_nputsdriven (interp.cu:143-227)              -> k_interp_t / k_interp (tile-staged)
 //   w_term_dft + deconv_2d + w_term_deconv + div_n_lm
@@ -218,12 +218,12 @@ __global__ void k_bin_count(DevGeom g, const double *__restrict__ uu, const doub
     if (bad) atomicOr(err, bad);
 }
 
-// Coarse placement: tmp[q] = j and slot[j] = q with q = the first position of
+// Coarse placement: tmp[position] = j with position = the first position of
 // j's bin + a rank claimed on the bin's cursor (bcur starts at bin_start).
 // With one cursor per bin (not per key) the partly written sectors of tmp stay
 // in L2 while the pass runs; k_records then orders each bin by residue.
 __global__ void k_bin_scatter(long long M, const unsigned *__restrict__ keys, int cbits, int *__restrict__ bcur,
-                              int *__restrict__ tmp, int *__restrict__ slot) {
+                              int *__restrict__ tmp) {
     const int lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
     const long long stride = (long long)gridDim.x * blockDim.x;
@@ -236,11 +236,7 @@ __global__ void k_bin_scatter(long long M, const unsigned *__restrict__ keys, in
         int base = 0;
         if (bin != BAD_KEY && lane == leader) base = atomicAdd(bcur + bin, __popc(peers));
         base = __shfl_sync(0xffffffffu, base, leader);
-        if (bin != BAD_KEY) {
-            const int q = base + __popc(peers & below);
-            tmp[q] = (int)j;
-            slot[j] = q;                 // the visibility's place in bin order (coalesced)
-        }
+        if (bin != BAD_KEY) tmp[base + __popc(peers & below)] = (int)j;
     }
 }
 
@@ -360,12 +356,12 @@ __global__ void __launch_bounds__(SCAN_T) k_scan_apply(const int *__restrict__ i
 // segment, by residue: position = a rank claimed on the cursor of their key
 // (kcur = the exclusive scan of the key counts).  Per position: fractional
 // offsets + packed start cell, the w-shift phase e^{i o_c w} (cuft.cu:19-39,
-// FP64) and the input index; per bin-order place q its final position qpos[q].
+// FP64) and the input index.
 template <typename T>
 __global__ void k_records(DevGeom g, const double *__restrict__ uu, const double *__restrict__ vv,
                           const double *__restrict__ ww, const double *__restrict__ foc,
                           const int *__restrict__ tmp, long long M, int *__restrict__ kcur, R<T> *__restrict__ rec,
-                          C<T> *__restrict__ ph, int *__restrict__ idx, int *__restrict__ qpos) {
+                          C<T> *__restrict__ ph, int *__restrict__ idx) {
     const int lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
     const long long stride = (long long)gridDim.x * blockDim.x;
@@ -405,117 +401,33 @@ __global__ void k_records(DevGeom g, const double *__restrict__ uu, const double
         sincos(g.o_center * w_eff(g, ww, row, foc[ch]), &sn, &cs);
         ph[p] = C<T>{(T)cs, (T)sn};
         idx[p] = j;
-        qpos[i] = p;                     // bin order -> final position (same bin segment)
     }
 }
 
-// c = vis * wgt * e^{i o_c w} in sorted order (ra_exec.cu:98-104), as a
-// permutation in two passes with local writes instead of one random gather:
-// k_vis_stage reads the caller's visibilities and weights in input order and
-// writes vis * wgt to each visibility's place in bin order (slot[j]; the
-// places of one bin fill in L2 while the pass runs); k_vis_place moves every
-// value inside its bin's segment to its final, residue-sorted position and
-// applies the w-shift phase there (reads and writes within one bin's segment).
+// c = vis * wgt * e^{i o_c w} gathered into bin order (ra_exec.cu:98-104).
 template <typename T>
-__global__ void k_vis_stage(long long j0, long long n, const int *__restrict__ slot, const C<T> *__restrict__ vis,
-                            const T *__restrict__ wgt, C<T> *__restrict__ stage) {
-    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
-         k += (long long)gridDim.x * blockDim.x) {
-        const long long j = j0 + k;
-        C<T> v = vis[j];
-        if (wgt) {
-            const T wt = wgt[j];
-            v.x *= wt;
-            v.y *= wt;
-        }
-        stage[slot[j]] = v;
+__global__ void k_vis_prep(long long M, const int *__restrict__ idx, const C<T> *__restrict__ ph,
+                           const C<T> *__restrict__ vis, const T *__restrict__ wgt, C<T> *__restrict__ cs) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < M;
+         i += (long long)gridDim.x * blockDim.x) {
+        int j = idx[i];
+        C<T> v = vis[j], e = ph[i];
+        T wt = wgt ? wgt[j] : (T)1;
+        cs[i] = C<T>{(v.x * e.x - v.y * e.y) * wt, (v.x * e.y + v.y * e.x) * wt};
     }
 }
 
+// vis = interp * wgt * e^{-i o_c w} scattered back to input order
+// (ra_exec.cu:56-89; the reference's weight "divide" invoker multiplies, utils.cu:189).
 template <typename T>
-__global__ void k_vis_place(long long q0, long long n, const int *__restrict__ qpos, const C<T> *__restrict__ stage,
-                            const C<T> *__restrict__ ph, C<T> *__restrict__ cs) {
-    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
-         k += (long long)gridDim.x * blockDim.x) {
-        const long long q = q0 + k;
-        const int p = qpos[q];
-        const C<T> v = stage[q], e = ph[p];
-        cs[p] = C<T>{v.x * e.x - v.y * e.y, v.x * e.y + v.y * e.x};
-    }
-}
-
-// vis = interp * wgt * e^{-i o_c w} (ra_exec.cu:56-89; the reference's weight
-// "divide" invoker multiplies, utils.cu:189), back in input order, as a
-// permutation in two passes with local writes: k_out_stage reads the
-// interpolated values in sorted order and writes value * conj(phase) to the
-// visibility's staging place; k_out_place writes vis[j] = staged value *
-// wgt[j] in staging order.  The staging places (k_out_maps, at set points)
-// group the visibilities by windows of 2^OUT_SHIFT consecutive input indices
-// inside their row slab, in the order of sorted position, so the first pass
-// writes about one open sector per window and the second writes and reads
-// the caller's arrays one window at a time.
-constexpr int OUT_SHIFT = 18;
-
-__device__ __forceinline__ long long slab_first_row_dev(long long nrow, int nslab, int k) {
-    return ((long long)k * nrow + nslab - 1) / nslab;
-}
-
-__global__ void k_out_maps(long long M, const int *__restrict__ idx, long long nrow, int nchan, int nslab, int bmax,
-                           int *__restrict__ ocur, int *__restrict__ dslot, int *__restrict__ jlist) {
-    const int lane = threadIdx.x & 31;
-    const unsigned below = (1u << lane) - 1u;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long p0 = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); p0 < M; p0 += stride) {
-        const long long p = p0 + lane;
-        int bucket = -1;
-        long long base_j = 0, j = 0;
-        if (p < M) {
-            j = idx[p];
-            const long long row = j / nchan;
-            const int k = nslab > 1 ? (int)(row * nslab / nrow) : 0;
-            const long long j0 = slab_first_row_dev(nrow, nslab, k) * nchan;
-            const int b = (int)((j - j0) >> OUT_SHIFT);
-            bucket = k * bmax + b;
-            base_j = j0 + ((long long)b << OUT_SHIFT);
-        }
-        const unsigned peers = __match_any_sync(0xffffffffu, bucket);
-        const int leader = __ffs(peers) - 1;
-        int base = 0;
-        if (bucket >= 0 && lane == leader) base = atomicAdd(ocur + bucket, __popc(peers));
-        base = __shfl_sync(0xffffffffu, base, leader);
-        if (bucket >= 0) {
-            const long long s = base_j + base + __popc(peers & below);
-            dslot[p] = (int)s;
-            jlist[s] = (int)j;
-        }
-    }
-}
-
-template <typename T>
-__global__ void k_out_stage(long long p0, long long n, const int *__restrict__ dslot, const C<T> *__restrict__ os,
-                            const C<T> *__restrict__ ph, C<T> *__restrict__ stage) {
-    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
-         k += (long long)gridDim.x * blockDim.x) {
-        const long long p = p0 + k;
-        const C<T> v = os[p], e = ph[p];
-        stage[dslot[p]] = C<T>{v.x * e.x + v.y * e.y, v.y * e.x - v.x * e.y};
-    }
-}
-
-template <typename T>
-__global__ void k_out_place(long long s0, long long n, const int *__restrict__ jlist, const C<T> *__restrict__ stage,
-                            const T *__restrict__ wgt, C<T> *__restrict__ vis) {
-    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
-         k += (long long)gridDim.x * blockDim.x) {
-        const long long s = s0 + k;
-        const int j = jlist[s];
-        C<T> v = stage[s];
-        if (wgt) {
-            const T wt = wgt[j];
-            v.x *= wt;
-            v.y *= wt;
-        }
-        vis[j] = v;
+__global__ void k_vis_out(long long M, const int *__restrict__ idx, const C<T> *__restrict__ ph,
+                          const C<T> *__restrict__ os, const T *__restrict__ wgt, C<T> *__restrict__ vis) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < M;
+         i += (long long)gridDim.x * blockDim.x) {
+        int j = idx[i];
+        C<T> v = os[i], e = ph[i];
+        T wt = wgt ? wgt[j] : (T)1;
+        vis[j] = C<T>{(v.x * e.x + v.y * e.y) * wt, (v.y * e.x - v.x * e.y) * wt};
     }
 }
 
@@ -1294,6 +1206,37 @@ k_spread_f32(DevGeom g, const int *__restrict__ bin_start, const int *__restrict
     }
 }
 
+// vis[idx[i]] = value * wgt * e^{-i o_c w} (ra_exec.cu:56-89; the weight
+// multiplies, utils.cu:189): the scatter of dirty2ms back to input order.
+template <typename T>
+__device__ __forceinline__ void vis_store(const VisIO &io, int i, C<T> v) {
+    const int j = io.idx[i];
+    const C<T> e = static_cast<const C<T> *>(io.ph)[i];
+    const T wt = io.wgt ? static_cast<const T *>(io.wgt)[j] : (T)1;
+    static_cast<C<T> *>(io.vis)[j] = C<T>{(v.x * e.x + v.y * e.y) * wt, (v.y * e.x - v.x * e.y) * wt};
+}
+
+// The same scatter in two halves: the loads (index, phase, weight) issued
+// before the gather so that their latency overlaps the shared-memory work.
+template <typename T> struct VisDst {
+    int j;
+    C<T> e;
+    T wt;
+};
+template <typename T>
+__device__ __forceinline__ VisDst<T> vis_dst(const VisIO &io, int i) {
+    VisDst<T> d;
+    d.j = io.idx[i];
+    d.e = static_cast<const C<T> *>(io.ph)[i];
+    d.wt = io.wgt ? static_cast<const T *>(io.wgt)[d.j] : (T)1;
+    return d;
+}
+template <typename T>
+__device__ __forceinline__ void vis_put(const VisIO &io, const VisDst<T> &d, C<T> v) {
+    static_cast<C<T> *>(io.vis)[d.j] =
+        C<T>{(v.x * d.e.x + v.y * d.e.y) * d.wt, (v.y * d.e.x - v.x * d.e.y) * d.wt};
+}
+
 // Interpolator tile layout: [tz][ty][tpitch], column c holding grid x =
 // x_al + c with x_al = ox rounded down to even (so a TMA box may start there),
 // i.e. tile cell lx of the bin at column lx + (ox & 1).
@@ -1364,7 +1307,7 @@ template <typename T, int KW>
 __global__ void __launch_bounds__(interp_threads<T>(), sizeof(T) == 4 ? 3 : 2)
 k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__ bin_count,
            const int *__restrict__ sub_end, const R<T> *__restrict__ rec, const C<T> *__restrict__ grid,
-           const WinTab<T> tab, C<T> *__restrict__ os, const __grid_constant__ CUtensorMap tmap, int *err) {
+           const WinTab<T> tab, const VisIO io, const __grid_constant__ CUtensorMap tmap, int *err) {
     constexpr int IT = interp_threads<T>(), IW = IT / 32;
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ C<T> partial[IT];      // per (column, part, lane) sums of split visibilities
@@ -1441,6 +1384,8 @@ k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
             const int i = start + m * stride;
             const int dz0 = part * KZ / S, dz1 = (part + 1) * KZ / S;
             R<T> r = rec[i];
+            VisDst<T> dst;
+            if (S == 1) dst = vis_dst<T>(io, i);
             T kx[KW], ky[KW];
 #pragma unroll
             for (int d = 0; d < KW; ++d) {
@@ -1471,7 +1416,7 @@ k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
                 ar = fma(sr, kz, ar);
                 ai = fma(si, kz, ai);
             }
-            if (S == 1) os[i] = C<T>{ar, ai};
+            if (S == 1) vis_put<T>(io, dst, C<T>{ar, ai});
             else partial[u * 32 + lane] = C<T>{ar, ai};
         }
         if (S > 1) {                                   // L * S <= IW: one pass
@@ -1495,7 +1440,7 @@ k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
                     v.x += w.x;
                     v.y += w.y;
                 }
-                os[start + m * stride] = v;
+                vis_store<T>(io, start + m * stride, v);
             }
         }
         __syncthreads();
@@ -1742,10 +1687,9 @@ void launch_bin_count(const DevGeom &g, const double *u, const double *v, const 
     k_bin_count<<<grid_for(g.nrow * g.nchan), NTHREADS, 0, st>>>(g, u, v, w, foc, keys, count, err);
 }
 
-void launch_bin_scatter(long long M, const unsigned *keys, int cbits, int *bcur, int *tmp, int *slot,
-                        cudaStream_t st) {
+void launch_bin_scatter(long long M, const unsigned *keys, int cbits, int *bcur, int *tmp, cudaStream_t st) {
     count_launch();
-    k_bin_scatter<<<grid_for(M), NTHREADS, 0, st>>>(M, keys, cbits, bcur, tmp, slot);
+    k_bin_scatter<<<grid_for(M), NTHREADS, 0, st>>>(M, keys, cbits, bcur, tmp);
 }
 
 void launch_bins_from_keys(const int *kstart, const int *total, long long nb, int cbits, int sub, int *bin_start,
@@ -1771,39 +1715,28 @@ void scan_ints(const int *in, int *out, long long n, bool inclusive, int *tmp, c
 
 template <typename T>
 void launch_records(const DevGeom &g, const double *u, const double *v, const double *w, const double *foc,
-                    const int *tmp, long long M, int *kcur, void *rec, void *ph, int *idx, int *qpos,
-                    cudaStream_t st) {
+                    const int *tmp, long long M, int *kcur, void *rec, void *ph, int *idx, cudaStream_t st) {
     count_launch();
     k_records<T><<<grid_for(M), NTHREADS, 0, st>>>(g, u, v, w, foc, tmp, M, kcur, reinterpret_cast<R<T> *>(rec),
-                                                   reinterpret_cast<C<T> *>(ph), idx, qpos);
+                                                   reinterpret_cast<C<T> *>(ph), idx);
 }
 
 template <typename T>
-void launch_vis_prep(long long j0, long long n, const int *slot, const int *qpos, const void *ph, const void *vis,
-                     const void *wgt, void *stage, void *cs, cudaStream_t st) {
-    if (n <= 0) return;
-    count_launch(2);
-    k_vis_stage<T><<<grid_for(n), NTHREADS, 0, st>>>(j0, n, slot, reinterpret_cast<const C<T> *>(vis),
-                                                     reinterpret_cast<const T *>(wgt), reinterpret_cast<C<T> *>(stage));
-    k_vis_place<T><<<grid_for(n), NTHREADS, 0, st>>>(j0, n, qpos, reinterpret_cast<const C<T> *>(stage),
-                                                     reinterpret_cast<const C<T> *>(ph), reinterpret_cast<C<T> *>(cs));
-}
-
-void launch_out_maps(long long M, const int *idx, long long nrow, int nchan, int nslab, int bmax, int *ocur,
-                     int *dslot, int *jlist, cudaStream_t st) {
+void launch_vis_prep(long long M, const int *idx, const void *ph, const void *vis, const void *wgt, void *cs,
+                     cudaStream_t st) {
     count_launch();
-    k_out_maps<<<grid_for(M), NTHREADS, 0, st>>>(M, idx, nrow, nchan, nslab, bmax, ocur, dslot, jlist);
+    k_vis_prep<T><<<grid_for(M), NTHREADS, 0, st>>>(M, idx, reinterpret_cast<const C<T> *>(ph),
+                                                    reinterpret_cast<const C<T> *>(vis),
+                                                    reinterpret_cast<const T *>(wgt), reinterpret_cast<C<T> *>(cs));
 }
 
 template <typename T>
-void launch_vis_out(long long p0, long long n, const int *dslot, const int *jlist, const void *os, const void *ph,
-                    const void *wgt, void *stage, void *vis, cudaStream_t st) {
-    if (n <= 0) return;
-    count_launch(2);
-    k_out_stage<T><<<grid_for(n), NTHREADS, 0, st>>>(p0, n, dslot, reinterpret_cast<const C<T> *>(os),
-                                                     reinterpret_cast<const C<T> *>(ph), reinterpret_cast<C<T> *>(stage));
-    k_out_place<T><<<grid_for(n), NTHREADS, 0, st>>>(p0, n, jlist, reinterpret_cast<const C<T> *>(stage),
-                                                     reinterpret_cast<const T *>(wgt), reinterpret_cast<C<T> *>(vis));
+void launch_vis_out(long long M, const int *idx, const void *ph, const void *os, const void *wgt, void *vis,
+                    cudaStream_t st) {
+    count_launch();
+    k_vis_out<T><<<grid_for(M), NTHREADS, 0, st>>>(M, idx, reinterpret_cast<const C<T> *>(ph),
+                                                   reinterpret_cast<const C<T> *>(os),
+                                                   reinterpret_cast<const T *>(wgt), reinterpret_cast<C<T> *>(vis));
 }
 
 size_t tile_smem_bytes(const TileGeom &tg, int esize, int kw, int wdeg) {
@@ -1840,8 +1773,8 @@ static WinTab<T> make_tab(const DevGeom &g, const double *ht) {
 
 template <typename T, int KW>
 static int launch_spread_kw(const DevGeom &g, size_t smem, const int *bs, const int *bc, const int *se,
-                            const void *rec, void *cs, void *grid, const double *wc, const double *ht, int nsm,
-                            cudaStream_t st) {
+                            const void *rec, void *cs, void *grid, const double *wc, const double *ht,
+                            const VisIO &io, long long M, int nsm, cudaStream_t st) {
     int blocks = 0, s;
     if constexpr (KW > 0 && sizeof(T) == 4) {
         auto kern = k_spread_f32<KW>;
@@ -1870,21 +1803,23 @@ static int launch_spread_kw(const DevGeom &g, size_t smem, const int *bs, const 
 template <typename T, int KW>
 static int launch_interp_kw(const DevGeom &g, size_t smem, const int *bs, const int *bc, const int *se,
                             const void *rec, const void *grid, void *os, const double *wc, const double *ht,
-                            const CUtensorMap *tmap, int *err, int nsm, cudaStream_t st) {
+                            const VisIO &io, long long M, const CUtensorMap *tmap, int *err, int nsm,
+                            cudaStream_t st) {
     int blocks = 0, s;
     if constexpr (KW > 0) {
         auto kern = k_interp_t<T, KW>;
         if ((s = launch_persistent(kern, smem, nsm, blocks, interp_threads<T>()))) return s;
         count_launch();
         kern<<<blocks, interp_threads<T>(), smem, st>>>(g, bs, bc, se, reinterpret_cast<const R<T> *>(rec),
-                                             reinterpret_cast<const C<T> *>(grid), make_tab<T>(g, ht),
-                                             reinterpret_cast<C<T> *>(os), *tmap, err);
+                                             reinterpret_cast<const C<T> *>(grid), make_tab<T>(g, ht), io,
+                                             *tmap, err);
     } else {
         auto kern = k_interp<T, 0>;
         if ((s = launch_persistent(kern, smem, nsm, blocks))) return s;
         count_launch();
         kern<<<blocks, NTHREADS, smem, st>>>(g, bs, bc, se, reinterpret_cast<const R<T> *>(rec),
                                              reinterpret_cast<const C<T> *>(grid), reinterpret_cast<C<T> *>(os), wc);
+        launch_vis_out<T>(M, io.idx, io.ph, os, io.wgt, io.vis, st);
     }
     return OK;
 }
@@ -1907,15 +1842,16 @@ static int launch_interp_kw(const DevGeom &g, size_t smem, const int *bs, const 
 
 template <typename T>
 int launch_spread(const DevGeom &g, size_t smem, const int *bs, const int *bc, const int *se,
-                  const void *rec, void *cs, void *grid, const double *wc, const double *ht, int nsm, cudaStream_t st) {
-    CURIG_KW_SWITCH(launch_spread_kw, g, smem, bs, bc, se, rec, cs, grid, wc, ht, nsm, st)
+                  const void *rec, void *cs, void *grid, const double *wc, const double *ht, VisIO io,
+                  long long M, int nsm, cudaStream_t st) {
+    CURIG_KW_SWITCH(launch_spread_kw, g, smem, bs, bc, se, rec, cs, grid, wc, ht, io, M, nsm, st)
 }
 
 template <typename T>
 int launch_interp(const DevGeom &g, size_t smem, const int *bs, const int *bc, const int *se,
-                  const void *rec, const void *grid, void *os, const double *wc, const double *ht,
-                  const CUtensorMap *tmap, int *err, int nsm, cudaStream_t st) {
-    CURIG_KW_SWITCH(launch_interp_kw, g, smem, bs, bc, se, rec, grid, os, wc, ht, tmap, err, nsm, st)
+                  const void *rec, const void *grid, void *os, const double *wc, const double *ht, VisIO io,
+                  long long M, const CUtensorMap *tmap, int *err, int nsm, cudaStream_t st) {
+    CURIG_KW_SWITCH(launch_interp_kw, g, smem, bs, bc, se, rec, grid, os, wc, ht, io, M, tmap, err, nsm, st)
 }
 
 template <typename T>
@@ -1982,17 +1918,17 @@ void launch_zero_tpad(int nx, int ny, int nf2, int nf3, void *t, cudaStream_t st
 #define CURIG_INSTANTIATE(T)                                                                          \
     template void launch_records<T>(const DevGeom &, const double *, const double *, const double *,  \
                                     const double *, const int *, long long, int *, void *, void *,    \
-                                    int *, int *, cudaStream_t);                                      \
-    template void launch_vis_prep<T>(long long, long long, const int *, const int *, const void *,     \
-                                     const void *, const void *, void *, void *, cudaStream_t);       \
-    template void launch_vis_out<T>(long long, long long, const int *, const int *, const void *,      \
-                                    const void *, const void *, void *, void *, cudaStream_t);        \
+                                    int *, cudaStream_t);                                             \
+    template void launch_vis_prep<T>(long long, const int *, const void *, const void *, const void *,\
+                                     void *, cudaStream_t);                                           \
+    template void launch_vis_out<T>(long long, const int *, const void *, const void *, const void *, \
+                                    void *, cudaStream_t);                                            \
     template int launch_spread<T>(const DevGeom &, size_t, const int *, const int *, const int *,     \
-                                  const void *, void *, void *, const double *, const double *, int,  \
-                                  cudaStream_t);                                                      \
+                                  const void *, void *, void *, const double *, const double *,       \
+                                  VisIO, long long, int, cudaStream_t);                               \
     template int launch_interp<T>(const DevGeom &, size_t, const int *, const int *, const int *,     \
                                   const void *, const void *, void *, const double *, const double *, \
-                                  const CUtensorMap *, int *, int, cudaStream_t);                     \
+                                  VisIO, long long, const CUtensorMap *, int *, int, cudaStream_t);   \
     template void launch_correct_m2d<T>(const DevCorr &, const void *, void *, cudaStream_t);         \
     template void launch_correct_d2m<T>(const DevCorr &, const void *, void *, cudaStream_t);         \
     template void launch_cols_to_t<T>(int, int, int, int, const void *, void *, cudaStream_t);         \

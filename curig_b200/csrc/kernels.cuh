@@ -64,4 +64,13 @@ template <typename T> struct WinTab {
     T c[TAB_KW][TAB_DEG];
 };
 
+// The caller's visibilities (input order [nrow][nchan]) and the plan's gather
+// tables, for the tile kernels that read or write them directly.
+struct VisIO {
+    const int *idx;        // sorted position -> input index
+    const void *ph;        // e^{i o_c w} per sorted position (complex T)
+    const void *wgt;       // weights in input order (T), may be null
+    void *vis;             // visibilities in input order (complex T)
+};
+
 }  // namespace curig

@@ -284,8 +284,7 @@ void plan_release_points(Plan *p) {
     dfree(p->d_wcoef, st); dfree(p->d_bin_count, st); dfree(p->d_bin_start, st);
     dfree(p->d_nsub, st); dfree(p->d_sub_end, st); dfree(p->d_keys_in, st); dfree(p->d_kcount, st);
     dfree(p->d_idx, st); dfree(p->d_err, st); dfree(p->d_keys, st); dfree(p->d_scan, st);
-    dfree(p->d_tmp, st); dfree(p->d_bcur, st); dfree(p->d_slot, st); dfree(p->d_qpos, st); dfree(p->d_stage, st);
-    dfree(p->d_dslot, st); dfree(p->d_jlist, st);
+    dfree(p->d_tmp, st); dfree(p->d_bcur, st);
     dfree(p->d_rec, st); dfree(p->d_ph, st); dfree(p->d_cs, st); dfree(p->d_grid, st);
     dfree(p->d_tgrid, st);
     fft_release(p);
@@ -601,7 +600,6 @@ retry_tiles:
     CU_TRY(dalloc(&p->d_keys_in, M * sizeof(unsigned), st));
     CU_TRY(dalloc(&p->d_kcount, nkeys * sizeof(int), st));
     CU_TRY(dalloc(&p->d_tmp, M * sizeof(int), st));
-    CU_TRY(dalloc(&p->d_slot, M * sizeof(int), st));
     CU_TRY(dalloc(&p->d_bcur, nb * sizeof(int), st));
     CU_TRY(dalloc(&p->d_bin_start, nb * sizeof(int), st));
     CU_TRY(dalloc(&p->d_bin_count, nb * sizeof(int), st));
@@ -613,7 +611,7 @@ retry_tiles:
     scan_ints(p->d_kcount, p->d_kcount, nkeys, false, p->d_scan, st);          // in place: first position per key
     launch_bins_from_keys(p->d_kcount, p->d_scan, nb, cbits, g.sub, p->d_bin_start, p->d_bin_count, p->d_nsub,
                           p->d_bcur, st);
-    launch_bin_scatter(M, p->d_keys_in, cbits, p->d_bcur, p->d_tmp, p->d_slot, st);
+    launch_bin_scatter(M, p->d_keys_in, cbits, p->d_bcur, p->d_tmp, st);
     scan_ints(p->d_nsub, p->d_sub_end, nb, true, p->d_scan, st);
     p->slab_sub_end.assign(nslab, 0);               // last sub-problem end of every slab
     for (int k = 0; k < nslab; ++k)
@@ -629,7 +627,6 @@ retry_tiles:
             herr = 0;
             CU_TRY(cudaMemsetAsync(p->d_err, 0, sizeof(int), st));
             dfree(p->d_keys_in, st); dfree(p->d_kcount, st); dfree(p->d_tmp, st); dfree(p->d_bcur, st);
-            dfree(p->d_slot, st);
             dfree(p->d_bin_start, st); dfree(p->d_bin_count, st);
             dfree(p->d_nsub, st); dfree(p->d_sub_end, st); dfree(p->d_scan, st);
             goto retry_tiles;
@@ -639,32 +636,13 @@ retry_tiles:
     CU_TRY(dalloc(&p->d_rec, M * 4 * (size_t)esize, st));
     CU_TRY(dalloc(&p->d_ph, M * 2 * (size_t)esize, st));
     CU_TRY(dalloc(&p->d_cs, M * 2 * (size_t)esize, st));
-    CU_TRY(dalloc(&p->d_stage, M * 2 * (size_t)esize, st));
     CU_TRY(dalloc(&p->d_idx, M * sizeof(int), st));
-    CU_TRY(dalloc(&p->d_qpos, M * sizeof(int), st));
     // each bin's visibilities (tmp) placed by residue; the key cursors start at
     // the scanned key counts
     if (p->opt.precision)
-        launch_records<float>(g, du, dv, dw, p->d_foc, p->d_tmp, M, p->d_kcount, p->d_rec, p->d_ph, p->d_idx,
-                              p->d_qpos, st);
+        launch_records<float>(g, du, dv, dw, p->d_foc, p->d_tmp, M, p->d_kcount, p->d_rec, p->d_ph, p->d_idx, st);
     else
-        launch_records<double>(g, du, dv, dw, p->d_foc, p->d_tmp, M, p->d_kcount, p->d_rec, p->d_ph, p->d_idx,
-                               p->d_qpos, st);
-    // dirty2ms output staging: windows of 2^18 input indices inside each row slab
-    {
-        long long maxslab = 0;
-        for (int k = 0; k < nslab; ++k) maxslab = std::max(maxslab, (p->slab_row[k + 1] - p->slab_row[k]) * nchan);
-        const long long bmax = (maxslab + (1LL << 18) - 1) >> 18;
-        const long long ncur = (long long)nslab * bmax;
-        CU_TRY(dalloc(&p->d_dslot, M * sizeof(int), st));
-        CU_TRY(dalloc(&p->d_jlist, M * sizeof(int), st));
-        if (ncur > nb) {                                // cursors: the bin cursors' buffer when it is large enough
-            dfree(p->d_bcur, st);
-            CU_TRY(dalloc(&p->d_bcur, ncur * sizeof(int), st));
-        }
-        CU_TRY(cudaMemsetAsync(p->d_bcur, 0, ncur * sizeof(int), st));
-        launch_out_maps(M, p->d_idx, nrow, nchan, nslab, (int)bmax, p->d_bcur, p->d_dslot, p->d_jlist, st);
-    }
+        launch_records<double>(g, du, dv, dw, p->d_foc, p->d_tmp, M, p->d_kcount, p->d_rec, p->d_ph, p->d_idx, st);
     dfree(p->d_keys_in, st);
     dfree(p->d_kcount, st);
     dfree(p->d_scan, st);
@@ -784,12 +762,14 @@ static int execute_t(Plan *p, int type, void *d_vis, const void *d_wgt, void *d_
     int s;
     if (type == 1) {
         mark(p, EV_M2D_BEGIN);
-        launch_vis_prep<T>(0, M, p->d_slot, p->d_qpos, p->d_ph, d_vis, d_wgt, p->d_stage, p->d_cs, st);
+        launch_vis_prep<T>(M, p->d_idx, p->d_ph, d_vis, d_wgt, p->d_cs, st);
         mark(p, EV_M2D_PREP);
         CU_TRY(cudaMemsetAsync(p->d_grid, 0, gbytes, st));
         mark(p, EV_M2D_ZERO);
+        const VisIO io{p->d_idx, p->d_ph, d_wgt, d_vis};
         s = launch_spread<T>(g, p->smem, p->d_bin_start, p->d_bin_count, p->d_sub_end, p->d_rec, p->d_cs,
-                             p->d_grid, p->d_wcoef, p->htab.empty() ? nullptr : p->htab.data(), p->nsm, st);
+                             p->d_grid, p->d_wcoef, p->htab.empty() ? nullptr : p->htab.data(), io, M, p->nsm,
+                             st);
         if (s) return s;
         mark(p, EV_M2D_SPREAD);
         s = plane_fft<T>(p, CUFFT_INVERSE, true);    // +1, cuft.cu:127-143
@@ -805,13 +785,13 @@ static int execute_t(Plan *p, int type, void *d_vis, const void *d_wgt, void *d_
         s = plane_fft<T>(p, CUFFT_FORWARD, false);   // -1
         if (s) return s;
         mark(p, EV_D2M_FFT);
+        const VisIO io{p->d_idx, p->d_ph, d_wgt, d_vis};
         s = launch_interp<T>(g, p->smem_interp, p->d_bin_start, p->d_bin_count, p->d_sub_end, p->d_rec, p->d_grid,
-                             p->d_cs, p->d_wcoef, p->htab.empty() ? nullptr : p->htab.data(), &p->tmap, p->d_err,
-                             p->nsm, st);
+                             p->d_cs, p->d_wcoef, p->htab.empty() ? nullptr : p->htab.data(), io, M, &p->tmap,
+                             p->d_err, p->nsm, st);
         if (s) return s;
         mark(p, EV_D2M_INTERP);
-        launch_vis_out<T>(0, M, p->d_dslot, p->d_jlist, p->d_cs, p->d_ph, d_wgt, p->d_stage, d_vis, st);
-        mark(p, EV_D2M_END);
+        mark(p, EV_D2M_END);                     // the scatter runs inside the interpolator
     }
     CU_TRY(cudaGetLastError());
     return OK;
@@ -849,6 +829,7 @@ static int execute_slabs_t(Plan *p, int type, void *d_vis, const void *d_wgt, vo
         gk.sub_hi = p->slab_sub_end[k];
         return gk.sub_hi > gk.sub_lo;
     };
+    const VisIO io{p->d_idx, p->d_ph, d_wgt, d_vis};
     const double *ht = p->htab.empty() ? nullptr : p->htab.data();
     int s;
     if (type == 1) {
@@ -857,11 +838,13 @@ static int execute_slabs_t(Plan *p, int type, void *d_vis, const void *d_wgt, vo
         for (int k = 0; k < ns; ++k) {
             CU_TRY(wait_slab(k));
             const long long i0 = p->slab_row[k] * p->nchan, i1 = p->slab_row[k + 1] * p->nchan;
-            launch_vis_prep<T>(i0, i1 - i0, p->d_slot, p->d_qpos, p->d_ph, d_vis, d_wgt, p->d_stage, p->d_cs, st);
+            if (i1 > i0)
+                launch_vis_prep<T>(i1 - i0, p->d_idx + i0, static_cast<const char *>(p->d_ph) + i0 * 2 * sizeof(T),
+                                   d_vis, d_wgt, static_cast<char *>(p->d_cs) + i0 * 2 * sizeof(T), st);
             DevGeom gk;
             if (slab_geom(k, gk) &&
                 (s = launch_spread<T>(gk, p->smem, p->d_bin_start, p->d_bin_count, p->d_sub_end, p->d_rec, p->d_cs,
-                                      p->d_grid, p->d_wcoef, ht, p->nsm, st)))
+                                      p->d_grid, p->d_wcoef, ht, io, p->nrow * p->nchan, p->nsm, st)))
                 return s;
         }
         if ((s = plane_fft<T>(p, CUFFT_INVERSE, true))) return s;
@@ -877,10 +860,9 @@ static int execute_slabs_t(Plan *p, int type, void *d_vis, const void *d_wgt, vo
             DevGeom gk;
             if (slab_geom(k, gk) &&
                 (s = launch_interp<T>(gk, p->smem_interp, p->d_bin_start, p->d_bin_count, p->d_sub_end, p->d_rec,
-                                      p->d_grid, p->d_cs, p->d_wcoef, ht, &p->tmap, p->d_err, p->nsm, st)))
+                                      p->d_grid, p->d_cs, p->d_wcoef, ht, io, p->nrow * p->nchan, &p->tmap,
+                                      p->d_err, p->nsm, st)))
                 return s;
-            const long long i0 = p->slab_row[k] * p->nchan, i1 = p->slab_row[k + 1] * p->nchan;
-            launch_vis_out<T>(i0, i1 - i0, p->d_dslot, p->d_jlist, p->d_cs, p->d_ph, d_wgt, p->d_stage, d_vis, st);
             CU_TRY(done_slab(k));
         }
     }

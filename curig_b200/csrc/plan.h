@@ -66,11 +66,6 @@ struct Plan {
     int *d_kcount = nullptr;                            // count / first position per key value
     int *d_bcur = nullptr, *d_tmp = nullptr;            // bin cursors; input index per position, bin order
     int *d_idx = nullptr;                               // input index per sorted position (bin order)
-    int *d_slot = nullptr;                              // bin-order place of each input visibility
-    int *d_qpos = nullptr;                              // final sorted position of each bin-order place
-    void *d_stage = nullptr;                            // visibilities in bin / staging order (both directions)
-    int *d_dslot = nullptr;                             // dirty2ms: staging place of each sorted position
-    int *d_jlist = nullptr;                             // dirty2ms: input index of each staging place
     int *d_err = nullptr;
     unsigned long long *d_keys = nullptr;
     int *d_scan = nullptr;                              // scan temporaries (total, block sums)
@@ -151,8 +146,7 @@ void launch_wrange(const double *w, int stride, long long nrow, unsigned long lo
 // binning: a counting sort over (bin, residue) keys (kernels.cu)
 void launch_bin_count(const DevGeom &g, const double *u, const double *v, const double *w, const double *foc,
                       unsigned *keys, int *count, int *err, cudaStream_t st);
-void launch_bin_scatter(long long M, const unsigned *keys, int cbits, int *bcur, int *tmp, int *slot,
-                        cudaStream_t st);
+void launch_bin_scatter(long long M, const unsigned *keys, int cbits, int *bcur, int *tmp, cudaStream_t st);
 void launch_bins_from_keys(const int *kstart, const int *total, long long nb, int cbits, int sub, int *bin_start,
                            int *bin_count, int *nsub, int *bcur, cudaStream_t st);
 // Prefix sum of n int32 values (exclusive or inclusive); tmp holds
@@ -162,31 +156,26 @@ void scan_ints(const int *in, int *out, long long n, bool inclusive, int *tmp, c
 size_t tile_smem_bytes(const TileGeom &tg, int esize, int kw, int wdeg);
 template <typename T>
 void launch_records(const DevGeom &g, const double *u, const double *v, const double *w, const double *foc,
-                    const int *tmp, long long M, int *kcur, void *rec, void *ph, int *idx, int *qpos,
+                    const int *tmp, long long M, int *kcur, void *rec, void *ph, int *idx, cudaStream_t st);
+template <typename T>
+void launch_vis_prep(long long M, const int *idx, const void *ph, const void *vis, const void *wgt, void *cs,
+                     cudaStream_t st);
+template <typename T>
+void launch_vis_out(long long M, const int *idx, const void *ph, const void *os, const void *wgt, void *vis,
                     cudaStream_t st);
-// cs[p] = vis[j] * wgt[j] * ph[p] for the input visibilities j in [j0, j0 + n)
-// (a row slab), whose sorted positions p fill the same range: two passes
-// through stage (bin order) with slot / qpos from the binning.
-template <typename T>
-void launch_vis_prep(long long j0, long long n, const int *slot, const int *qpos, const void *ph, const void *vis,
-                     const void *wgt, void *stage, void *cs, cudaStream_t st);
-// dirty2ms output: staging places of the sorted positions (set points), then
-// vis[j] = os[p] * conj(ph[p]) * wgt[j] for the sorted positions [p0, p0 + n)
-// of a row slab (whose staging places fill the same range).
-void launch_out_maps(long long M, const int *idx, long long nrow, int nchan, int nslab, int bmax, int *ocur,
-                     int *dslot, int *jlist, cudaStream_t st);
-template <typename T>
-void launch_vis_out(long long p0, long long n, const int *dslot, const int *jlist, const void *os, const void *ph,
-                    const void *wgt, void *stage, void *vis, cudaStream_t st);
-// Tile kernels: launch_spread spreads cs (vis * wgt * phase in sorted order);
-// launch_interp writes the interpolated values to os in sorted order.
+// Tile kernels.  launch_spread spreads cs (vis * wgt * phase in bin order,
+// written by k_vis_prep); launch_interp interpolates and scatters
+// wgt * conj(phase) * value to io.vis — inside the tile kernel for widths up to
+// 12 (the random writes overlap the shared-memory work), through os and
+// k_vis_out for the generic wider kernel.
 template <typename T>
 int launch_spread(const DevGeom &g, size_t smem, const int *bs, const int *bc, const int *se,
-                  const void *rec, void *cs, void *grid, const double *wc, const double *ht, int nsm, cudaStream_t st);
+                  const void *rec, void *cs, void *grid, const double *wc, const double *ht, VisIO io,
+                  long long M, int nsm, cudaStream_t st);
 template <typename T>
 int launch_interp(const DevGeom &g, size_t smem, const int *bs, const int *bc, const int *se,
-                  const void *rec, const void *grid, void *os, const double *wc, const double *ht,
-                  const CUtensorMap *tmap, int *err, int nsm, cudaStream_t st);
+                  const void *rec, const void *grid, void *os, const double *wc, const double *ht, VisIO io,
+                  long long M, const CUtensorMap *tmap, int *err, int nsm, cudaStream_t st);
 template <typename T>
 void launch_correct_m2d(const DevCorr &cc, const void *grid, void *dirty, cudaStream_t st);
 template <typename T>
