@@ -118,6 +118,10 @@ lib.curig_nufft_execute.restype = c_int
 lib.curig_nufft_destroy.argtypes = [c_void_p]
 lib.curig_nufft_destroy.restype = c_int
 lib.curig_default_opts.restype = None
+lib.curig_nufft_setpts3.argtypes = [c_void_p, c_int64, _P, c_int64, _P]
+lib.curig_nufft_setpts3.restype = c_int
+lib.curig_nufft_info3.argtypes = [c_void_p, ctypes.POINTER(c_int), ctypes.POINTER(c_double)]
+lib.curig_nufft_info3.restype = c_int
 lib.curig_test_tile_wait.argtypes = [c_int64, c_int]
 lib.curig_test_tile_wait.restype = None
 

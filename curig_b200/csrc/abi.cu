@@ -266,6 +266,8 @@ extern "C" int curig_makeplan(int type, int nx, int ny, double psx, double psy, 
 // 1 and 2 with the same kernel-width, grid-size and correction rules.
 struct curig_nufft_s {
     Plan *p = nullptr;
+    Nufft3 *t3 = nullptr;                 // type 3
+    curig_opts opts{};
     int type = 1, dim = 1, n1 = 0, n2 = 1, iflag = 1;
     double *d_uvw = nullptr;
 };
@@ -274,9 +276,24 @@ extern "C" int curig_nufft_makeplan(int type, int dim, int n1, int n2, double ep
                                     const curig_opts *opts, curig_nufft *out) {
     if (!out) return fail(ERR_ARG, "null plan pointer");
     *out = nullptr;
-    if ((type != 1 && type != 2) || (dim != 1 && dim != 2) || n1 <= 0 || (dim == 2 && n2 <= 0) ||
-        (iflag != 1 && iflag != -1))
+    if ((type != 1 && type != 2 && type != 3) || (dim != 1 && dim != 2) || (type == 3 && dim != 1) || n1 <= 0 ||
+        (dim == 2 && n2 <= 0) || (iflag != 1 && iflag != -1))
         return fail(ERR_ARG, "invalid NUFFT plan arguments");
+    if (type == 3) {                                   // sizes come with the points (curig_nufft_setpts3)
+        KernelParams kp;
+        int st = setup_kernel(eps, sigma, kp);
+        if (st != OK) return fail(st, "invalid NUFFT tolerance or upsampling factor");
+        if (opts && opts->precision != 0 && opts->precision != 1) return fail(ERR_ARG, "invalid precision");
+        *out = new curig_nufft_s;
+        (*out)->type = 3;
+        (*out)->dim = 1;
+        (*out)->n1 = n1;
+        (*out)->iflag = iflag;
+        if (opts) (*out)->opts = *opts;
+        else curig_default_opts(&(*out)->opts);
+        (*out)->t3 = nufft3_create(iflag, eps, sigma, (*out)->opts.precision, (cudaStream_t)(*out)->opts.stream);
+        return OK;
+    }
     Options o = to_options(opts);
     o.w_term = 1;
     Plan *p = nullptr;
@@ -293,8 +310,22 @@ extern "C" int curig_nufft_makeplan(int type, int dim, int n1, int n2, double ep
     return OK;
 }
 
+extern "C" int curig_nufft_setpts3(curig_nufft h, int64_t m, const double *d_x, int64_t n, const double *d_s) {
+    if (!h || h->type != 3) return fail(ERR_ARG, "not a type-3 plan");
+    int s = nufft3_setpts(h->t3, m, d_x, n, d_s, &h->opts);
+    if (s != OK) return fail(s, "type-3 NUFFT setpts failed");
+    return OK;
+}
+
+extern "C" int curig_nufft_info3(curig_nufft h, int *nf, double *dinfo) {
+    if (!h || h->type != 3) return fail(ERR_ARG, "not a type-3 plan");
+    nufft3_info(h->t3, nf, dinfo);
+    return OK;
+}
+
 extern "C" int curig_nufft_setpts(curig_nufft h, int64_t m, const double *d_x, const double *d_y) {
     if (!h || !d_x || m <= 0 || (h->dim == 2 && !d_y)) return fail(ERR_ARG, "invalid NUFFT points");
+    if (h->type == 3) return fail(ERR_ARG, "type-3 plans take their points with curig_nufft_setpts3");
     Plan *p = h->p;
     if (h->d_uvw) cudaFreeAsync(h->d_uvw, p->st);
     h->d_uvw = nullptr;
@@ -310,6 +341,11 @@ extern "C" int curig_nufft_setpts(curig_nufft h, int64_t m, const double *d_x, c
 
 extern "C" int curig_nufft_execute(curig_nufft h, void *d_c, void *d_fk) {
     if (!h || !d_c || !d_fk) return fail(ERR_ARG, "invalid NUFFT execute arguments");
+    if (h->type == 3) {
+        int s = nufft3_execute(h->t3, d_c, d_fk);
+        if (s != OK) return fail(s, "type-3 NUFFT execute failed");
+        return OK;
+    }
     int s = plan_execute(h->p, d_c, nullptr, d_fk, h->type);
     if (s != OK) return fail(s, h->p->last_error.empty() ? "NUFFT execute failed" : h->p->last_error);
     return OK;
@@ -317,6 +353,11 @@ extern "C" int curig_nufft_execute(curig_nufft h, void *d_c, void *d_fk) {
 
 extern "C" int curig_nufft_destroy(curig_nufft h) {
     if (!h) return OK;
+    if (h->type == 3) {
+        nufft3_destroy(h->t3);
+        delete h;
+        return OK;
+    }
     if (h->d_uvw) cudaFreeAsync(h->d_uvw, h->p->st);
     plan_destroy(h->p);
     delete h;

@@ -22,7 +22,7 @@ NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-I" + HERE, "-I" + os.path.join(ROOT, "include")]
-SOURCES = ["params.cpp", "kernels.cu", "plan.cu", "abi.cu", "learned.cu"]
+SOURCES = ["params.cpp", "kernels.cu", "plan.cu", "abi.cu", "learned.cu", "nufft3.cu"]
 HEADERS = ["curig_internal.h", "kernels.cuh", "plan.h"]
 
 

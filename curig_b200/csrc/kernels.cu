@@ -953,7 +953,9 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
 // ------------------------------------------------------------------ FP32 spreader
 // The FP32 tile kernels order each bin by the residue mod 16 of its start
 // cells (NCLS classes; the sort key's residue) and give every class two lanes
-// of a warp: lane 2k + f takes elements f, f + 2, f + 4, ... of class k.  A
+// of a warp, one in each half-warp: lane k + 16 f takes elements f, f + 2,
+// f + 4, ... of class k (8-byte shared loads are served half a warp at a
+// time, so the two lanes of a class must not share a half).  A
 // tile cell's two words (re, im, or the high and low word of one component)
 // are adjacent, so cell c covers banks 2c and 2c + 1 (mod 32): cells of
 // different classes never share a bank, and the two lanes of one class write
@@ -1019,7 +1021,7 @@ k_spread_f32(DevGeom g, const int *__restrict__ bin_start, const int *__restrict
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int total = g.sub_hi ? g.sub_hi : sub_end[g.nbins - 1];
     const int tx = g.tpitch, txy = g.tpitch * g.ty;
-    const int klass = lane >> 1, f = lane & 1;
+    const int klass = lane & 15, f = lane >> 4;
     for (int s = g.sub_lo + blockIdx.x; s < total; s += gridDim.x) {
         long long b;
         int start, stride, n;
@@ -1062,13 +1064,48 @@ k_spread_f32(DevGeom g, const int *__restrict__ bin_start, const int *__restrict
                 int e = m > 0.f ? ilogb(m) + 1 : 0;       // 2^(e-1) <= m < 2^e
                 k = FIX_BITS - e;
             } else {
-                float bmax = 0.f;                         // largest kw x kw box sum of the start columns
-                for (int e = threadIdx.x; e < txy; e += TTHREADS) {
-                    const int x = e % tx, y = e / tx;
-                    float a = 0.f;
-                    for (int yy = max(0, y - KW + 1); yy <= y; ++yy)
-                        for (int xx = max(0, x - KW + 1); xx <= x; ++xx) a += colsum[yy * tx + xx];
-                    bmax = fmaxf(bmax, a);
+                // largest kw x kw box sum of the start-column sums: windows of
+                // kw rows summed in place down each column (thread per
+                // column), then windows of kw columns along each row (thread
+                // per row); the last kw values ride in registers
+                const int ty = g.ty;
+                if (threadIdx.x < tx) {
+                    const int x = threadIdx.x;
+                    float ring[KW], a = 0.f;
+#pragma unroll
+                    for (int d = 0; d < KW; ++d) ring[d] = 0.f;
+                    for (int y0 = 0; y0 < ty; y0 += KW) {
+#pragma unroll
+                        for (int d = 0; d < KW; ++d) {
+                            const int y = y0 + d;
+                            if (y < ty) {
+                                const float v = colsum[y * tx + x];
+                                a += v - ring[d];
+                                ring[d] = v;
+                                colsum[y * tx + x] = a;
+                            }
+                        }
+                    }
+                }
+                __syncthreads();
+                float bmax = 0.f;
+                if (threadIdx.x < ty) {
+                    const float *row = colsum + threadIdx.x * tx;
+                    float ring[KW], a = 0.f;
+#pragma unroll
+                    for (int d = 0; d < KW; ++d) ring[d] = 0.f;
+                    for (int x0 = 0; x0 < tx; x0 += KW) {
+#pragma unroll
+                        for (int d = 0; d < KW; ++d) {
+                            const int x = x0 + d;
+                            if (x < tx) {
+                                const float v = row[x];
+                                a += v - ring[d];
+                                ring[d] = v;
+                                bmax = fmaxf(bmax, a);
+                            }
+                        }
+                    }
                 }
                 for (int o = 16; o > 0; o >>= 1) bmax = fmaxf(bmax, __shfl_xor_sync(0xffffffffu, bmax, o));
                 __syncthreads();                          // every thread has read redbuf
@@ -1086,7 +1123,7 @@ k_spread_f32(DevGeom g, const int *__restrict__ bin_start, const int *__restrict
             qinv = ldexp(1.0, -k);
         }
         __syncthreads();
-        // class schedule: lane 2k + f, element 2t + f of class k at step t;
+        // class schedule: lane k + 16 f, element 2t + f of class k at step t;
         // chunks of few steps split each visibility's w-planes into S parts
         const int T = class_steps(cls, n);
         int c0, nk;
@@ -1365,7 +1402,7 @@ k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
         int L, c0 = 0, nk = 0;
         if constexpr (sizeof(T) == 4) {
             L = class_steps(cls, n);
-            class_range(cls, lane >> 1, n, c0, nk);
+            class_range(cls, lane & 15, n, c0, nk);
         } else {
             L = (n + 31) >> 5;
         }
@@ -1374,7 +1411,7 @@ k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
             const int k = u / S, part = u - k * S;
             int m;
             if constexpr (sizeof(T) == 4) {
-                const int e = 2 * k + (lane & 1);
+                const int e = 2 * k + (lane >> 4);
                 if (e >= nk) continue;
                 m = c0 + e;
             } else {
@@ -1428,7 +1465,7 @@ k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
                     while (q < NCLS - 1 && cls[q + 1] <= m) ++q;
                     const int e = m - cls[q];
                     if (e < 0 || (e >> 1) >= L) continue;   // (unreachable for sorted chunks)
-                    ln = 2 * q + (e & 1);
+                    ln = q + 16 * (e & 1);
                     k = e >> 1;
                 } else {
                     ln = m / L;

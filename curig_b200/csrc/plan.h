@@ -10,6 +10,8 @@
 #include <tuple>
 #include <vector>
 
+struct curig_opts;                 // include/curig.h
+
 namespace curig {
 
 struct Options {
@@ -198,6 +200,16 @@ void set_tile_wait(long long polls, int noissue);
 // destroy the cached cuFFT handles no plan holds (returns how many); number cached
 int fft_cache_trim();
 int fft_cache_size();
+
+// Generic NUFFT type 3 in one dimension (nufft3.cu): points x[m] with
+// strengths c -> frequencies s[n]; the grid's series by the type-2 NUFFT.
+struct Nufft3;
+Nufft3 *nufft3_create(int iflag, double eps, double sigma, int precision, cudaStream_t st);
+int nufft3_setpts(Nufft3 *p, long long m, const double *d_x, long long n, const double *d_s,
+                  const ::curig_opts *opts);
+int nufft3_execute(Nufft3 *p, const void *d_c, void *d_f);
+void nufft3_info(const Nufft3 *p, int *nf, double *dinfo);
+void nufft3_destroy(Nufft3 *p);
 
 // global learned-window registry (set through the C ABI)
 int registry_set_window(int kw, int degree, const double *coef, double eps_reached);

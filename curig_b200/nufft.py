@@ -1,8 +1,11 @@
-"""Generic NUFFT of types 1 and 2 in one or two dimensions (device arrays),
-built on the w-free gridder of this library (curig_nufft_* in include/curig.h).
+"""Generic NUFFT of types 1 and 2 in one or two dimensions and of type 3 in
+one dimension (device arrays); types 1 and 2 run on the w-free gridder of this
+library, type 3 spreads onto its own grid and evaluates it with a type 2
+(curig_nufft_* in include/curig.h).
 
 Type 1: fk[k] = sum_j c_j exp(i iflag k.x_j), modes k = index - n/2;
 type 2: c_j = sum_k fk[k] exp(i iflag k.x_j).  Points in radians (periodic).
+Type 3: f_k = sum_j c_j exp(i iflag s_k x_j), any real points and frequencies.
 """
 from __future__ import annotations
 
@@ -43,6 +46,48 @@ class Nufft:
     def execute(self, c, fk):
         """Type 1 reads c [m], writes fk (n_modes); type 2 reads fk, writes c."""
         _lib.check(_lib.lib.curig_nufft_execute(self._h, _lib.ptr(c), _lib.ptr(fk)), "nufft_execute")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lib.curig_nufft_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # pragma: no cover
+            pass
+
+
+class Nufft3:
+    """Type-3 NUFFT in one dimension: f_k = sum_j c_j exp(i iflag s_k x_j) for
+    points x[m] with strengths c and frequencies s[n] (curig_nufft_setpts3)."""
+
+    def __init__(self, epsilon, iflag=1, sigma=2.0, precision="fp64", stream=None):
+        self.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        self._opts = _lib.make_opts(self.precision, stream=_stream_handle(stream))
+        h = ctypes.c_void_p()
+        _lib.check(_lib.lib.curig_nufft_makeplan(3, 1, 1, 1, float(epsilon), int(iflag), float(sigma),
+                                                 ctypes.byref(self._opts), ctypes.byref(h)), "nufft_makeplan")
+        self._h = h
+        self._keep = None
+
+    def setpts(self, x, s):
+        """x [m] points and s [n] frequencies: contiguous float64 CUDA tensors."""
+        self._keep = (x, s)
+        self.m, self.n = int(x.shape[0]), int(s.shape[0])
+        _lib.check(_lib.lib.curig_nufft_setpts3(self._h, self.m, _lib.ptr(x), self.n, _lib.ptr(s)), "nufft_setpts3")
+
+    def info(self):
+        nf = ctypes.c_int()
+        d = (ctypes.c_double * 6)()
+        _lib.check(_lib.lib.curig_nufft_info3(self._h, ctypes.byref(nf), d), "nufft_info3")
+        return {"nf": nf.value, "i_center": d[0], "i_half": d[1], "o_center": d[2], "o_half": d[3],
+                "gamma": d[4], "h": d[5]}
+
+    def execute(self, c, f):
+        """Reads the strengths c [m], writes f [n]."""
+        _lib.check(_lib.lib.curig_nufft_execute(self._h, _lib.ptr(c), _lib.ptr(f)), "nufft_execute")
 
     def close(self):
         if getattr(self, "_h", None):

@@ -223,6 +223,21 @@ int curig_nufft_setpts(curig_nufft plan, int64_t m, const double *d_x, const dou
 int curig_nufft_execute(curig_nufft plan, void *d_c, void *d_fk);
 int curig_nufft_destroy(curig_nufft plan);
 
+/* Generic NUFFT type 3 in one dimension (nonuniform points to nonuniform
+ * frequencies): f_k = sum_j c_j e^{i iflag s_k x_j}, j < m, k < n; the
+ * reference's cunufft_setting type 3, dim 1 (src/fourier/cuft.cu:249-424, with
+ * its pre/post stages cuft.cu:19-124; test/nufft_1d_3_1_test.cu).  Make the plan
+ * with curig_nufft_makeplan(3, 1, n, 1, epsilon, iflag, sigma, opts, &plan) (n1:
+ * the number of frequencies, informative), then give the device float64
+ * points x[m] and frequencies s[n] here; curig_nufft_execute(plan, d_c, d_f)
+ * maps strengths c[m] to values f[n] (complex, complex64 when
+ * opts->precision = 1).  Sizes (grid nf, scale gamma, cell h) follow the
+ * reference's set_nhg_type3 (contrib/common.cpp:161-195). */
+int curig_nufft_setpts3(curig_nufft plan, int64_t m, const double *d_x, int64_t n, const double *d_s);
+/* nf and dinfo[0..5] = input centre, input half width, output centre, output
+ * half width, gamma, h of a type-3 plan with points */
+int curig_nufft_info3(curig_nufft plan, int *nf, double *dinfo);
+
 /* Last error text of this thread (static storage, empty if none). */
 const char *curig_last_error(void);
 

@@ -63,6 +63,70 @@ def test_nufft_rejects_bad_arguments():
     from curig_b200._lib import CurigError
     from curig_b200.nufft import Nufft
     with pytest.raises(CurigError):
-        Nufft(3, (16,), 1e-6)
+        Nufft(3, (16, 16), 1e-6)                   # type 3 is one-dimensional
     with pytest.raises(CurigError):
         Nufft(1, (16, 16), 1e-6, iflag=2)
+
+
+# ------------------------------------------------------------------ type 3
+def _direct3(x, s, c, iflag):
+    return np.exp(1j * iflag * np.outer(s, x)) @ c
+
+
+def _type3(x, s, c, iflag, eps, precision="fp64"):
+    import torch
+    from curig_b200.nufft import Nufft3
+    cdt = torch.complex128 if precision == "fp64" else torch.complex64
+    p = Nufft3(eps, iflag, precision=precision)
+    p.setpts(torch.from_numpy(np.ascontiguousarray(x, dtype=np.float64)).cuda(),
+             torch.from_numpy(np.ascontiguousarray(s, dtype=np.float64)).cuda())
+    out = torch.empty(len(s), dtype=cdt, device="cuda")
+    p.execute(torch.from_numpy(np.ascontiguousarray(c)).to(cdt).cuda(), out)
+    info = p.info()
+    p.close()
+    return out.cpu().numpy(), info
+
+
+@pytest.mark.gpu
+def test_type3_reference_case_points_to_frequencies():
+    """test/nufft_1d_3_1_test.cu:32-62,210-241 of the reference: M = 100 points
+    u_i = 2 + i pi / M, strengths (uniform(-1,1) * 1000, i), N = 100 frequencies
+    k_i = -i / N, epsilon 1e-6, iflag +1, against the direct sum."""
+    M, N, eps = 100, 100, 1e-6
+    rng = np.random.default_rng(31)
+    u = 2.0 + np.arange(M) * np.pi / M
+    c = rng.uniform(-1, 1, M) * 1000 + 1j * np.arange(M)
+    k = -np.arange(N) / N
+    got, info = _type3(u, k, c, +1, eps)
+    ref = _direct3(u, k, c, +1)
+    assert info["nf"] >= 2 * 7 and info["nf"] % 2 == 0
+    assert np.linalg.norm(got - ref) <= 10 * eps * np.linalg.norm(ref)
+
+
+@pytest.mark.gpu
+def test_type3_reference_case_single_frequency_to_points():
+    """test/nufft_1d_3_2_test.cu:31-95,110-160 of the reference: values at one
+    frequency (k = 0) transformed to M = 25 points u_i = 2 + i with iflag -1,
+    epsilon 1e-12 -- the same type 3 with points and frequencies exchanged."""
+    M, eps = 25, 1e-12
+    k = np.array([0.0])
+    fk = np.array([0.7 - 0.3j])
+    u = 2.0 + np.arange(M, dtype=np.float64)
+    got, _ = _type3(k, u, fk, -1, eps)
+    ref = _direct3(k, u, fk, -1)
+    assert np.linalg.norm(got - ref) <= 1e-9 * np.linalg.norm(ref)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("iflag", (1, -1))
+@pytest.mark.parametrize("precision,eps,tol", [("fp64", 1e-9, 1e-8), ("fp64", 1e-4, 1e-3), ("fp32", 1e-5, 5e-5)])
+def test_type3_random_wide_ranges(iflag, precision, eps, tol):
+    rng = np.random.default_rng(7 + iflag)
+    m, n = 3000, 2000
+    x = rng.uniform(-30.0, 50.0, m)
+    s = rng.uniform(-80.0, 20.0, n)
+    c = rng.standard_normal(m) + 1j * rng.standard_normal(m)
+    got, info = _type3(x, s, c, iflag, eps, precision)
+    ref = _direct3(x, s, c, iflag)
+    assert abs(info["i_center"] - (x.max() + x.min()) / 2) < 1e-12 * 50
+    assert np.linalg.norm(got - ref) <= tol * np.linalg.norm(ref)
