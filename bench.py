@@ -63,6 +63,8 @@ def args_():
     ap.add_argument("--bin", type=int, default=0, help="bin edge in cells (0 automatic)")
     ap.add_argument("--smem", type=int, default=0, help="shared-memory budget per tile CTA (bytes)")
     ap.add_argument("--sub", type=int, default=0, help="visibilities per tile chunk (0 automatic)")
+    ap.add_argument("--sparse", type=int, default=0,
+                    help="FP32 spreader: chunks below this many visibilities skip the tile (0 automatic, -1 never)")
     ap.add_argument("--slabs", type=int, default=0,
                     help="row slabs of the one-shot calls timed as e2e (0 automatic, 1..8)")
     ap.add_argument("--error-table", action="store_true",
@@ -517,7 +519,7 @@ def main():
             d_, o_ = torch.empty((a.npix, a.npix), dtype=c_, device=dev), torch.empty_like(v_)
         plan = GridderPlan(1, a.npix, a.npix, psx, psx, eps, 2.0, -1, precision=prec, window=win,
                            stream=stream, bin_xy=a.bin, sub=a.sub, smem_budget=a.smem,
-                           accumulate=acc_mode if accumulate is None else accumulate)
+                           accumulate=acc_mode if accumulate is None else accumulate, sparse=a.sparse)
 
         def step():
             plan.setpts(uvw, freq)

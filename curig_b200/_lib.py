@@ -47,14 +47,14 @@ dirty2ms_2.restype = c_int
 class CurigOpts(ctypes.Structure):
     _fields_ = [("precision", c_int), ("window", c_int), ("bin_xy", c_int), ("sub", c_int),
                 ("smem_budget", c_int64), ("stream", c_void_p), ("accumulate", c_int), ("w_term", c_int),
-                ("grid_x", c_int), ("grid_y", c_int), ("bin_z", c_int), ("slabs", c_int)]
+                ("grid_x", c_int), ("grid_y", c_int), ("bin_z", c_int), ("slabs", c_int), ("sparse", c_int)]
 
 
 def make_opts(precision: int = 0, window: int = 0, bin_xy: int = 0, sub: int = 0,
               smem_budget: int = 0, stream: int | None = None, accumulate: int = 0, w_term: int = 0,
-              grid_x: int = 0, grid_y: int = 0, bin_z: int = 0, slabs: int = 0) -> CurigOpts:
+              grid_x: int = 0, grid_y: int = 0, bin_z: int = 0, slabs: int = 0, sparse: int = 0) -> CurigOpts:
     return CurigOpts(precision, window, bin_xy, sub, smem_budget, stream or None, accumulate, w_term,
-                     grid_x, grid_y, bin_z, slabs)
+                     grid_x, grid_y, bin_z, slabs, sparse)
 
 
 _P = c_void_p

@@ -34,6 +34,7 @@ static Options to_options(const curig_opts *o) {
         opt.grid_x = o->grid_x;
         opt.grid_y = o->grid_y;
         opt.bin_z = o->bin_z;
+        opt.sparse = o->sparse;
     }
     return opt;
 }

@@ -476,6 +476,10 @@ __device__ __forceinline__ void red_add_v4(float *p, float a, float b, float c, 
     asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(d)
                  : "memory");
 }
+// 8-byte vector reduction into global memory (address 8-byte aligned).
+__device__ __forceinline__ void red_add_v2(float *p, float a, float b) {
+    asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(a), "f"(b) : "memory");
+}
 __device__ __forceinline__ void atomic_add_c(double2 *p, double2 v) {
     atomicAdd(&p->x, v.x);
     atomicAdd(&p->y, v.y);
@@ -1031,6 +1035,45 @@ k_spread_f32(DevGeom g, const int *__restrict__ bin_start, const int *__restrict
         const int ox = (int)bxi * g.bx - g.hkw, oy = (int)byi * g.by - g.hkw;
         const int oz = g.zpad ? (int)bzi * g.bz - g.hkw : 0;
         const int shift = ox & 1, x_al = ox - shift;
+        if (n < g.sparse_n) {
+            // A sparse chunk: its cells receive about one tap each, so the
+            // tile would only add its fixed cost (zeroing, statistics, flush);
+            // each thread adds one visibility's taps straight to the grid
+            // with 8-byte vector reductions (FP32 sums, as the flush's).
+            // Uniform across the CTA; no shared memory is touched.
+            for (int v = threadIdx.x; v < n; v += TTHREADS) {
+                const int i = start + v * stride;
+                const float4 r = rec[i];
+                const float2 c = cs[i];
+                float kx[KW], ky[KW];
+#pragma unroll
+                for (int d = 0; d < KW; ++d) {
+                    kx[d] = win_tap<float>(g, tab, r.x, d);
+                    ky[d] = win_tap<float>(g, tab, r.y, d);
+                }
+                const int cb = cell_bits(r.w);
+                const int gx0 = ox + (cb & 0x3ff), gy0 = oy + ((cb >> 10) & 0x3ff), gz0 = oz + ((cb >> 20) & 0xfff);
+                int gxs[KW];
+#pragma unroll
+                for (int dx = 0; dx < KW; ++dx) gxs[dx] = wrap3(gx0 + dx, g.nf1);
+                const int KZ = g.no_w ? 1 : KW;
+#pragma unroll 1
+                for (int dz = 0; dz < KZ; ++dz) {
+                    const float kz = g.no_w ? 1.f : win_tap<float>(g, tab, r.z, dz);
+                    const int gz = g.zpad ? wrap3(gz0 + dz, g.nf3) : gz0 + dz;
+                    const float cr = c.x * kz, ci = c.y * kz;
+#pragma unroll
+                    for (int dy = 0; dy < KW; ++dy) {
+                        float2 *row = grid + ((long long)gz * g.nf2 + wrap3(gy0 + dy, g.nf2)) * g.nf1;
+                        const float ar = cr * ky[dy], ai = ci * ky[dy];
+#pragma unroll
+                        for (int dx = 0; dx < KW; ++dx)
+                            red_add_v2(reinterpret_cast<float *>(row + gxs[dx]), ar * kx[dx], ai * kx[dx]);
+                    }
+                }
+            }
+            continue;
+        }
         float4 *tv = reinterpret_cast<float4 *>(smem);
         for (int e = threadIdx.x; e < nwords / 4; e += TTHREADS) tv[e] = make_float4(0.f, 0.f, 0.f, 0.f);
         if (one)

@@ -28,6 +28,7 @@ struct Options {
     int grid_x = 0, grid_y = 0;   // oversampled grid along the nxdirty / nydirty axes (0: sigma rule)
     int bin_z = 0;                // w-planes per tile slab (0: automatic)
     int slabs = 1;                // row slabs of the sort (one-shot copy / compute pipeline), 1..MAX_SLABS
+    int sparse = 0;               // FP32 spreader: chunks below this skip the tile (0: automatic, < 0: never)
 };
 
 struct Plan {
@@ -135,6 +136,9 @@ int plan_execute(Plan *p, void *d_vis, const void *d_wgt, void *d_dirty, int typ
 int plan_execute_slabs(Plan *p, int type, void *d_vis, const void *d_wgt, void *d_dirty,
                        const cudaEvent_t *ready, const cudaEvent_t *done, int nev, bool prologue_done = false);
 constexpr int MAX_SLABS = 8;
+// FP32 spreader: chunks with fewer visibilities spread straight to the grid
+// (each cell of such a tile receives about one tap)
+constexpr int DEFAULT_SPARSE_N = 192;
 // first row of slab k of nslab over nrow rows (k = nslab gives nrow)
 inline long long slab_first_row(long long nrow, int nslab, int k) {
     return ((long long)k * nrow + nslab - 1) / nslab;

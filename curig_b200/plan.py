@@ -47,14 +47,14 @@ class GridderPlan:
 
     def __init__(self, kind, nxdirty, nydirty, pixsize_x, pixsize_y, epsilon, sigma=2.0, sign=-1,
                  precision="fp64", window="es", stream=None, bin_xy=0, sub=0, smem_budget=0,
-                 accumulate=0, w_term=0, grid_x=0, grid_y=0, bin_z=0):
+                 accumulate=0, w_term=0, grid_x=0, grid_y=0, bin_z=0, sparse=0):
         self.kind = kind
         self.nxdirty, self.nydirty = int(nxdirty), int(nydirty)
         self.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
         self.window = WINDOWS[window] if isinstance(window, str) else int(window)
         self._stream = _stream_handle(stream)
         self._opts = _lib.make_opts(self.precision, self.window, bin_xy, sub, smem_budget, self._stream,
-                                    accumulate, w_term, grid_x, grid_y, bin_z)
+                                    accumulate, w_term, grid_x, grid_y, bin_z, sparse=sparse)
         h = ctypes.c_void_p()
         _lib.check(_lib.lib.curig_makeplan(kind, self.nxdirty, self.nydirty, float(pixsize_x),
                                            float(pixsize_y), float(epsilon), float(sigma), int(sign),
