@@ -15,7 +15,8 @@
 // Where the reference evaluates the grid's series by a direct sum over all nf
 // grid points for every frequency (in its test driver), this evaluation is
 // this library's own type-2 NUFFT of the grid at the points theta_k (grid
-// point m is mode m - nf/2): O(nf log nf + n kw) instead of O(n nf).
+// point m is mode m - nf/2): O(nf log nf + n kw) instead of O(n nf).  Kernels
+// wider than 12 (epsilon below about 1e-11) keep the direct sum.
 #include "plan.h"
 
 #include "../../include/curig.h"
@@ -101,6 +102,33 @@ __global__ void k_t3_spread(long long m, const double *__restrict__ xp, const do
             atomicAdd(&grid[idx].x, (T)(cr * w));
             atomicAdd(&grid[idx].y, (T)(ci * w));
         }
+    }
+}
+
+// The grid's series by direct summation (tolerances that need kernels wider
+// than the type-2 NUFFT's tile kernels take): thread per frequency, the phase
+// e^{i iflag theta (m - nf/2)} advanced by one rotation per grid point and
+// taken afresh from sincos every 64 points.
+template <typename T>
+__global__ void k_t3_direct(long long n, const double *__restrict__ theta, int iflag, int nf,
+                            const typename cplx_t<T>::type *__restrict__ grid, typename cplx_t<T>::type *__restrict__ F) {
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+         k += (long long)gridDim.x * blockDim.x) {
+        const double th = theta[k] * iflag;
+        double sr, cr;
+        sincos(th, &sr, &cr);
+        double ar = 0.0, ai = 0.0, er = 0.0, ei = 0.0;
+        for (int m = 0; m < nf; ++m) {
+            if ((m & 63) == 0) sincos(th * (double)(m - nf / 2), &ei, &er);
+            const double gr = grid[m].x, gi = grid[m].y;
+            ar += gr * er - gi * ei;
+            ai += gr * ei + gi * er;
+            const double nr = er * cr - ei * sr;
+            ei = er * sr + ei * cr;
+            er = nr;
+        }
+        F[k].x = (T)ar;
+        F[k].y = (T)ai;
     }
 }
 
@@ -210,7 +238,9 @@ int nufft3_setpts(Nufft3 *p, long long m, const double *d_x, long long n, const 
     k_t3_points<<<grid_blocks(m), 256, 0, p->st>>>(m, d_x, p->i_c, p->gamma, p->o_c, p->iflag, p->d_xp, p->d_pre);
     k_t3_targets<<<grid_blocks(n), 256, 0, p->st>>>(n, d_s, p->o_c, p->gamma, p->h, p->i_c, p->iflag, nq, p->d_quad,
                                                     p->d_quad + MAX_QUAD, p->d_theta, p->d_post);
-    // the grid's Fourier series at theta_k: a type-2 NUFFT with nf modes
+    // the grid's Fourier series at theta_k: a type-2 NUFFT with nf modes (its
+    // tile kernels take widths up to 12; beyond, direct summation)
+    if (p->kp.kw > TAB_KW) return cudaGetLastError() == cudaSuccess ? OK : ERR_CUDA;
     curig_opts o;
     curig_default_opts(&o);
     if (opts) o = *opts;
@@ -222,7 +252,7 @@ int nufft3_setpts(Nufft3 *p, long long m, const double *d_x, long long n, const 
 }
 
 int nufft3_execute(Nufft3 *p, const void *d_c, void *d_f) {
-    if (!p || !p->inner || !d_c || !d_f) return ERR_ARG;
+    if (!p || !p->d_grid || !d_c || !d_f) return ERR_ARG;
     const size_t esz = p->precision ? 8 : 16;
     if (cudaMemsetAsync(p->d_grid, 0, (size_t)p->nf * esz, p->st) != cudaSuccess) return ERR_CUDA;
     count_launch(2);
@@ -235,8 +265,20 @@ int nufft3_execute(Nufft3 *p, const void *d_c, void *d_f) {
                                                                  static_cast<const double2 *>(d_c), p->nf, p->kp.kw,
                                                                  p->kp.beta, p->kp.c, static_cast<double2 *>(p->d_grid));
     }
-    int s = curig_nufft_execute(p->inner, p->d_F, p->d_grid);
-    if (s != OK) return s;
+    if (p->inner) {
+        int s = curig_nufft_execute(p->inner, p->d_F, p->d_grid);
+        if (s != OK) return s;
+    } else {
+        count_launch();
+        if (p->precision)
+            k_t3_direct<float><<<grid_blocks(p->n), 256, 0, p->st>>>(p->n, p->d_theta, p->iflag, p->nf,
+                                                                    static_cast<const float2 *>(p->d_grid),
+                                                                    static_cast<float2 *>(p->d_F));
+        else
+            k_t3_direct<double><<<grid_blocks(p->n), 256, 0, p->st>>>(p->n, p->d_theta, p->iflag, p->nf,
+                                                                     static_cast<const double2 *>(p->d_grid),
+                                                                     static_cast<double2 *>(p->d_F));
+    }
     if (p->precision)
         k_t3_finish<float><<<grid_blocks(p->n), 256, 0, p->st>>>(p->n, p->d_post, static_cast<const float2 *>(p->d_F),
                                                                 static_cast<float2 *>(d_f));
