@@ -745,43 +745,6 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
         const int ox = (int)bxi * g.bx - g.hkw, oy = (int)byi * g.by - g.hkw;
         const int oz = g.zpad ? (int)bzi * g.bz - g.hkw : 0;
         const int shift = ox & 1, x_al = ox - shift;
-        if (n < g.sparse_n) {
-            // A sparse chunk (one channel per call leaves about 33 visibilities
-            // per tile): each thread adds one visibility's taps straight to the
-            // grid with FP64 global atomics, skipping the tile's fixed cost.
-            // Uniform across the CTA; no shared memory is touched.
-            for (int v = threadIdx.x; v < n; v += TTHREADS) {
-                const int i = start + v * stride;
-                const R<T> r = rec[i];
-                const C<T> c = cs[i];
-                T kx[KW], ky[KW];
-#pragma unroll
-                for (int d = 0; d < KW; ++d) {
-                    kx[d] = win_tap<T>(g, tab, r.x, d);
-                    ky[d] = win_tap<T>(g, tab, r.y, d);
-                }
-                const int cb = cell_bits(r.w);
-                const int gx0 = ox + (cb & 0x3ff), gy0 = oy + ((cb >> 10) & 0x3ff), gz0 = oz + ((cb >> 20) & 0xfff);
-                int gxs[KW];
-#pragma unroll
-                for (int dx = 0; dx < KW; ++dx) gxs[dx] = wrap3(gx0 + dx, g.nf1);
-                const int KZ = g.no_w ? 1 : KW;
-#pragma unroll 1
-                for (int dz = 0; dz < KZ; ++dz) {
-                    const T kz = g.no_w ? (T)1 : win_tap<T>(g, tab, r.z, dz);
-                    const int gz = g.zpad ? wrap3(gz0 + dz, g.nf3) : gz0 + dz;
-                    const T cr = c.x * kz, ci = c.y * kz;
-#pragma unroll
-                    for (int dy = 0; dy < KW; ++dy) {
-                        C<T> *row = grid + ((long long)gz * g.nf2 + wrap3(gy0 + dy, g.nf2)) * g.nf1;
-                        const T ar = cr * ky[dy], ai = ci * ky[dy];
-#pragma unroll
-                        for (int dx = 0; dx < KW; ++dx) atomic_add_c(row + gxs[dx], C<T>{ar * kx[dx], ai * kx[dx]});
-                    }
-                }
-            }
-            continue;
-        }
         float4 *tv = reinterpret_cast<float4 *>(smem);
         for (int e = threadIdx.x; e < nvec; e += TTHREADS) tv[e] = make_float4(0.f, 0.f, 0.f, 0.f);
         if (!fix && !fix64)                              // (ntile is even: 24-byte cells fill whole float4s)

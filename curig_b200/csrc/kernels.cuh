@@ -19,7 +19,7 @@ struct DevGeom {
     double ibx, iby, ibz;          // 1 / bx, 1 / by, 1 / bz
     int tx, ty, tz, zpad;
     int sub;                       // visibilities per sub-problem
-    int sparse_n;                  // spreader: chunks of fewer visibilities skip the tile
+    int sparse_n;                  // FP32 spreader: chunks of fewer visibilities skip the tile
     int cbits;                     // bits of the in-tile start cell in the sort key (0: bin only)
     int smode;                     // tile accumulation: 0 two-word int32, 1 float atomics, 2 one-word int32
                                    // (FP64: 1 double atomics, else int64 + int32)

@@ -136,10 +136,12 @@ int plan_execute(Plan *p, void *d_vis, const void *d_wgt, void *d_dirty, int typ
 int plan_execute_slabs(Plan *p, int type, void *d_vis, const void *d_wgt, void *d_dirty,
                        const cudaEvent_t *ready, const cudaEvent_t *done, int nev, bool prologue_done = false);
 constexpr int MAX_SLABS = 8;
-// Spreader: chunks with fewer visibilities spread straight to the grid (each
-// cell of such a tile receives about one tap); the FP64 tile (24 bytes per
-// cell, one CTA per SM) costs more to zero and flush, hence the higher bound
-constexpr int DEFAULT_SPARSE_N_F32 = 192, DEFAULT_SPARSE_N_F64 = 384;
+// FP32 spreader: chunks with fewer visibilities spread straight to the grid
+// (each cell of such a tile receives about one tap).  FP64 keeps the tile for
+// every chunk: its scattered double atomics measured slower than the flush's
+// row-contiguous ones (one channel of the 4096^2 configuration: 203 against
+// 85 ms per ms2dirty call).
+constexpr int DEFAULT_SPARSE_N = 192;
 // first row of slab k of nslab over nrow rows (k = nslab gives nrow)
 inline long long slab_first_row(long long nrow, int nslab, int k) {
     return ((long long)k * nrow + nslab - 1) / nslab;
