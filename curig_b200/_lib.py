@@ -118,6 +118,11 @@ lib.curig_nufft_execute.restype = c_int
 lib.curig_nufft_destroy.argtypes = [c_void_p]
 lib.curig_nufft_destroy.restype = c_int
 lib.curig_default_opts.restype = None
+lib.curig_nufft3d_makeplan.argtypes = [c_int, c_int, c_int, c_int, c_double, c_int, c_double,
+                                       ctypes.POINTER(CurigOpts), ctypes.POINTER(c_void_p)]
+lib.curig_nufft3d_makeplan.restype = c_int
+lib.curig_nufft3d_setpts.argtypes = [c_void_p, c_int64, _P, _P, _P]
+lib.curig_nufft3d_setpts.restype = c_int
 lib.curig_nufft_setpts3.argtypes = [c_void_p, c_int64, _P, c_int64, _P]
 lib.curig_nufft_setpts3.restype = c_int
 lib.curig_nufft_info3.argtypes = [c_void_p, ctypes.POINTER(c_int), ctypes.POINTER(c_double)]

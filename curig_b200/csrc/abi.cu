@@ -269,8 +269,9 @@ struct curig_nufft_s {
     Plan *p = nullptr;
     Nufft3 *t3 = nullptr;                 // type 3
     curig_opts opts{};
-    int type = 1, dim = 1, n1 = 0, n2 = 1, iflag = 1;
+    int type = 1, dim = 1, n1 = 0, n2 = 1, n3 = 1, iflag = 1;
     double *d_uvw = nullptr;
+    const double *d_z = nullptr;          // 3-D: the third coordinate, for setpts
 };
 
 extern "C" int curig_nufft_makeplan(int type, int dim, int n1, int n2, double eps, int iflag, double sigma,
@@ -311,6 +312,41 @@ extern "C" int curig_nufft_makeplan(int type, int dim, int n1, int n2, double ep
     return OK;
 }
 
+// Generic 3-D NUFFT of types 1 and 2: the w-free gridder with a periodic third
+// axis of the NUFFT's own grid size (opts n3): a point (x, y, z) becomes the
+// row s (x, y, z) / 2pi at frequency c, and the third axis is transformed and
+// corrected like the first two (k_correct3_m2d / k_correct3_d2m).  Modes
+// [n1][n2][n3], mode k = index - n/2 on every axis.
+extern "C" int curig_nufft3d_makeplan(int type, int n1, int n2, int n3, double eps, int iflag, double sigma,
+                                      const curig_opts *opts, curig_nufft *out) {
+    if (!out) return fail(ERR_ARG, "null plan pointer");
+    *out = nullptr;
+    if ((type != 1 && type != 2) || n1 <= 0 || n2 <= 0 || n3 <= 0 || (iflag != 1 && iflag != -1))
+        return fail(ERR_ARG, "invalid 3-D NUFFT plan arguments");
+    Options o = to_options(opts);
+    o.w_term = 0;
+    o.n3 = n3;
+    Plan *p = nullptr;
+    int s = plan_create(type, n1, n2, 1.0, 1.0, eps, sigma, 1, o, &p);
+    if (s != OK) return fail(s, "3-D NUFFT plan creation failed");
+    *out = new curig_nufft_s;
+    (*out)->p = p;
+    (*out)->type = type;
+    (*out)->dim = 3;
+    (*out)->n1 = n1;
+    (*out)->n2 = n2;
+    (*out)->n3 = n3;
+    (*out)->iflag = iflag;
+    return OK;
+}
+
+extern "C" int curig_nufft3d_setpts(curig_nufft h, int64_t m, const double *d_x, const double *d_y,
+                                    const double *d_z) {
+    if (!h || h->dim != 3 || !d_y || !d_z) return fail(ERR_ARG, "not a 3-D plan, or missing coordinates");
+    h->d_z = d_z;
+    return curig_nufft_setpts(h, m, d_x, d_y);
+}
+
 extern "C" int curig_nufft_setpts3(curig_nufft h, int64_t m, const double *d_x, int64_t n, const double *d_s) {
     if (!h || h->type != 3) return fail(ERR_ARG, "not a type-3 plan");
     int s = nufft3_setpts(h->t3, m, d_x, n, d_s, &h->opts);
@@ -325,7 +361,8 @@ extern "C" int curig_nufft_info3(curig_nufft h, int *nf, double *dinfo) {
 }
 
 extern "C" int curig_nufft_setpts(curig_nufft h, int64_t m, const double *d_x, const double *d_y) {
-    if (!h || !d_x || m <= 0 || (h->dim == 2 && !d_y)) return fail(ERR_ARG, "invalid NUFFT points");
+    if (!h || !d_x || m <= 0 || (h->dim >= 2 && !d_y) || (h->dim == 3 && !h->d_z))
+        return fail(ERR_ARG, "invalid NUFFT points");
     if (h->type == 3) return fail(ERR_ARG, "type-3 plans take their points with curig_nufft_setpts3");
     Plan *p = h->p;
     if (h->d_uvw) cudaFreeAsync(h->d_uvw, p->st);
@@ -333,7 +370,7 @@ extern "C" int curig_nufft_setpts(curig_nufft h, int64_t m, const double *d_x, c
     if (cudaMallocAsync((void **)&h->d_uvw, 3 * m * sizeof(double), p->st) != cudaSuccess)
         return fail(ERR_NOMEM, "out of device memory");
     const double sgn = h->type == 1 ? (double)h->iflag : -(double)h->iflag;
-    launch_nupts_uvw(m, d_x, h->dim == 2 ? d_y : nullptr, sgn, h->d_uvw, p->st);
+    launch_nupts_uvw(m, d_x, h->dim >= 2 ? d_y : nullptr, h->dim == 3 ? h->d_z : nullptr, sgn, h->d_uvw, p->st);
     const double freq = SPEEDOFLIGHT;                   // f / c = 1
     int s = plan_setpts(p, m, 1, h->d_uvw, h->d_uvw + 1, h->d_uvw + 2, 3, &freq);
     if (s != OK) return fail(s, p->last_error.empty() ? "NUFFT setpts failed" : p->last_error);

@@ -1671,6 +1671,86 @@ __global__ void k_correct_d2m(DevCorr cc, const C<T> *__restrict__ dirty, C<T> *
     }
 }
 
+// Generic 3-D NUFFT (types 1 and 2): the third axis is a periodic grid of nf3
+// planes like the first two, so after the planes' 2-D transforms (the image
+// columns in T[z][x'][y]) the modes k3 = iz - n3/2 are the planes' series
+// sum_p T[p] e^{+2 pi i k3 p / nf3}, divided by psi1 psi2 psi3 (the grid tables
+// with the half-grid sign, as the first two axes).  Modes fk [nx][ny][n3],
+// n3 fastest; pixel (ix, iy) maps to T's column as in k_correct_m2d.  The
+// phase is advanced by one rotation per term and taken afresh every 64 terms.
+__device__ __forceinline__ void col3(const DevCorr &cc, int ix, int iy, int &r, int &s, long long &off) {
+    const int hx = cc.nx / 2, hy = cc.ny / 2;
+    int w2, xp;
+    if (ix >= hx) { r = ix - hx; w2 = r; } else { r = hx - ix; w2 = cc.nf2 - r; }
+    if (iy >= hy) { s = iy - hy; xp = s; } else { s = hy - iy; xp = cc.ny - s; }
+    off = (long long)xp * cc.nf2 + w2;
+}
+
+template <typename T>
+__global__ void k_correct3_m2d(DevCorr cc, const C<T> *__restrict__ tg, C<T> *__restrict__ fk) {
+    const long long total = (long long)cc.nx * cc.ny * cc.n3;
+    const long long plane = (long long)cc.ny * cc.nf2;
+    for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < total;
+         o += (long long)gridDim.x * blockDim.x) {
+        const int iz = (int)(o % cc.n3);
+        const long long pix = o / cc.n3;
+        const int iy = (int)(pix % cc.ny), ix = (int)(pix / cc.ny);
+        int r, s;
+        long long off;
+        col3(cc, ix, iy, r, s, off);
+        const int k3 = iz - cc.n3 / 2;
+        const double th = 2.0 * PI_D * (double)k3 / (double)cc.nf3;
+        double sr, cr, er = 1.0, ei = 0.0, ar = 0.0, ai = 0.0;
+        sincos(th, &sr, &cr);
+        for (int p = 0; p < cc.nf3; ++p) {
+            if ((p & 63) == 0) sincos(th * (double)p, &ei, &er);
+            const C<T> v = tg[p * plane + off];
+            ar += (double)v.x * er - (double)v.y * ei;
+            ai += (double)v.x * ei + (double)v.y * er;
+            const double nr = er * cr - ei * sr;
+            ei = er * sr + ei * cr;
+            er = nr;
+        }
+        const double den = cc.psi1[s] * cc.psi2[r] * cc.psi3[k3 < 0 ? -k3 : k3];
+        fk[o] = C<T>{(T)(ar / den), (T)(ai / den)};
+    }
+}
+
+// Type 2: plane p at pixel (ix, iy) = sum_k3 fk[ix][iy][k3] / (psi1 psi2 psi3)
+// e^{-2 pi i k3 p / nf3}, written where k_correct_d2m writes (the other rows of
+// T are zeroed by k_zero_tpad).  Thread per (plane, pixel), pixel x fastest.
+template <typename T>
+__global__ void k_correct3_d2m(DevCorr cc, const C<T> *__restrict__ fk, C<T> *__restrict__ tg) {
+    const long long total = (long long)cc.nx * cc.ny * cc.nf3;
+    const long long plane = (long long)cc.ny * cc.nf2;
+    for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < total;
+         o += (long long)gridDim.x * blockDim.x) {
+        const int ix = (int)(o % cc.nx);
+        const long long t = o / cc.nx;
+        const int iy = (int)(t % cc.ny), p = (int)(t / cc.ny);
+        int r, s;
+        long long off;
+        col3(cc, ix, iy, r, s, off);
+        const C<T> *f = fk + ((long long)ix * cc.ny + iy) * cc.n3;
+        const double th = -2.0 * PI_D * (double)p / (double)cc.nf3;    // phase step per k3
+        double sr, cr, er = 1.0, ei = 0.0, ar = 0.0, ai = 0.0;
+        sincos(th, &sr, &cr);
+        for (int iz = 0; iz < cc.n3; ++iz) {
+            const int k3 = iz - cc.n3 / 2;
+            if ((iz & 63) == 0) sincos(th * (double)k3, &ei, &er);
+            const double w = 1.0 / cc.psi3[k3 < 0 ? -k3 : k3];
+            const double vr = (double)f[iz].x * w, vi = (double)f[iz].y * w;
+            ar += vr * er - vi * ei;
+            ai += vr * ei + vi * er;
+            const double nr = er * cr - ei * sr;
+            ei = er * sr + ei * cr;
+            er = nr;
+        }
+        const double den = cc.psi1[s] * cc.psi2[r];
+        tg[p * plane + off] = C<T>{(T)(ar / den), (T)(ai / den)};
+    }
+}
+
 // psi-hat of the window on the grid (deconv.cu:60-103): out[k] =
 // 2 sum_i g_i cos((x_i - N + 1) / (N - 1) pi k), N = nf/2 + 1, the same
 // arithmetic as the host psi_hat_grid.
@@ -1951,6 +2031,22 @@ void launch_correct_d2m(const DevCorr &cc, const void *dirty, void *grid, cudaSt
 }
 
 template <typename T>
+void launch_correct3_m2d(const DevCorr &cc, const void *tgrid, void *fk, cudaStream_t st) {
+    const long long total = (long long)cc.nx * cc.ny * cc.n3;
+    count_launch();
+    k_correct3_m2d<T><<<grid_for(total, 128), 128, 0, st>>>(cc, reinterpret_cast<const C<T> *>(tgrid),
+                                                            reinterpret_cast<C<T> *>(fk));
+}
+
+template <typename T>
+void launch_correct3_d2m(const DevCorr &cc, const void *fk, void *tgrid, cudaStream_t st) {
+    const long long total = (long long)cc.nx * cc.ny * cc.nf3;
+    count_launch();
+    k_correct3_d2m<T><<<grid_for(total, 128), 128, 0, st>>>(cc, reinterpret_cast<const C<T> *>(fk),
+                                                            reinterpret_cast<C<T> *>(tgrid));
+}
+
+template <typename T>
 void launch_cols_to_t(int ny, int nf1, int nf2, int nf3, const void *grid, void *t, cudaStream_t st) {
     count_launch();
     dim3 g((ny + 31) / 32, (nf2 + 31) / 32, nf3);
@@ -1968,19 +2064,20 @@ void launch_t_to_grid(int ny, int nf1, int nf2, int nf3, const void *t, void *gr
 
 // Nonuniform points of the generic NUFFT as gridder rows: (s x / 2pi, s y / 2pi, 0)
 // (with unit pixels and frequency c the gridder's phase is then +-k.x).
-__global__ void k_nupts_uvw(long long m, const double *__restrict__ x, const double *__restrict__ y, double s,
-                            double *__restrict__ uvw) {
+__global__ void k_nupts_uvw(long long m, const double *__restrict__ x, const double *__restrict__ y,
+                            const double *__restrict__ z, double s, double *__restrict__ uvw) {
     for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < m;
          j += (long long)gridDim.x * blockDim.x) {
         uvw[3 * j] = s * x[j] * INV_2PI;
         uvw[3 * j + 1] = y ? s * y[j] * INV_2PI : 0.0;
-        uvw[3 * j + 2] = 0.0;
+        uvw[3 * j + 2] = z ? s * z[j] * INV_2PI : 0.0;
     }
 }
 
-void launch_nupts_uvw(long long m, const double *x, const double *y, double s, double *uvw, cudaStream_t st) {
+void launch_nupts_uvw(long long m, const double *x, const double *y, const double *z, double s, double *uvw,
+                      cudaStream_t st) {
     count_launch();
-    k_nupts_uvw<<<grid_for(m), NTHREADS, 0, st>>>(m, x, y, s, uvw);
+    k_nupts_uvw<<<grid_for(m), NTHREADS, 0, st>>>(m, x, y, z, s, uvw);
 }
 
 void launch_psi_grid(int n, int nq, const double *qx, const double *qg, double *out, cudaStream_t st) {
@@ -2011,6 +2108,8 @@ void launch_zero_tpad(int nx, int ny, int nf2, int nf3, void *t, cudaStream_t st
                                   VisIO, long long, const CUtensorMap *, int *, int, cudaStream_t);   \
     template void launch_correct_m2d<T>(const DevCorr &, const void *, void *, cudaStream_t);         \
     template void launch_correct_d2m<T>(const DevCorr &, const void *, void *, cudaStream_t);         \
+    template void launch_correct3_m2d<T>(const DevCorr &, const void *, void *, cudaStream_t);        \
+    template void launch_correct3_d2m<T>(const DevCorr &, const void *, void *, cudaStream_t);        \
     template void launch_cols_to_t<T>(int, int, int, int, const void *, void *, cudaStream_t);         \
     template void launch_t_to_grid<T>(int, int, int, int, const void *, void *, cudaStream_t);         \
     template void launch_zero_tpad<T>(int, int, int, int, void *, cudaStream_t);

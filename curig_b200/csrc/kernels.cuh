@@ -53,6 +53,8 @@ struct DevCorr {
     const double *qg;              // quadrature weights * window
     const double *psi1;            // [nf1/2+1]
     const double *psi2;            // [nf2/2+1]
+    int n3;                        // generic 3-D NUFFT: modes along z (0: w-stacking or 2-D)
+    const double *psi3;            // 3-D NUFFT: [nf3/2+1], like psi1 / psi2
 };
 
 enum ErrFlag : int { EF_NONFINITE = 1, EF_RANGE = 2, EF_TIMEOUT = 4 };

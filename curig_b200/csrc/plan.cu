@@ -280,7 +280,7 @@ int plan_create(int type, int nx, int ny, double psx, double psy, double eps, do
 
 void plan_release_points(Plan *p) {
     cudaStream_t st = p->st;
-    dfree(p->d_foc, st); dfree(p->d_quad, st); dfree(p->d_psi1, st); dfree(p->d_psi2, st);
+    dfree(p->d_foc, st); dfree(p->d_quad, st); dfree(p->d_psi1, st); dfree(p->d_psi2, st); dfree(p->d_psi3, st);
     dfree(p->d_wcoef, st); dfree(p->d_bin_count, st); dfree(p->d_bin_start, st);
     dfree(p->d_nsub, st); dfree(p->d_sub_end, st); dfree(p->d_keys_in, st); dfree(p->d_kcount, st);
     dfree(p->d_idx, st); dfree(p->d_err, st); dfree(p->d_keys, st); dfree(p->d_scan, st);
@@ -343,6 +343,7 @@ static int choose_tiles(Plan *p, int esize, bool force_slabs) {
     };
     double z0 = zstart(p->wmin_eff), z1 = zstart(p->wmax_eff);
     bool nowrap = gp.no_w || (!force_slabs && z0 >= 0.0 && z1 <= gp.nf3 - kw && gp.nf3 <= 4000);
+    if (p->opt.n3 > 0) nowrap = false;                  // 3-D NUFFT: the third axis is periodic
     const int cand[] = {96, 64, 48, 32, 24, 20, 16, 12, 10, 8, 6, 4, 2};
     double best = 1e30;
     int bb = 0, bz_best = 0;
@@ -443,10 +444,18 @@ int plan_setpts_geometry(Plan *p, long long nrow, int nchan, const double *du, c
     GridRequest req;
     req.grid_x = p->opt.grid_x;
     req.grid_y = p->opt.grid_y;
-    req.no_w = p->opt.w_term == 1;
+    req.no_w = p->opt.w_term == 1 || p->opt.n3 > 0;
     int s = grid_params(p->nx, p->ny, p->psx, p->psy, lo, hi, p->eps, p->sigma, p->sign, p->gp, kw_override, req);
     if (s != OK) return s;
     if (req.no_w && p->gp.kp.kw > TAB_KW) return ERR_UNSUPPORTED;   // thread-per-visibility kernels only
+    if (p->opt.n3 > 0) {        // generic 3-D NUFFT: a periodic third axis of the NUFFT's own size
+        GridParams &g3 = p->gp;
+        g3.no_w = 0;
+        g3.nf3 = get_num_cells(p->opt.n3, g3.kp);
+        g3.gamma = 1.0;
+        g3.i_center = g3.i_half = g3.o_center = g3.o_half = 0.0;
+        g3.h = 2 * PI_D / g3.nf3;
+    }
     p->win.kw = p->gp.kp.kw;
     // 3. correction tables (deconv.cu:60-197): psi1, psi2 on the grid, quadrature for psi3
     //    (psi1 / psi2 evaluated on the device from the quadrature: no host work
@@ -463,6 +472,10 @@ int plan_setpts_geometry(Plan *p, long long nrow, int nchan, const double *du, c
     CU_TRY(cudaMemcpyAsync(p->d_quad + MAX_QUAD, qg, nq * sizeof(double), cudaMemcpyHostToDevice, st));
     launch_psi_grid(gp.nf1 / 2 + 1, nq, p->d_quad, p->d_quad + MAX_QUAD, p->d_psi1, st);
     launch_psi_grid(gp.nf2 / 2 + 1, nq, p->d_quad, p->d_quad + MAX_QUAD, p->d_psi2, st);
+    if (p->opt.n3 > 0) {
+        CU_TRY(dalloc(&p->d_psi3, (gp.nf3 / 2 + 1) * sizeof(double), st));
+        launch_psi_grid(gp.nf3 / 2 + 1, nq, p->d_quad, p->d_quad + MAX_QUAD, p->d_psi3, st);
+    }
     if (p->win.kind == 1) {
         CU_TRY(dalloc(&p->d_wcoef, p->win.coef.size() * sizeof(double), st));
         CU_TRY(cudaMemcpyAsync(p->d_wcoef, p->win.coef.data(), p->win.coef.size() * sizeof(double),
@@ -473,6 +486,7 @@ int plan_setpts_geometry(Plan *p, long long nrow, int nchan, const double *du, c
     cc.psx = gp.pixsize_x; cc.psy = gp.pixsize_y; cc.o_center = gp.o_center; cc.i_center = gp.i_center;
     cc.gamma = gp.gamma; cc.h = gp.h; cc.nquad = nq; cc.no_w = gp.no_w;
     cc.qx = p->d_quad; cc.qg = p->d_quad + MAX_QUAD; cc.psi1 = p->d_psi1; cc.psi2 = p->d_psi2;
+    cc.n3 = p->opt.n3; cc.psi3 = p->d_psi3;
 
     // 4. fine grid and FFT plans
     size_t gbytes = (size_t)gp.nf1 * gp.nf2 * gp.nf3 * 2 * esize;
@@ -776,12 +790,14 @@ static int execute_t(Plan *p, int type, void *d_vis, const void *d_wgt, void *d_
         s = plane_fft<T>(p, CUFFT_INVERSE, true);    // +1, cuft.cu:127-143
         if (s) return s;
         mark(p, EV_M2D_FFT);
-        launch_correct_m2d<T>(p->dc, p->d_tgrid, d_dirty, st);
+        if (p->opt.n3 > 0) launch_correct3_m2d<T>(p->dc, p->d_tgrid, d_dirty, st);
+        else launch_correct_m2d<T>(p->dc, p->d_tgrid, d_dirty, st);
         mark(p, EV_M2D_END);
     } else {
         mark(p, EV_D2M_BEGIN);
         launch_zero_tpad<T>(p->nx, p->ny, gp.nf2, gp.nf3, p->d_tgrid, st);
-        launch_correct_d2m<T>(p->dc, d_dirty, p->d_tgrid, st);
+        if (p->opt.n3 > 0) launch_correct3_d2m<T>(p->dc, d_dirty, p->d_tgrid, st);
+        else launch_correct_d2m<T>(p->dc, d_dirty, p->d_tgrid, st);
         mark(p, EV_D2M_CORRECT);
         s = plane_fft<T>(p, CUFFT_FORWARD, false);   // -1
         if (s) return s;

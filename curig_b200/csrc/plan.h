@@ -29,6 +29,7 @@ struct Options {
     int bin_z = 0;                // w-planes per tile slab (0: automatic)
     int slabs = 1;                // row slabs of the sort (one-shot copy / compute pipeline), 1..MAX_SLABS
     int sparse = 0;               // FP32 spreader: chunks below this skip the tile (0: automatic, < 0: never)
+    int n3 = 0;                   // generic 3-D NUFFT: modes along the third axis (0: the gridder)
 };
 
 struct Plan {
@@ -64,6 +65,7 @@ struct Plan {
 
     // device buffers owned by the plan
     double *d_foc = nullptr, *d_quad = nullptr, *d_psi1 = nullptr, *d_psi2 = nullptr, *d_wcoef = nullptr;
+    double *d_psi3 = nullptr;          // generic 3-D NUFFT: window transform on the third axis [nf3/2+1]
     int *d_bin_count = nullptr, *d_bin_start = nullptr, *d_nsub = nullptr, *d_sub_end = nullptr;
     unsigned *d_keys_in = nullptr;                      // sort key per visibility (input order)
     int *d_kcount = nullptr;                            // count / first position per key value
@@ -189,6 +191,11 @@ template <typename T>
 void launch_correct_m2d(const DevCorr &cc, const void *grid, void *dirty, cudaStream_t st);
 template <typename T>
 void launch_correct_d2m(const DevCorr &cc, const void *dirty, void *grid, cudaStream_t st);
+// generic 3-D NUFFT: modes fk [nx][ny][n3] from / to the transformed planes
+template <typename T>
+void launch_correct3_m2d(const DevCorr &cc, const void *tgrid, void *fk, cudaStream_t st);
+template <typename T>
+void launch_correct3_d2m(const DevCorr &cc, const void *fk, void *tgrid, cudaStream_t st);
 template <typename T>
 void launch_cols_to_t(int ny, int nf1, int nf2, int nf3, const void *grid, void *t, cudaStream_t st);
 template <typename T>
@@ -196,7 +203,8 @@ void launch_t_to_grid(int ny, int nf1, int nf2, int nf3, const void *t, void *gr
 template <typename T>
 void launch_zero_tpad(int nx, int ny, int nf2, int nf3, void *t, cudaStream_t st);
 void launch_psi_grid(int n, int nq, const double *qx, const double *qg, double *out, cudaStream_t st);
-void launch_nupts_uvw(long long m, const double *x, const double *y, double s, double *uvw, cudaStream_t st);
+void launch_nupts_uvw(long long m, const double *x, const double *y, const double *z, double s, double *uvw,
+                      cudaStream_t st);
 
 int plan_device_status(Plan *p);
 // Bound on the polls of the interpolator's tile-load wait for plans whose

@@ -18,30 +18,38 @@ from .plan import PRECISIONS, _stream_handle
 
 
 class Nufft:
-    """One type-1 or type-2 transform with n_modes = (n1,) or (n1, n2)."""
+    """One type-1 or type-2 transform with n_modes = (n1,), (n1, n2) or (n1, n2, n3)."""
 
     def __init__(self, nufft_type, n_modes, epsilon, iflag=1, sigma=2.0, precision="fp64", stream=None):
         n_modes = tuple(int(n) for n in n_modes)
-        if len(n_modes) not in (1, 2):
-            raise ValueError("n_modes must have one or two entries")
+        if len(n_modes) not in (1, 2, 3):
+            raise ValueError("n_modes must have one to three entries")
         self.type, self.n_modes = int(nufft_type), n_modes
         self.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
         self._opts = _lib.make_opts(self.precision, stream=_stream_handle(stream))
         h = ctypes.c_void_p()
-        _lib.check(_lib.lib.curig_nufft_makeplan(self.type, len(n_modes), n_modes[0],
-                                                 n_modes[1] if len(n_modes) == 2 else 1, float(epsilon),
-                                                 int(iflag), float(sigma), ctypes.byref(self._opts),
-                                                 ctypes.byref(h)), "nufft_makeplan")
+        if len(n_modes) == 3:
+            _lib.check(_lib.lib.curig_nufft3d_makeplan(self.type, *n_modes, float(epsilon), int(iflag), float(sigma),
+                                                       ctypes.byref(self._opts), ctypes.byref(h)), "nufft3d_makeplan")
+        else:
+            _lib.check(_lib.lib.curig_nufft_makeplan(self.type, len(n_modes), n_modes[0],
+                                                     n_modes[1] if len(n_modes) == 2 else 1, float(epsilon),
+                                                     int(iflag), float(sigma), ctypes.byref(self._opts),
+                                                     ctypes.byref(h)), "nufft_makeplan")
         self._h = h
         self._keep = None
 
-    def setpts(self, x, y=None):
-        """x (and y): contiguous float64 CUDA tensors of the m point coordinates."""
-        if len(self.n_modes) == 2 and y is None:
-            raise ValueError("two-dimensional transform needs y")
-        self._keep = (x, y)
+    def setpts(self, x, y=None, z=None):
+        """x (y, z): contiguous float64 CUDA tensors of the m point coordinates."""
+        if len(self.n_modes) >= 2 and y is None or len(self.n_modes) == 3 and z is None:
+            raise ValueError(f"{len(self.n_modes)}-dimensional transform needs {len(self.n_modes)} coordinates")
+        self._keep = (x, y, z)
         self.m = int(x.shape[0])
-        _lib.check(_lib.lib.curig_nufft_setpts(self._h, self.m, _lib.ptr(x), _lib.ptr(y)), "nufft_setpts")
+        if len(self.n_modes) == 3:
+            _lib.check(_lib.lib.curig_nufft3d_setpts(self._h, self.m, _lib.ptr(x), _lib.ptr(y), _lib.ptr(z)),
+                       "nufft3d_setpts")
+        else:
+            _lib.check(_lib.lib.curig_nufft_setpts(self._h, self.m, _lib.ptr(x), _lib.ptr(y)), "nufft_setpts")
 
     def execute(self, c, fk):
         """Type 1 reads c [m], writes fk (n_modes); type 2 reads fk, writes c."""

@@ -237,6 +237,16 @@ int curig_nufft_destroy(curig_nufft plan);
  * opts->precision = 1).  Sizes (grid nf, scale gamma, cell h) follow the
  * reference's set_nhg_type3 (contrib/common.cpp:161-195). */
 int curig_nufft_setpts3(curig_nufft plan, int64_t m, const double *d_x, int64_t n, const double *d_s);
+
+/* Generic NUFFT, types 1 and 2 in three dimensions (the reference's
+ * cunufft_setting with dim 3, src/fourier/cuft.cu:293-305): modes fk
+ * [n1][n2][n3] (n3 fastest), mode k = index - n/2 on every axis; points
+ * x, y, z (device float64, radians, periodic).  Type 1: fk[k] = sum_j c_j
+ * e^{i iflag k.x_j}; type 2: c_j = sum_k fk[k] e^{i iflag k.x_j}.  Execute and
+ * destroy with curig_nufft_execute / curig_nufft_destroy. */
+int curig_nufft3d_makeplan(int type, int n1, int n2, int n3, double epsilon, int iflag, double sigma,
+                           const curig_opts *opts, curig_nufft *plan);
+int curig_nufft3d_setpts(curig_nufft plan, int64_t m, const double *d_x, const double *d_y, const double *d_z);
 /* nf and dinfo[0..5] = input centre, input half width, output centre, output
  * half width, gamma, h of a type-3 plan with points */
 int curig_nufft_info3(curig_nufft plan, int *nf, double *dinfo);

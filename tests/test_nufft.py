@@ -130,3 +130,43 @@ def test_type3_random_wide_ranges(iflag, precision, eps, tol):
     ref = _direct3(x, s, c, iflag)
     assert abs(info["i_center"] - (x.max() + x.min()) / 2) < 1e-12 * 50
     assert np.linalg.norm(got - ref) <= tol * np.linalg.norm(ref)
+
+
+# ------------------------------------------------------------------ 3-D types 1 and 2
+def _direct3d(x, y, z, n_modes, iflag):
+    ks = [np.arange(n) - n // 2 for n in n_modes]
+    ph = (np.outer(x, ks[0])[:, :, None, None] + np.outer(y, ks[1])[:, None, :, None]
+          + np.outer(z, ks[2])[:, None, None, :])
+    return np.exp(1j * iflag * ph).reshape(len(x), -1)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n_modes,iflag", [((12, 10, 8), 1), ((12, 10, 8), -1), ((16, 6, 21), 1)])
+@pytest.mark.parametrize("precision,eps,tol", [("fp64", 1e-10, 1e-9), ("fp32", 1e-5, 3e-5)])
+def test_nufft_3d_types_1_and_2_match_direct(n_modes, iflag, precision, eps, tol):
+    """The reference's cunufft_setting in three dimensions (src/fourier/cuft.cu:293-305)."""
+    import torch
+    from curig_b200.nufft import Nufft
+    rng = np.random.default_rng(sum(n_modes) + 7 * iflag)
+    m = 600
+    x, y, z = (rng.uniform(-np.pi, np.pi, m) for _ in range(3))
+    z[:40] *= 2.2                                   # periodic beyond [-pi, pi) on the third axis too
+    c = rng.standard_normal(m) + 1j * rng.standard_normal(m)
+    fk = rng.standard_normal(n_modes) + 1j * rng.standard_normal(n_modes)
+    E = _direct3d(x, y, z, n_modes, iflag)
+    cdt = torch.complex128 if precision == "fp64" else torch.complex64
+    dx, dy, dz = (torch.from_numpy(a).cuda() for a in (x, y, z))
+    p1 = Nufft(1, n_modes, eps, iflag, precision=precision)
+    p1.setpts(dx, dy, dz)
+    out = torch.empty(n_modes, dtype=cdt, device="cuda")
+    p1.execute(torch.from_numpy(c).to(cdt).cuda(), out)
+    ref1 = (c @ E).reshape(n_modes)
+    assert np.linalg.norm(out.cpu().numpy() - ref1) <= tol * np.linalg.norm(ref1)
+    p2 = Nufft(2, n_modes, eps, iflag, precision=precision)
+    p2.setpts(dx, dy, dz)
+    cout = torch.empty(m, dtype=cdt, device="cuda")
+    p2.execute(cout, torch.from_numpy(fk).to(cdt).cuda())
+    ref2 = E @ fk.reshape(-1)
+    assert np.linalg.norm(cout.cpu().numpy() - ref2) <= tol * np.linalg.norm(ref2)
+    p1.close()
+    p2.close()
