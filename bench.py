@@ -558,6 +558,7 @@ def main():
             torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
             ms = float(t.item())
         info = plan.info()
+        info["error_estimate"] = plan.error_estimate()
         plan.close()
         st = {k: float(np.mean([s[k] for s in stages])) for k in stages[0]}
         return {"value": M * world / (ms / 1e3), "ms": ms, "stages": st, "info": info,
@@ -728,7 +729,7 @@ def main():
             "data": "synthetic (seeded Gaussian uv density, uniform w, complex-normal vis; generated on device)",
             "config": bench_config(a, world),
             "plan": {"window": window, "kw": info["kw"], "nf": [info["nf1"], info["nf2"], info["nf3"]],
-                     "bin_xy": info["bin_xy"],
+                     "bin_xy": info["bin_xy"], "error_estimate": info["error_estimate"],
                      "accumulate": ({1: "float atomics", 2: "one-word int32 fixed point",
                                      3: "two-word int32 fixed point (exact)"}[acc_mode] if a.precision == "fp32" else
                                     "double atomics" if acc_mode == 1 else "int64 + int32 fixed point (exact)")},

@@ -84,6 +84,8 @@ lib.curig_destroy.argtypes = [c_void_p]
 lib.curig_destroy.restype = c_int
 lib.curig_plan_info.argtypes = [c_void_p, ctypes.POINTER(c_int), ctypes.POINTER(c_double)]
 lib.curig_plan_info.restype = c_int
+lib.curig_plan_error.argtypes = [c_void_p, ctypes.POINTER(c_double)]
+lib.curig_plan_error.restype = c_int
 lib.curig_set_window.argtypes = [c_int, c_int, _P, c_double]
 lib.curig_set_window.restype = c_int
 lib.curig_clear_windows.argtypes = []

@@ -103,6 +103,13 @@ class GridderPlan:
         out.update(beta=dd[0], gamma=dd[1], h=dd[2], w_center=dd[3], w_half=dd[4], nm1_center=dd[5])
         return out
 
+    def error_estimate(self) -> dict:
+        """Estimated relative L2 error of this plan's results against the FP64
+        direct transform, with its parts (curig_plan_error)."""
+        e = (ctypes.c_double * 4)()
+        _lib.check(_lib.lib.curig_plan_error(self._h, e), "plan_error")
+        return {"total": e[0], "window": e[1], "arithmetic": e[2], "accumulation": e[3]}
+
     def close(self):
         if getattr(self, "_h", None):
             _lib.lib.curig_destroy(self._h)

@@ -108,9 +108,25 @@ def test_cfg2_against_dft(cfg2, L, eps, form):
     v = _oneshot(L, 2, prec, acc, cfg2["freq"], uvw, vis, wgt, img, eps)
     ed = _rel(d.reshape(-1)[cfg2["pix"]], cfg2["truth_d"])
     ev = _rel(v.reshape(-1)[cfg2["vidx"]], cfg2["truth_v"])
-    print(f"\n[cfg2 {NROW}x{NCHAN}] eps {eps:g} {form}: ms2dirty vs DFT {ed:.3e}, dirty2ms vs DFT {ev:.3e}")
+    est = _estimate(cfg2, prec, acc, eps)
+    print(f"\n[cfg2 {NROW}x{NCHAN}] eps {eps:g} {form}: ms2dirty vs DFT {ed:.3e}, dirty2ms vs DFT {ev:.3e}, "
+          f"stated {est:.3e}")
     # the reference's width rule reaches about 1.1-1.4 eps here; FP32 adds ~3e-7 (one word ~1.5e-6)
     assert ed <= 3 * eps and ev <= 3 * eps
+    # the error each plan states for its results (curig_plan_error) holds within a factor of 2
+    assert est / 2 <= max(ed, ev) <= 2 * est
+
+
+def _estimate(cfg2, prec, acc, eps):
+    """curig_plan_error of a device plan with the same options (ms2dirty)."""
+    import torch
+    from curig_b200.plan import GridderPlan
+    p = GridderPlan(1, NPIX, NPIX, PSX, PSX, eps, 2.0, -1, precision="fp32" if prec else "fp64", window="es",
+                    accumulate=acc)
+    p.setpts(torch.from_numpy(cfg2["uvw"]).cuda(), cfg2["freq"])
+    est = p.error_estimate()["total"]
+    p.close()
+    return est
 
 
 def _reflib_cfg2():
