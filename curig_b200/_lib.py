@@ -103,6 +103,8 @@ lib.curig_window_nparams.argtypes = []
 lib.curig_window_nparams.restype = c_int
 lib.curig_train_window.argtypes = [c_int, c_double, c_int, c_double, _P, _P]
 lib.curig_train_window.restype = c_int
+lib.curig_train_window_mc.argtypes = [c_int, c_double, c_int, c_double, ctypes.c_uint64, _P, _P]
+lib.curig_train_window_mc.restype = c_int
 lib.curig_window_loss_grad.argtypes = [c_int, c_double, _P, _P, _P]
 lib.curig_window_loss_grad.restype = c_int
 lib.curig_window_table.argtypes = [c_int, c_double, _P, c_int, _P]

@@ -38,7 +38,18 @@ struct TrainGeom {
     double lr, b1, b2, eps;
     int step;                                        // Adam step (1-based)
     int want_update;                                 // 0: loss / gradient only
+    int mc;                                          // 1: random visibility offsets per step
+    unsigned long long seed;                         // their stream
 };
+
+// Uniform [0, 1) from (seed, step, i): splitmix64 of the three, top 53 bits.
+__device__ __forceinline__ double mc_uniform(unsigned long long seed, int step, int i) {
+    unsigned long long z = seed + 0x9e3779b97f4a7c15ULL * ((unsigned long long)step * 1048576ULL + (unsigned)i + 1);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    z ^= z >> 31;
+    return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
 
 __device__ __forceinline__ double es_log(double x2, double beta) {
     // beta * (sqrt(1 - x^2) - 1) written without cancellation
@@ -65,8 +76,10 @@ __device__ __forceinline__ double mlp_forward(const float *__restrict__ P, doubl
 
 __device__ __forceinline__ double point_t(const TrainGeom &G, const double *__restrict__ qx, int p) {
     if (p < G.nf * G.W) {
+        // visibility i at fractional cell offset f: a fixed grid of offsets, or
+        // (Monte-Carlo training) offsets drawn afresh at every step
         int i = p / G.W, d = p - i * G.W;
-        double f = (i + 0.5) / G.nf;
+        double f = G.mc ? mc_uniform(G.seed, G.step, i) : (i + 0.5) / G.nf;
         return ceil(f - 0.5 * G.W) + d - f;
     }
     return qx[p - G.nf * G.W] * 0.5 * G.W;          // Gauss-Legendre node on [-W/2, W/2]
@@ -297,8 +310,8 @@ extern "C" int curig_window_loss_grad(int W, double sigma, const float *params, 
     return cudaGetLastError() == cudaSuccess ? OK : ERR_CUDA;
 }
 
-extern "C" int curig_train_window(int W, double sigma, int iters, double lr, float *params,
-                                  double *loss_hist) {
+static int train_loop(int W, double sigma, int iters, double lr, int mc, unsigned long long seed, float *params,
+                      double *loss_hist) {
     if (!params || iters < 0) return ERR_ARG;
     TrainBuffers B;
     TrainGeom G;
@@ -306,6 +319,8 @@ extern "C" int curig_train_window(int W, double sigma, int iters, double lr, flo
     if (s) return s;
     G.want_update = 1;
     G.lr = lr;
+    G.mc = mc;
+    G.seed = seed;
     for (int it = 0; it < iters; ++it) {
         G.step = it + 1;
         count_launch();
@@ -315,6 +330,16 @@ extern "C" int curig_train_window(int W, double sigma, int iters, double lr, flo
     if (cudaDeviceSynchronize() != cudaSuccess) return ERR_CUDA;
     cudaMemcpy(params, B.P, NPAR * 4, cudaMemcpyDeviceToHost);
     return cudaGetLastError() == cudaSuccess ? OK : ERR_CUDA;
+}
+
+extern "C" int curig_train_window(int W, double sigma, int iters, double lr, float *params,
+                                  double *loss_hist) {
+    return train_loop(W, sigma, iters, lr, 0, 0, params, loss_hist);
+}
+
+extern "C" int curig_train_window_mc(int W, double sigma, int iters, double lr, uint64_t seed, float *params,
+                                     double *loss_hist) {
+    return train_loop(W, sigma, iters, lr, 1, seed, params, loss_hist);
 }
 
 // Piecewise Chebyshev interpolation of the trained window (normalised to a

@@ -52,12 +52,19 @@ def loss_and_grad(W: int, params: np.ndarray, sigma: float = 2.0):
     return float(loss[0]), grad
 
 
-def train(W: int, iters: int = 3000, lr: float = 3e-3, sigma: float = 2.0, params=None, seed: int = 0):
-    """Adam on the GPU; returns (params, loss history)."""
+def train(W: int, iters: int = 3000, lr: float = 3e-3, sigma: float = 2.0, params=None, seed: int = 0,
+          mc_seed=None):
+    """Adam on the GPU; returns (params, loss history).  mc_seed: train on
+    random visibility offsets drawn afresh at every step (64 per step) from that
+    seed, instead of the fixed grid of offsets."""
     p = init_params(seed) if params is None else np.array(params, dtype=np.float32)
     hist = np.zeros(max(iters, 1))
-    _lib.check(_lib.lib.curig_train_window(W, sigma, iters, lr, p.ctypes.data, hist.ctypes.data),
-               "train_window")
+    if mc_seed is None:
+        _lib.check(_lib.lib.curig_train_window(W, sigma, iters, lr, p.ctypes.data, hist.ctypes.data),
+                   "train_window")
+    else:
+        _lib.check(_lib.lib.curig_train_window_mc(W, sigma, iters, lr, int(mc_seed), p.ctypes.data,
+                                                  hist.ctypes.data), "train_window_mc")
     return p, hist[:iters]
 
 

@@ -164,6 +164,12 @@ void curig_clear_windows(void);
  * curig_set_window.  No counterpart in the reference. */
 int curig_window_nparams(void);
 int curig_train_window(int W, double sigma, int iters, double lr, float *params, double *loss_hist);
+/* The same training on method-generated random visibilities: every step draws
+ * 64 visibility positions (fractional cell offsets, uniform, from `seed`) and
+ * takes the gradient of their gridding error against the exact DFT over the
+ * image band; iters steps see 64 * iters random visibilities. */
+int curig_train_window_mc(int W, double sigma, int iters, double lr, uint64_t seed, float *params,
+                          double *loss_hist);
 int curig_window_loss_grad(int W, double sigma, const float *params, double *loss, float *grad);
 int curig_window_table(int W, double sigma, const float *params, int degree, double *coef);
 
