@@ -636,11 +636,15 @@ def main():
     try:
         prof = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
         key = f"{dom}_{a.precision}_kw{info['kw']}"
-        if key in prof:
+        wl = prof.get("workload", {})
+        same = all(wl.get(k) == v for k, v in (("nrow", a.nrow), ("nchan", a.nchan), ("npix", a.npix),
+                                               ("fov", a.fov), ("eps", a.eps)))
+        if key in prof and same:
             traffic = prof[key]["bytes_per_launch"]
     except Exception:
         pass
-    roof = {"bound": "hbm", "kernel": f"k_{dom}_t", "achieved": round(achieved, 1), "peak": peak,
+    kname = {"spread": "k_spread_f32" if a.precision == "fp32" else "k_spread_t", "interp": "k_interp_t"}
+    roof = {"bound": "hbm", "kernel": kname[dom], "achieved": round(achieved, 1), "peak": peak,
             "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
             "traffic": traffic, "algorithmic_bytes": alg[dom], "kernel_ms": round(st[dom], 3)}
     # The spreader's binding limit is shared-memory integer atomics (FP32 tiles: two
@@ -651,7 +655,7 @@ def main():
     if a.precision == "fp32" and clk_mhz:
         taps = M * info["kw"] ** 3 / (st["spread"] / 1e3)
         tap_peak = 27.6 / 2 * torch.cuda.get_device_properties(dev).multi_processor_count * clk_mhz * 1e6
-        roof["shared_atomic_bound"] = {"kernel": "k_spread_t", "achieved_taps_per_s": taps,
+        roof["shared_atomic_bound"] = {"kernel": kname["spread"], "achieved_taps_per_s": taps,
                                        "peak_taps_per_s": tap_peak, "frac": round(taps / tap_peak, 4),
                                        "peak_basis": "27.6 int32 shared atomics / clock / SM (measured), "
                                                      "2 per tap, sampled SM clock"}
