@@ -242,6 +242,16 @@ __global__ void k_bin_scatter(long long M, const unsigned *__restrict__ keys, in
 
 // Per bin, from the scanned key counts: first sorted position, count and the
 // number of sub-problems (chunks of at most `sub` visibilities).
+// Bin of every sub-problem: bin b owns sub-problems [sub_end[b] - nsub, sub_end[b])
+// (sub_end = inclusive scan of the per-bin counts).
+__global__ void k_chunk_bins(long long nb, const int *__restrict__ sub_end, int *__restrict__ cbin) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < nb; b += stride) {
+        const int lo = b ? sub_end[b - 1] : 0, hi = sub_end[b];
+        for (int s = lo; s < hi; ++s) cbin[s] = (int)b;
+    }
+}
+
 __global__ void k_bins_from_keys(const int *__restrict__ kstart, const int *__restrict__ total, long long nb,
                                  int cbits, int sub, int *__restrict__ bin_start, int *__restrict__ bin_count,
                                  int *__restrict__ nsub, int *__restrict__ bcur) {
@@ -651,7 +661,7 @@ __device__ __forceinline__ T win_tap(const DevGeom &g, const WinTab<T> &tab, T u
 __device__ __forceinline__ void sub_range(const DevGeom &g, const int *bin_start, const int *bin_count,
                                           const int *sub_end, int s, long long &b, int &start, int &stride,
                                           int &n) {
-    b = find_bin(sub_end, g.nbins, s);
+    b = g.cbin ? g.cbin[s] : find_bin(sub_end, g.nbins, s);
     int cnt = bin_count[b];
     int nsb = (cnt + g.sub - 1) / g.sub;
     int j = s - (sub_end[b] - nsb);
@@ -969,23 +979,23 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
 // the lanes of classes that have run out (steps = the largest class / 2).
 constexpr int NCLS = 16;
 
-// Class boundaries of a chunk whose positions (start + k * stride, k < n) are
-// sorted by class: cls[q] = first k of class q, cls[NCLS] = n.  All threads
-// call it; the caller synchronises before reading cls.
-template <typename RT>
-__device__ __forceinline__ void chunk_classes(const RT *__restrict__ rec, int start, int stride, int n, int txy,
-                                              int tx, int *cls, int nthreads) {
-    auto klass = [&](int k) {
-        const int cb = cell_bits(rec[start + k * stride].w);
-        return ((((cb >> 20) & 0xfff) * txy + ((cb >> 10) & 0x3ff) * tx + (cb & 0x3ff)) & (NCLS - 1));
-    };
-    for (int k = threadIdx.x; k < n; k += nthreads) {
-        const int c = klass(k);
-        const int prev = k ? klass(k - 1) : -1;
-        for (int q = prev + 1; q <= c; ++q) cls[q] = k;
-        if (k == n - 1)
-            for (int q = c + 1; q <= NCLS; ++q) cls[q] = n;
+// Class boundaries of chunk j of bin b (positions first + j + k * nsb, k < n,
+// first = the bin's first position): cls[q] = the first k of class q,
+// cls[NCLS] = n.  The bin is in class order and g.ccls holds the end of every
+// class run, so class q starts at position ccls[16 b + q - 1] (q > 0) and the
+// chunk's elements before it number ceil((start_q - first - j) / nsb).
+// Threads 0..NCLS write one entry each; the caller synchronises before reading.
+__device__ __forceinline__ void chunk_classes(const DevGeom &g, long long b, int first, int j, int nsb, int n,
+                                              int *cls) {
+    const int q = threadIdx.x;
+    if (q > NCLS) return;
+    int v = n;
+    if (q < NCLS) {
+        const int s0 = q ? g.ccls[(b << 4) + q - 1] : first;
+        const int d = s0 - first - j;
+        v = d <= 0 ? 0 : min((d + nsb - 1) / nsb, n);
     }
+    cls[q] = v;
 }
 
 // Warp steps of the class schedule: the largest class, halved (rounded up).
@@ -1001,6 +1011,104 @@ __device__ __forceinline__ int class_steps(const int *cls, int n) {
 __device__ __forceinline__ void class_range(const int *cls, int q, int n, int &c0, int &nk) {
     c0 = min(max(cls[q], 0), n);
     nk = min(max(cls[q + 1] - c0, 0), n - c0);
+}
+
+// One chunk's warp steps of the class schedule (see k_spread_f32), for one
+// accumulation mode (MODE: 2 one-word int32, 0 two-word int32, 1 float).  A
+// lane's two words of a cell are its first word (word f) and second word
+// (word 1 - f); the amplitude components are ordered to match once per
+// visibility.  The next step's record and amplitude are loaded before this
+// step's taps, so their latency overlaps the shared-memory atomics.
+struct TapRun {
+    int start, stride, c0, nk, T, S, KZ, txy, tx, shift, warp, f;
+    float q;
+};
+
+template <int KW, int MODE>
+__device__ __forceinline__ void spread_steps(const DevGeom &g, const WinTab<float> &tab,
+                                             const float4 *__restrict__ rec, const float2 *__restrict__ cs, int *wA,
+                                             int *wB, const TapRun &t) {
+    const int steps = t.T * t.S;
+    auto fetch = [&](int u, float4 &r, float2 &c, int &part) {
+        if (u >= steps) return false;
+        const int k = u / t.S;
+        const int e = 2 * k + t.f;
+        if (e >= t.nk) return false;
+        part = u - k * t.S;
+        const int i = t.start + (t.c0 + e) * t.stride;
+        r = rec[i];
+        c = cs[i];
+        return true;
+    };
+    float4 rn = make_float4(0.f, 0.f, 0.f, 0.f);
+    float2 cn = make_float2(0.f, 0.f);
+    int pn = 0;
+    bool hn = fetch(t.warp, rn, cn, pn);
+    for (int u = t.warp; u < steps; u += TWARPS) {
+        const float4 r = rn;
+        const float2 c = cn;
+        const int part = pn;
+        const bool have = hn;
+        hn = fetch(u + TWARPS, rn, cn, pn);
+        if (!have) continue;
+        const int dz0 = part * t.KZ / t.S, dz1 = (part + 1) * t.KZ / t.S;
+        float kx[KW], ky[KW];
+#pragma unroll
+        for (int d = 0; d < KW; ++d) {
+            kx[d] = win_tap<float>(g, tab, r.x, d);
+            ky[d] = win_tap<float>(g, tab, r.y, d);
+        }
+        const int cb = cell_bits(r.w);
+        const int cell = ((cb >> 20) & 0xfff) * t.txy + ((cb >> 10) & 0x3ff) * t.tx + (cb & 0x3ff) + t.shift;
+        const int p0 = 2 * cell + t.f, d1 = 1 - 2 * t.f;     // first word; second word = first + d1
+        if constexpr (MODE == 0) {
+            const float cr = c.x * t.q, ci = c.y * t.q;
+#pragma unroll 1
+            for (int dz = dz0; dz < dz1; ++dz) {
+                const float kz = g.no_w ? 1.f : win_tap<float>(g, tab, r.z, dz);
+                const float zr = cr * kz, zi = ci * kz;
+#pragma unroll
+                for (int dy = 0; dy < KW; ++dy) {
+                    const float ar = zr * ky[dy], ai = zi * ky[dy];
+                    const int o = p0 + 2 * (dz * t.txy + dy * t.tx);
+                    int *a0 = wA + o, *a1 = a0 + d1, *b0 = wB + o, *b1 = b0 + d1;
+#pragma unroll
+                    for (int dx = 0; dx < KW; ++dx) {
+                        int hr, lr, hi, li;
+                        split_fix(ar * kx[dx], hr, lr);
+                        split_fix(ai * kx[dx], hi, li);
+                        atomicAdd(a0 + 2 * dx, t.f ? lr : hr);
+                        atomicAdd(a1 + 2 * dx, t.f ? hr : lr);
+                        atomicAdd(b0 + 2 * dx, t.f ? li : hi);
+                        atomicAdd(b1 + 2 * dx, t.f ? hi : li);
+                    }
+                }
+            }
+        } else {
+            // this lane's first word holds component f, its second word the other
+            const float c1 = (t.f ? c.y : c.x) * t.q, c2 = (t.f ? c.x : c.y) * t.q;
+#pragma unroll 1
+            for (int dz = dz0; dz < dz1; ++dz) {
+                const float kz = g.no_w ? 1.f : win_tap<float>(g, tab, r.z, dz);
+                const float z1 = c1 * kz, z2 = c2 * kz;
+#pragma unroll
+                for (int dy = 0; dy < KW; ++dy) {
+                    const float a1 = z1 * ky[dy], a2 = z2 * ky[dy];
+                    int *w1 = wA + p0 + 2 * (dz * t.txy + dy * t.tx), *w2 = w1 + d1;
+#pragma unroll
+                    for (int dx = 0; dx < KW; ++dx) {
+                        if constexpr (MODE == 2) {
+                            atomicAdd(w1 + 2 * dx, round_fix(a1, kx[dx]));
+                            atomicAdd(w2 + 2 * dx, round_fix(a2, kx[dx]));
+                        } else {
+                            atomicAdd(reinterpret_cast<float *>(w1) + 2 * dx, a1 * kx[dx]);
+                            atomicAdd(reinterpret_cast<float *>(w2) + 2 * dx, a2 * kx[dx]);
+                        }
+                    }
+                }
+            }
+        }
+    }
 }
 
 // FP32 tile accumulation (g.smode): 2 one-word int32 fixed point [re, im] per
@@ -1037,38 +1145,57 @@ k_spread_f32(DevGeom g, const int *__restrict__ bin_start, const int *__restrict
         const int shift = ox & 1, x_al = ox - shift;
         if (n < g.sparse_n) {
             // A sparse chunk: its cells receive about one tap each, so the
-            // tile would only add its fixed cost (zeroing, statistics, flush);
-            // each thread adds one visibility's taps straight to the grid
-            // with 8-byte vector reductions (FP32 sums, as the flush's).
+            // tile would only add its fixed cost (zeroing, statistics, flush).
+            // One warp per visibility adds its taps straight to the grid:
+            // the lanes hold the kx, ky, kz tap values (a shuffle apart), and
+            // item t of a plane (row dy = t / P, cell pair p = t % P of the P
+            // pairs from the even column at or below the first x) is one
+            // 16-byte vector reduction (FP32 sums, as the flush's); the
+            // periodic wrap keeps a pair whole (nf1 is even).
             // Uniform across the CTA; no shared memory is touched.
-            for (int v = threadIdx.x; v < n; v += TTHREADS) {
+            constexpr int P = (KW + 2) / 2, NT = 3 * KW;
+            const int KZ = g.no_w ? 1 : KW;
+            for (int v = warp; v < n; v += TWARPS) {
                 const int i = start + v * stride;
                 const float4 r = rec[i];
                 const float2 c = cs[i];
-                float kx[KW], ky[KW];
-#pragma unroll
-                for (int d = 0; d < KW; ++d) {
-                    kx[d] = win_tap<float>(g, tab, r.x, d);
-                    ky[d] = win_tap<float>(g, tab, r.y, d);
-                }
+                auto tapval = [&](int t) {       // t < NT: axis t / KW, tap t % KW
+                    const int ax = t / KW, d = t - ax * KW;
+                    if (ax == 2 && g.no_w) return d == 0 ? 1.f : 0.f;
+                    return win_tap<float>(g, tab, ax == 0 ? r.x : ax == 1 ? r.y : r.z, d);
+                };
+                const float tv0 = lane < NT ? tapval(lane) : 0.f;
+                float tv1 = 0.f;
+                if constexpr (NT > 32) tv1 = lane + 32 < NT ? tapval(lane + 32) : 0.f;
+                auto tap = [&](int t) {          // uniform call: every lane shuffles
+                    const float a0 = __shfl_sync(0xffffffffu, tv0, t & 31);
+                    if constexpr (NT > 32) {
+                        const float a1 = __shfl_sync(0xffffffffu, tv1, t & 31);
+                        return t < 32 ? a0 : a1;
+                    }
+                    return a0;
+                };
                 const int cb = cell_bits(r.w);
                 const int gx0 = ox + (cb & 0x3ff), gy0 = oy + ((cb >> 10) & 0x3ff), gz0 = oz + ((cb >> 20) & 0xfff);
-                int gxs[KW];
-#pragma unroll
-                for (int dx = 0; dx < KW; ++dx) gxs[dx] = wrap3(gx0 + dx, g.nf1);
-                const int KZ = g.no_w ? 1 : KW;
+                const int sh = gx0 & 1;
+                for (int t0 = 0; t0 < KW * P; t0 += 32) {
+                    const int t = t0 + lane;
+                    const int dy = min(t / P, KW - 1), pp = t - (t / P) * P;
+                    const int d0 = 2 * pp - sh, d1 = d0 + 1;
+                    const float x0 = tap(d0 >= 0 && d0 < KW ? d0 : 0);
+                    const float x1 = tap(d1 < KW ? d1 : 0);
+                    const float ky = tap(KW + dy);
+                    const float k0 = d0 >= 0 && d0 < KW ? x0 : 0.f, k1 = d1 < KW ? x1 : 0.f;
+                    const bool act = t < KW * P && d0 < KW;
+                    const int gx = wrap3(gx0 - sh + 2 * pp, g.nf1), gy = wrap3(gy0 + dy, g.nf2);
 #pragma unroll 1
-                for (int dz = 0; dz < KZ; ++dz) {
-                    const float kz = g.no_w ? 1.f : win_tap<float>(g, tab, r.z, dz);
-                    const int gz = g.zpad ? wrap3(gz0 + dz, g.nf3) : gz0 + dz;
-                    const float cr = c.x * kz, ci = c.y * kz;
-#pragma unroll
-                    for (int dy = 0; dy < KW; ++dy) {
-                        float2 *row = grid + ((long long)gz * g.nf2 + wrap3(gy0 + dy, g.nf2)) * g.nf1;
-                        const float ar = cr * ky[dy], ai = ci * ky[dy];
-#pragma unroll
-                        for (int dx = 0; dx < KW; ++dx)
-                            red_add_v2(reinterpret_cast<float *>(row + gxs[dx]), ar * kx[dx], ai * kx[dx]);
+                    for (int dz = 0; dz < KZ; ++dz) {
+                        const float kz = tap(2 * KW + dz);
+                        if (!act) continue;
+                        const int gz = g.zpad ? wrap3(gz0 + dz, g.nf3) : gz0 + dz;
+                        const float cr = c.x * kz * ky, ci = c.y * kz * ky;
+                        red_add_v4(reinterpret_cast<float *>(grid + ((long long)gz * g.nf2 + gy) * g.nf1 + gx),
+                                   cr * k0, ci * k0, cr * k1, ci * k1);
                     }
                 }
             }
@@ -1092,7 +1219,7 @@ k_spread_f32(DevGeom g, const int *__restrict__ bin_start, const int *__restrict
                     atomicAdd(colsum + ((cb >> 10) & 0x3ff) * tx + (cb & 0x3ff), mc);
                 }
             }
-        chunk_classes(rec, start, stride, n, txy, tx, cls, TTHREADS);
+        chunk_classes(g, b, bin_start[b], start - bin_start[b], stride, n, cls);
         float q = 1.f;
         double qinv = 1.0;
         if (fixed) {
@@ -1107,49 +1234,31 @@ k_spread_f32(DevGeom g, const int *__restrict__ bin_start, const int *__restrict
                 int e = m > 0.f ? ilogb(m) + 1 : 0;       // 2^(e-1) <= m < 2^e
                 k = FIX_BITS - e;
             } else {
-                // largest kw x kw box sum of the start-column sums: windows of
-                // kw rows summed in place down each column (thread per
-                // column), then windows of kw columns along each row (thread
-                // per row); the last kw values ride in registers
-                const int ty = g.ty;
-                if (threadIdx.x < tx) {
-                    const int x = threadIdx.x;
-                    float ring[KW], a = 0.f;
+                // largest kw x kw box sum of the start-column sums: sums of
+                // kw rows of each column into the first txy words of the
+                // zeroed tile, then sums of kw of those along each row (every
+                // thread a few cells); the borrowed words are zeroed again
+                float *vs = reinterpret_cast<float *>(wA);
+                for (int e = threadIdx.x; e < txy; e += TTHREADS) {
+                    const int y = e / tx, x = e - y * tx;
+                    float a = 0.f;
 #pragma unroll
-                    for (int d = 0; d < KW; ++d) ring[d] = 0.f;
-                    for (int y0 = 0; y0 < ty; y0 += KW) {
-#pragma unroll
-                        for (int d = 0; d < KW; ++d) {
-                            const int y = y0 + d;
-                            if (y < ty) {
-                                const float v = colsum[y * tx + x];
-                                a += v - ring[d];
-                                ring[d] = v;
-                                colsum[y * tx + x] = a;
-                            }
-                        }
-                    }
+                    for (int d = 0; d < KW; ++d)
+                        if (y - d >= 0) a += colsum[(y - d) * tx + x];
+                    vs[e] = a;
                 }
                 __syncthreads();
                 float bmax = 0.f;
-                if (threadIdx.x < ty) {
-                    const float *row = colsum + threadIdx.x * tx;
-                    float ring[KW], a = 0.f;
+                for (int e = threadIdx.x; e < txy; e += TTHREADS) {
+                    const int y = e / tx, x = e - y * tx;
+                    float a = 0.f;
 #pragma unroll
-                    for (int d = 0; d < KW; ++d) ring[d] = 0.f;
-                    for (int x0 = 0; x0 < tx; x0 += KW) {
-#pragma unroll
-                        for (int d = 0; d < KW; ++d) {
-                            const int x = x0 + d;
-                            if (x < tx) {
-                                const float v = row[x];
-                                a += v - ring[d];
-                                ring[d] = v;
-                                bmax = fmaxf(bmax, a);
-                            }
-                        }
-                    }
+                    for (int d = 0; d < KW; ++d)
+                        if (x - d >= 0) a += vs[y * tx + x - d];
+                    bmax = fmaxf(bmax, a);
                 }
+                __syncthreads();                          // every read of vs is done
+                for (int e = threadIdx.x; e < txy; e += TTHREADS) vs[e] = 0.f;
                 for (int o = 16; o > 0; o >>= 1) bmax = fmaxf(bmax, __shfl_xor_sync(0xffffffffu, bmax, o));
                 __syncthreads();                          // every thread has read redbuf
                 if (lane == 0) redbuf[warp] = bmax;
@@ -1168,70 +1277,16 @@ k_spread_f32(DevGeom g, const int *__restrict__ bin_start, const int *__restrict
         __syncthreads();
         // class schedule: lane k + 16 f, element 2t + f of class k at step t;
         // chunks of few steps split each visibility's w-planes into S parts
-        const int T = class_steps(cls, n);
-        int c0, nk;
-        class_range(cls, klass, n, c0, nk);
-        const int KZ = g.no_w ? 1 : KW;
-        const int S = max(1, min(KZ, TWARPS / max(T, 1)));
-        for (int u = warp; u < T * S; u += TWARPS) {
-            const int t = u / S, part = u - t * S;
-            const int e = 2 * t + f;
-            if (e >= nk) continue;
-            const int i = start + (c0 + e) * stride;
-            const int dz0 = part * KZ / S, dz1 = (part + 1) * KZ / S;
-            const float4 r = rec[i];
-            float2 c = cs[i];
-            float kx[KW], ky[KW];
-#pragma unroll
-            for (int d = 0; d < KW; ++d) {
-                kx[d] = win_tap<float>(g, tab, r.x, d);
-                ky[d] = win_tap<float>(g, tab, r.y, d);
-            }
-            const int cb = cell_bits(r.w);
-            const int cell = ((cb >> 20) & 0xfff) * txy + ((cb >> 10) & 0x3ff) * tx + (cb & 0x3ff) + shift;
-            const int p0 = 2 * cell + f, p1 = 2 * cell + 1 - f;   // this lane's first / second word
-            c.x *= q;
-            c.y *= q;
-#pragma unroll 1
-            for (int dz = dz0; dz < dz1; ++dz) {
-                const float kz = g.no_w ? 1.f : win_tap<float>(g, tab, r.z, dz);
-                const float cr = c.x * kz, ci = c.y * kz;
-                const int oz = 2 * dz * txy;
-#pragma unroll
-                for (int dy = 0; dy < KW; ++dy) {
-                    const float ar = cr * ky[dy], ai = ci * ky[dy];
-                    const int o = oz + 2 * dy * tx;
-                    if (one) {
-                        const float a0 = f ? ai : ar, a1 = f ? ar : ai;
-                        int *r0 = wA + p0 + o, *r1 = wA + p1 + o;
-#pragma unroll
-                        for (int dx = 0; dx < KW; ++dx) {
-                            atomicAdd(r0 + 2 * dx, round_fix(a0, kx[dx]));
-                            atomicAdd(r1 + 2 * dx, round_fix(a1, kx[dx]));
-                        }
-                    } else if (two) {
-                        int *a0 = wA + p0 + o, *a1 = wA + p1 + o, *b0 = wB + p0 + o, *b1 = wB + p1 + o;
-#pragma unroll
-                        for (int dx = 0; dx < KW; ++dx) {
-                            int hr, lr, hi, li;
-                            split_fix(ar * kx[dx], hr, lr);
-                            split_fix(ai * kx[dx], hi, li);
-                            atomicAdd(a0 + 2 * dx, f ? lr : hr);
-                            atomicAdd(a1 + 2 * dx, f ? hr : lr);
-                            atomicAdd(b0 + 2 * dx, f ? li : hi);
-                            atomicAdd(b1 + 2 * dx, f ? hi : li);
-                        }
-                    } else {
-                        const float a0 = f ? ai : ar, a1 = f ? ar : ai;
-                        float *r0 = reinterpret_cast<float *>(wA) + p0 + o, *r1 = reinterpret_cast<float *>(wA) + p1 + o;
-#pragma unroll
-                        for (int dx = 0; dx < KW; ++dx) {
-                            atomicAdd(r0 + 2 * dx, a0 * kx[dx]);
-                            atomicAdd(r1 + 2 * dx, a1 * kx[dx]);
-                        }
-                    }
-                }
-            }
+        {
+            const int T = class_steps(cls, n);
+            int c0, nk;
+            class_range(cls, klass, n, c0, nk);
+            const int KZ = g.no_w ? 1 : KW;
+            const int S = max(1, min(KZ, TWARPS / max(T, 1)));
+            const TapRun run{start, stride, c0, nk, T, S, KZ, txy, tx, shift, warp, f, q};
+            if (one) spread_steps<KW, 2>(g, tab, rec, cs, wA, wB, run);
+            else if (two) spread_steps<KW, 0>(g, tab, rec, cs, wA, wB, run);
+            else spread_steps<KW, 1>(g, tab, rec, cs, wA, wB, run);
         }
         __syncthreads();
         // Flush: cell pairs in memory order (one 16-byte shared load per pair
@@ -1417,7 +1472,7 @@ k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
         const bool inner = g.use_tma && x_al >= 0 && x_al + g.tpitch <= g.nf1 && oy >= 0 &&
                            oy + g.ty <= g.nf2 && (!g.zpad || (oz >= 0 && oz + g.tz <= g.nf3));
         // FP32 class schedule (the classes are read while the tile loads)
-        if constexpr (sizeof(T) == 4) chunk_classes(rec, start, stride, n, txy, tx, cls, IT);
+        if constexpr (sizeof(T) == 4) chunk_classes(g, b, bin_start[b], start - bin_start[b], stride, n, cls);
         if (inner) {
             if (threadIdx.x == 0) {
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // earlier reads of the tile
@@ -1857,6 +1912,11 @@ void launch_bins_from_keys(const int *kstart, const int *total, long long nb, in
     count_launch();
     k_bins_from_keys<<<grid_for(nb), NTHREADS, 0, st>>>(kstart, total, nb, cbits, sub, bin_start, bin_count, nsub,
                                                         bcur);
+}
+
+void launch_chunk_bins(long long nb, const int *sub_end, int *cbin, cudaStream_t st) {
+    count_launch();
+    k_chunk_bins<<<grid_for(nb), NTHREADS, 0, st>>>(nb, sub_end, cbin);
 }
 
 long long scan_temp_ints(long long n) { return (n + SCAN_B - 1) / SCAN_B + 1; }

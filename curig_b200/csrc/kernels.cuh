@@ -34,6 +34,9 @@ struct DevGeom {
     long long nbins_slab;          // bins of one row slab (nbx * nby * nbz)
     int nslab;                     // row slabs (sort key major part; 1 = none)
     int sub_lo, sub_hi;            // sub-problem window of one launch (sub_hi 0: all)
+    const int *cbin;               // bin of every sub-problem (set by the binning)
+    const int *ccls;               // FP32 tile kernels: per (bin, start-cell residue mod 16) key, the end
+                                   // of its run in bin order (the class boundaries of every bin)
     double beta, c;                // ES parameters
     int wkind, wdeg;               // window kind (0 ES, 1 polynomial), degree
     // visibility geometry

@@ -283,6 +283,7 @@ void plan_release_points(Plan *p) {
     dfree(p->d_foc, st); dfree(p->d_quad, st); dfree(p->d_psi1, st); dfree(p->d_psi2, st); dfree(p->d_psi3, st);
     dfree(p->d_wcoef, st); dfree(p->d_bin_count, st); dfree(p->d_bin_start, st);
     dfree(p->d_nsub, st); dfree(p->d_sub_end, st); dfree(p->d_keys_in, st); dfree(p->d_kcount, st);
+    dfree(p->d_cbin, st); p->dg.cbin = nullptr; p->dg.ccls = nullptr;
     dfree(p->d_idx, st); dfree(p->d_err, st); dfree(p->d_keys, st); dfree(p->d_scan, st);
     dfree(p->d_tmp, st); dfree(p->d_bcur, st);
     dfree(p->d_rec, st); dfree(p->d_ph, st); dfree(p->d_cs, st); dfree(p->d_grid, st);
@@ -659,10 +660,24 @@ retry_tiles:
     else
         launch_records<double>(g, du, dv, dw, p->d_foc, p->d_tmp, M, p->d_kcount, p->d_rec, p->d_ph, p->d_idx, st);
     dfree(p->d_keys_in, st);
-    dfree(p->d_kcount, st);
     dfree(p->d_scan, st);
     dfree(p->d_tmp, st);
     dfree(p->d_bcur, st);
+    // the key cursors now hold the end of every (bin, residue) run: the class
+    // boundaries of the FP32 tile kernels; every sub-problem's bin
+    if (f32tile) {
+        g.ccls = p->d_kcount;
+    } else {
+        dfree(p->d_kcount, st);
+        g.ccls = nullptr;
+    }
+    const int nsubs = p->slab_sub_end.empty() ? 0 : p->slab_sub_end.back();
+    g.cbin = nullptr;
+    if (nsubs > 0) {
+        CU_TRY(dalloc(&p->d_cbin, (size_t)nsubs * sizeof(int), st));
+        launch_chunk_bins(nb, p->d_sub_end, p->d_cbin, st);
+        g.cbin = p->d_cbin;
+    }
     // TMA descriptor of the grid for the interpolator's interior tile boxes
     // ({tpitch, ty, tz} cells in 8-byte elements: one per FP32 cell, two per
     // FP64 cell; box edges <= 256 elements, x starts 16-byte aligned)

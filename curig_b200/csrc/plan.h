@@ -68,7 +68,9 @@ struct Plan {
     double *d_psi3 = nullptr;          // generic 3-D NUFFT: window transform on the third axis [nf3/2+1]
     int *d_bin_count = nullptr, *d_bin_start = nullptr, *d_nsub = nullptr, *d_sub_end = nullptr;
     unsigned *d_keys_in = nullptr;                      // sort key per visibility (input order)
-    int *d_kcount = nullptr;                            // count / first position per key value
+    int *d_kcount = nullptr;                            // count / first position per key value; after the
+                                                        // records (FP32 tiles): end of every key's run
+    int *d_cbin = nullptr;                              // bin of every sub-problem
     int *d_bcur = nullptr, *d_tmp = nullptr;            // bin cursors; input index per position, bin order
     int *d_idx = nullptr;                               // input index per sorted position (bin order)
     int *d_err = nullptr;
@@ -139,11 +141,13 @@ int plan_execute_slabs(Plan *p, int type, void *d_vis, const void *d_wgt, void *
                        const cudaEvent_t *ready, const cudaEvent_t *done, int nev, bool prologue_done = false);
 constexpr int MAX_SLABS = 8;
 // FP32 spreader: chunks with fewer visibilities spread straight to the grid
-// (each cell of such a tile receives about one tap).  FP64 keeps the tile for
+// (each cell of such a tile receives about one tap; the 4096^2 configuration
+// with 1.6e8 visibilities measured the spreader at 19.5 ms for 64-192 and
+// 20.7 ms for 384).  FP64 keeps the tile for
 // every chunk: its scattered double atomics measured slower than the flush's
 // row-contiguous ones (one channel of the 4096^2 configuration: 203 against
 // 85 ms per ms2dirty call).
-constexpr int DEFAULT_SPARSE_N = 192;
+constexpr int DEFAULT_SPARSE_N = 128;
 // first row of slab k of nslab over nrow rows (k = nslab gives nrow)
 inline long long slab_first_row(long long nrow, int nslab, int k) {
     return ((long long)k * nrow + nslab - 1) / nslab;
@@ -158,6 +162,7 @@ void launch_wrange(const double *w, int stride, long long nrow, unsigned long lo
 void launch_bin_count(const DevGeom &g, const double *u, const double *v, const double *w, const double *foc,
                       unsigned *keys, int *count, int *err, cudaStream_t st);
 void launch_bin_scatter(long long M, const unsigned *keys, int cbits, int *bcur, int *tmp, cudaStream_t st);
+void launch_chunk_bins(long long nb, const int *sub_end, int *cbin, cudaStream_t st);
 void launch_bins_from_keys(const int *kstart, const int *total, long long nb, int cbits, int sub, int *bin_start,
                            int *bin_count, int *nsub, int *bcur, cudaStream_t st);
 // Prefix sum of n int32 values (exclusive or inclusive); tmp holds

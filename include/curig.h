@@ -86,7 +86,7 @@ typedef struct curig_opts {
                              2 from 64 MiB, else 1).  Plans ignore it. */
     int sparse;           /* FP32 tile spreader: a chunk of fewer visibilities than this adds its
                              taps straight to the grid instead of through a shared-memory tile
-                             (0: automatic, 192; negative: always the tile; FP64 ignores it) */
+                             (0: automatic, 128; negative: always the tile; FP64 ignores it) */
 } curig_opts;
 
 void curig_default_opts(curig_opts *opts);
