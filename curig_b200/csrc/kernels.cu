@@ -755,6 +755,52 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
         const int ox = (int)bxi * g.bx - g.hkw, oy = (int)byi * g.by - g.hkw;
         const int oz = g.zpad ? (int)bzi * g.bz - g.hkw : 0;
         const int shift = ox & 1, x_al = ox - shift;
+        if (sizeof(T) == 8 && n < g.sparse_n) {
+            // A sparse FP64 chunk: one warp per visibility adds its taps
+            // straight to the grid with double atomics (the lanes hold the kx,
+            // ky, kz tap values, a shuffle apart; item t of the kz x ky x kx
+            // block is one cell, so a warp instruction covers whole rows).
+            // Uniform across the CTA; no shared memory is touched.
+            constexpr int NT = 3 * KW;
+            const int KZ = g.no_w ? 1 : KW, items = KZ * KW * KW;
+            for (int v = warp; v < n; v += TWARPS) {
+                const int i = start + v * stride;
+                const R<T> r = rec[i];
+                const C<T> c = cs[i];
+                auto tapval = [&](int t) {        // t < NT: axis t / KW, tap t % KW
+                    const int ax = t / KW, d = t - ax * KW;
+                    if (ax == 2 && g.no_w) return d == 0 ? (T)1 : (T)0;
+                    return win_tap<T>(g, tab, ax == 0 ? r.x : ax == 1 ? r.y : r.z, d);
+                };
+                const T tv0 = lane < NT ? tapval(lane) : (T)0;
+                T tv1 = 0;
+                if constexpr (NT > 32) tv1 = lane + 32 < NT ? tapval(lane + 32) : (T)0;
+                auto tap = [&](int t) {           // uniform call: every lane shuffles
+                    const T a0 = __shfl_sync(0xffffffffu, tv0, t & 31);
+                    if constexpr (NT > 32) {
+                        const T a1 = __shfl_sync(0xffffffffu, tv1, t & 31);
+                        return t < 32 ? a0 : a1;
+                    }
+                    return a0;
+                };
+                const int cb = cell_bits(r.w);
+                const int gx0 = ox + (cb & 0x3ff), gy0 = oy + ((cb >> 10) & 0x3ff), gz0 = oz + ((cb >> 20) & 0xfff);
+                for (int t0 = 0; t0 < items; t0 += 32) {
+                    const int t = t0 + lane, tt = min(t, items - 1);
+                    const int dz = tt / (KW * KW), rem = tt - dz * (KW * KW), dy = rem / KW, dx = rem - dy * KW;
+                    const T kx = tap(dx), ky = tap(KW + dy), kz = tap(2 * KW + dz);
+                    if (t < items) {
+                        const int gz = g.zpad ? wrap3(gz0 + dz, g.nf3) : gz0 + dz;
+                        C<T> *cell = grid + ((long long)gz * g.nf2 + wrap3(gy0 + dy, g.nf2)) * g.nf1 +
+                                     wrap3(gx0 + dx, g.nf1);
+                        const T ar = c.x * kz * ky, ai = c.y * kz * ky;
+                        atomicAdd(&cell->x, ar * kx);
+                        atomicAdd(&cell->y, ai * kx);
+                    }
+                }
+            }
+            continue;
+        }
         float4 *tv = reinterpret_cast<float4 *>(smem);
         for (int e = threadIdx.x; e < nvec; e += TTHREADS) tv[e] = make_float4(0.f, 0.f, 0.f, 0.f);
         if (!fix && !fix64)                              // (ntile is even: 24-byte cells fill whole float4s)
@@ -1207,16 +1253,29 @@ k_spread_f32(DevGeom g, const int *__restrict__ bin_start, const int *__restrict
             for (int e = threadIdx.x; e < txy; e += TTHREADS) colsum[e] = 0.f;
         __syncthreads();
         // chunk statistics: largest component of c, one word: start-column sums
+        // (four elements per thread in flight: the loads are issued first)
         float m = 0.f;
         if (fixed)
-            for (int k = threadIdx.x; k < n; k += TTHREADS) {
-                const int i = start + k * stride;
-                const float2 c = cs[i];
-                const float mc = fmaxf(fabsf(c.x), fabsf(c.y));
-                m = fmaxf(m, mc);
-                if (one) {
-                    const int cb = cell_bits(rec[i].w);
-                    atomicAdd(colsum + ((cb >> 10) & 0x3ff) * tx + (cb & 0x3ff), mc);
+            for (int k0 = threadIdx.x; k0 < n; k0 += 4 * TTHREADS) {
+                float2 cc[4];
+                int cb[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int k = k0 + u * TTHREADS;
+                    cc[u] = make_float2(0.f, 0.f);
+                    cb[u] = 0;
+                    if (k < n) {
+                        const int i = start + k * stride;
+                        cc[u] = cs[i];
+                        if (one) cb[u] = cell_bits(rec[i].w);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const float mc = fmaxf(fabsf(cc[u].x), fabsf(cc[u].y));
+                    m = fmaxf(m, mc);
+                    if (one && k0 + u * TTHREADS < n)
+                        atomicAdd(colsum + ((cb[u] >> 10) & 0x3ff) * tx + (cb[u] & 0x3ff), mc);
                 }
             }
         chunk_classes(g, b, bin_start[b], start - bin_start[b], stride, n, cls);

@@ -549,7 +549,8 @@ retry_tiles:
     g.bx = tg.bx; g.by = tg.by; g.bz = tg.bz; g.nbx = tg.nbx; g.nby = tg.nby; g.nbz = tg.nbz;
     g.ibx = 1.0 / tg.bx; g.iby = 1.0 / tg.by; g.ibz = tg.bz > 0 ? 1.0 / tg.bz : 0.0;
     g.tx = tg.tx; g.ty = tg.ty; g.tz = tg.tz; g.zpad = tg.zpad; g.sub = tg.sub;
-    g.sparse_n = esize != 4 || p->opt.sparse < 0 ? 0 : p->opt.sparse > 0 ? p->opt.sparse : DEFAULT_SPARSE_N;
+    g.sparse_n = p->opt.sparse < 0 ? 0 : p->opt.sparse > 0 ? p->opt.sparse
+                 : esize == 4 ? DEFAULT_SPARSE_N : DEFAULT_SPARSE_N64;
     g.tpitch = (tg.tx + 2) & ~1;
     g.use_tma = 0;                          // set once the grid's TMA descriptor exists
     g.tma_polls = g_tma_polls.load();

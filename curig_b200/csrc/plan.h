@@ -140,14 +140,14 @@ int plan_execute(Plan *p, void *d_vis, const void *d_wgt, void *d_dirty, int typ
 int plan_execute_slabs(Plan *p, int type, void *d_vis, const void *d_wgt, void *d_dirty,
                        const cudaEvent_t *ready, const cudaEvent_t *done, int nev, bool prologue_done = false);
 constexpr int MAX_SLABS = 8;
-// FP32 spreader: chunks with fewer visibilities spread straight to the grid
-// (each cell of such a tile receives about one tap; the 4096^2 configuration
-// with 1.6e8 visibilities measured the spreader at 19.5 ms for 64-192 and
-// 20.7 ms for 384).  FP64 keeps the tile for
-// every chunk: its scattered double atomics measured slower than the flush's
-// row-contiguous ones (one channel of the 4096^2 configuration: 203 against
-// 85 ms per ms2dirty call).
+// Tile spreaders: chunks with fewer visibilities spread straight to the grid
+// (each cell of such a tile receives about one tap), one warp per visibility.
+// Measured thresholds at 4096^2 (ms of the spreader): FP32 with 1.6e8
+// visibilities 19.5 for 64-192, 20.7 for 384; FP64 with one channel (1e7
+// visibilities, the reference ABI's call) 33.9 with the tile only, 21.0 / 19.5
+// / 17.7 / 20.7 for 32 / 64 / 128 / 256.
 constexpr int DEFAULT_SPARSE_N = 128;
+constexpr int DEFAULT_SPARSE_N64 = 128;
 // first row of slab k of nslab over nrow rows (k = nslab gives nrow)
 inline long long slab_first_row(long long nrow, int nslab, int k) {
     return ((long long)k * nrow + nslab - 1) / nslab;

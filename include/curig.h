@@ -84,9 +84,9 @@ typedef struct curig_opts {
                              dirty2ms downloads slab k while slab k+1 is interpolated);
                              0 = automatic (3 from 1 GiB of visibilities and weights,
                              2 from 64 MiB, else 1).  Plans ignore it. */
-    int sparse;           /* FP32 tile spreader: a chunk of fewer visibilities than this adds its
+    int sparse;           /* tile spreaders: a chunk of fewer visibilities than this adds its
                              taps straight to the grid instead of through a shared-memory tile
-                             (0: automatic, 128; negative: always the tile; FP64 ignores it) */
+                             (0: automatic, 128 in FP32 and FP64; negative: always the tile) */
 } curig_opts;
 
 void curig_default_opts(curig_opts *opts);

@@ -121,13 +121,13 @@ def test_disk2000_256_against_reference_truth(C):
 
 # ---------------------------------------------------------------- multi-channel, FP32, plan API
 def _plan_run(kind, nx, ny, psx, psy, eps, sign, uvw, freq, vis=None, wgt=None, dirty=None,
-              precision="fp64", window="es", accumulate=0, sub=0):
+              precision="fp64", window="es", accumulate=0, sub=0, sparse=0):
     import torch
     from curig_b200 import GridderPlan
     dt = torch.complex128 if precision == "fp64" else torch.complex64
     rt = torch.float64 if precision == "fp64" else torch.float32
     p = GridderPlan(kind, nx, ny, psx, psy, eps, 2.0, sign, precision=precision, window=window,
-                    accumulate=accumulate, sub=sub)
+                    accumulate=accumulate, sub=sub, sparse=sparse)
     d_uvw = torch.from_numpy(np.ascontiguousarray(uvw)).cuda()
     p.setpts(d_uvw, freq)
     nrow, nchan = uvw.shape[0], len(freq)
@@ -149,14 +149,17 @@ def _plan_run(kind, nx, ny, psx, psy, eps, sign, uvw, freq, vis=None, wgt=None, 
     return out, info
 
 
+# sparse: 0 the default split (chunks below 128 visibilities straight to the
+# grid, one warp per visibility), -1 every chunk through a tile, 1 << 30 no tile
+@pytest.mark.parametrize("sparse", [0, -1, 1 << 30])
 @pytest.mark.parametrize("accumulate", [0, 1, 2, 3])
 @pytest.mark.parametrize("precision,eps,tol", [("fp64", 1e-9, 1e-8), ("fp64", 1e-5, 1e-4),
                                                ("fp32", 1e-5, 2e-5), ("fp32", 1e-4, 2e-4)])
-def test_multichannel_plan_vs_dft(C, precision, eps, tol, accumulate):
+def test_multichannel_plan_vs_dft(C, precision, eps, tol, accumulate, sparse):
     freq, uvw, ms, wgt = disk_inputs(3000, 4, 128, 2.0, f0=0.9e9, fmax=1.1e9, max_pix=60, wmax=300)
     psx = psy = 2.0 * np.pi / 180 / 128
     d, info = _plan_run(1, 128, 128, psx, psy, eps, -1, uvw, freq, vis=ms, wgt=wgt, precision=precision,
-                        accumulate=accumulate)
+                        accumulate=accumulate, sparse=sparse)
     pix = np.random.default_rng(1).integers(0, 128 * 128, 600)
     ref = dft.ms2dirty_dft(uvw, freq, ms, wgt, 128, 128, psx, psy, -1, pix=pix)
     assert l2err(ref, d.ravel()[pix]) < tol
