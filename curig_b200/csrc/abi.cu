@@ -59,11 +59,12 @@ extern "C" int curig_release_memory(void) {
 // One call with host buffers: allocate, copy in, plan, execute, copy out, free
 // (the reference's ms2dirty_exec / dirty2ms_exec life cycle, cugridder.cu:330-582),
 // pipelined over row slabs.  A copy stream uploads uvw first (set points needs
-// it), then for dirty2ms the image, then each slab's visibilities / weights
-// with an event per slab; the plan's stream spreads slab k as soon as it is on
-// the device (ms2dirty), or interpolates slab k and a download stream returns
-// its rows while slab k+1 is interpolated (dirty2ms).  With pinned host
-// buffers the transfers in both directions overlap the kernels.
+// it, and the w range it yields sizes the planes that the image's correction
+// fills), then for dirty2ms the image, then each slab's visibilities /
+// weights with an event per slab; the plan's stream spreads slab k as soon as
+// it is on the device (ms2dirty), or interpolates slab k and a download stream
+// returns its rows while slab k+1 is interpolated (dirty2ms).  With pinned
+// host buffers the transfers in both directions overlap the kernels.
 static int oneshot(int type, long long nrow, int nchan, int nx, int ny, double psx, double psy,
                    const double *freq, const double *uvw, void *vis, const void *wgt, void *dirty,
                    double eps, double sigma, int sign, const curig_opts *opts) {
@@ -80,11 +81,15 @@ static int oneshot(int type, long long nrow, int nchan, int nx, int ny, double p
     const size_t rs = opt.precision ? 4 : 8, cs = 2 * rs;
     const size_t M = (size_t)nrow * nchan, npix = (size_t)nx * ny;
     const size_t row_bytes = (size_t)nchan * (cs + (wgt ? rs : 0));
-    // automatic: 3 slabs from 1 GiB of visibilities + weights, 2 from 64 MiB
-    // (at 1.9 GB, 1 / 2 / 3 / 4 slabs: 142 / 124 / 122 / 131 ms per ms2dirty + dirty2ms)
+    // automatic: 3 slabs from 1 GiB of visibilities + weights, 2 from 384 MiB.
+    // Slabs overlap the transfers with the tile kernels but split every bin
+    // (more chunks and tile loads).  ms2dirty + dirty2ms at 4096^2 with 1e7
+    // rows, 1 / 2 / 3 slabs: FP32 16 channels (1.9 GB) 137.0 / 119.5 / 113.5 ms,
+    // FP32 4 channels (480 MB) 64.0 / 61.7 / 64.9 ms, FP64 1 channel (240 MB,
+    // the reference ABI's call) 93.5 / 106.5 / 116.5 ms.
     const size_t up_bytes = (size_t)nrow * row_bytes;
     int nslab = opts && opts->slabs > 0 ? opts->slabs
-                                        : up_bytes >= ((size_t)1 << 30) ? 3 : up_bytes >= ((size_t)64 << 20) ? 2 : 1;
+                                        : up_bytes >= ((size_t)1 << 30) ? 3 : up_bytes >= ((size_t)384 << 20) ? 2 : 1;
     if (nslab > nrow) nslab = (int)nrow;
     opt.slabs = nslab;
     double *d_uvw = nullptr;

@@ -83,7 +83,7 @@ typedef struct curig_opts {
                              (1 .. 8; ms2dirty spreads slab k while slab k+1 is uploaded,
                              dirty2ms downloads slab k while slab k+1 is interpolated);
                              0 = automatic (3 from 1 GiB of visibilities and weights,
-                             2 from 64 MiB, else 1).  Plans ignore it. */
+                             2 from 384 MiB, else 1).  Plans ignore it. */
     int sparse;           /* tile spreaders: a chunk of fewer visibilities than this adds its
                              taps straight to the grid instead of through a shared-memory tile
                              (0: automatic, 128 in FP32 and FP64; negative: always the tile) */
