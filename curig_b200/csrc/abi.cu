@@ -145,10 +145,9 @@ static int oneshot(int type, long long nrow, int nchan, int nx, int ny, double p
         } else if (s == OK) {
             // dirty2ms: the grid preparation (plan's stream) runs while a second
             // stream bins the visibilities; neither depends on the other
-            if (!chk(cudaEventRecord(ev_geom, st)) || !chk(cudaStreamWaitEvent(bn, ev_geom, 0)) ||
-                !chk(cudaStreamWaitEvent(st, ev_img, 0)))
+            if (!chk(cudaEventRecord(ev_geom, st)) || !chk(cudaStreamWaitEvent(bn, ev_geom, 0)))
                 s = ERR_CUDA;
-            if (s == OK) s = plan_d2m_prologue(p, d_dirty);
+            if (s == OK) s = plan_d2m_prologue(p, d_dirty, ev_img);
             if (s == OK) s = plan_setpts_bin(p, bn);
             if (s == OK && (!chk(cudaEventRecord(ev_bin, bn)) || !chk(cudaStreamWaitEvent(st, ev_bin, 0))))
                 s = ERR_CUDA;

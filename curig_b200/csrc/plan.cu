@@ -912,9 +912,10 @@ int plan_execute_slabs(Plan *p, int type, void *d_vis, const void *d_wgt, void *
 }
 
 template <typename T>
-static int d2m_prologue_t(Plan *p, const void *d_dirty) {
+static int d2m_prologue_t(Plan *p, const void *d_dirty, cudaEvent_t image_ready) {
     const GridParams &gp = p->gp;
-    launch_zero_tpad<T>(p->nx, p->ny, gp.nf2, gp.nf3, p->d_tgrid, p->st);
+    launch_zero_tpad<T>(p->nx, p->ny, gp.nf2, gp.nf3, p->d_tgrid, p->st);   // needs no image
+    if (image_ready) CU_TRY(cudaStreamWaitEvent(p->st, image_ready, 0));
     launch_correct_d2m<T>(p->dc, d_dirty, p->d_tgrid, p->st);
     int s = plane_fft<T>(p, CUFFT_FORWARD, false);
     if (s) return s;
@@ -922,9 +923,10 @@ static int d2m_prologue_t(Plan *p, const void *d_dirty) {
     return OK;
 }
 
-int plan_d2m_prologue(Plan *p, const void *d_dirty) {
+int plan_d2m_prologue(Plan *p, const void *d_dirty, cudaEvent_t image_ready) {
     if (!p || !p->geom_ready || !d_dirty) return ERR_ARG;
-    return p->opt.precision ? d2m_prologue_t<float>(p, d_dirty) : d2m_prologue_t<double>(p, d_dirty);
+    return p->opt.precision ? d2m_prologue_t<float>(p, d_dirty, image_ready)
+                            : d2m_prologue_t<double>(p, d_dirty, image_ready);
 }
 
 // Error flags raised by kernels of earlier executes (an interpolator tile load

@@ -124,8 +124,9 @@ int plan_setpts_geometry(Plan *p, long long nrow, int nchan, const double *du, c
                          const double *dw, int stride, const double *h_freq);
 int plan_setpts_bin(Plan *p, cudaStream_t st);
 // dirty2ms grid preparation (corrections, per-plane screens, transforms) on
-// the plan's stream; needs only the geometry stage.
-int plan_d2m_prologue(Plan *p, const void *d_dirty);
+// the plan's stream; needs only the geometry stage.  With image_ready, the
+// stream waits for it after clearing the buffer rows the image does not fill.
+int plan_d2m_prologue(Plan *p, const void *d_dirty, cudaEvent_t image_ready = nullptr);
 int plan_execute(Plan *p, void *d_vis, const void *d_wgt, void *d_dirty, int type = 0);
 // The same transform run slab by slab (the one-shot copy / compute pipeline).
 // ms2dirty: before slab k the plan's stream waits for ready[k] (the upload of
