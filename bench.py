@@ -59,7 +59,7 @@ def args_():
                     help="skip timing the reference's own GPU library (oracle/_ref) beside this one")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--accumulate", type=int, default=0, help="tile accumulation: 0 automatic, 1 float atomics, 2 one-word int32 fixed point, 3 two-word (exact); FP64: 1 double atomics, else exact int64 + int32")
+    ap.add_argument("--accumulate", type=int, default=0, help="tile accumulation: 0 automatic, 1 float atomics, 2 one-word int32 fixed point, 3 two-word (exact); FP64: 1 double atomics, else exact three-word int32")
     ap.add_argument("--bin", type=int, default=0, help="bin edge in cells (0 automatic)")
     ap.add_argument("--smem", type=int, default=0, help="shared-memory budget per tile CTA (bytes)")
     ap.add_argument("--sub", type=int, default=0, help="visibilities per tile chunk (0 automatic)")
@@ -595,7 +595,7 @@ def main():
         r = time_arm("es", a.eps, max(2, a.steps // 2), 2, precision="fp64", accumulate=0)
         arms["fp64_es_reference_rule"] = {"value": r["value"], "ms_per_step": round(r["ms"], 3),
                                           "kw": r["info"]["kw"], "window": "es",
-                                          "accumulate": "int64 + int32 fixed point (exact)"}
+                                          "accumulate": "three-word int32 fixed point (exact)"}
         torch.cuda.empty_cache()
 
     # batch of 8 independent problems through the autograd pair (single process)
@@ -736,7 +736,7 @@ def main():
                      "bin_xy": info["bin_xy"], "error_estimate": info["error_estimate"],
                      "accumulate": ({1: "float atomics", 2: "one-word int32 fixed point",
                                      3: "two-word int32 fixed point (exact)"}[acc_mode] if a.precision == "fp32" else
-                                    "double atomics" if acc_mode == 1 else "int64 + int32 fixed point (exact)")},
+                                    "double atomics" if acc_mode == 1 else "three-word int32 fixed point (exact)")},
             "reference_gpu": refgpu,
             "e2e": e2e, "gpu_launches": int(head["launches"]), "clocks": head["clocks"],
             "roofline": roof, "cpu_baseline": cpu, "arms": arms, "batch8_autograd": batch8,

@@ -99,7 +99,7 @@ struct TileGeom {
     int nbx = 0, nby = 0, nbz = 0;     // number of bins per axis
     int zpad = 1;                      // 1: tile z = bz + kw with offset; 0: tile z = nf3
     int sub = 1024;                    // visibilities per sub-problem
-    int fix = 0;                       // spreader tile: 1 two-word, 2 one-word int32 fixed point, 3 int64 + int32 (FP64)
+    int fix = 0;                       // spreader tile: 1 two-word, 2 one-word int32 fixed point, 3 three-word int32 (FP64)
     size_t smem_bytes = 0;
     long long nbins() const { return (long long)nbx * nby * nbz; }
 };

@@ -704,21 +704,28 @@ __device__ __forceinline__ int round_fix(float a, float k) {
     return __float_as_int(fmaf(a, k, 12582912.0f)) - 0x4B400000;
 }
 
-// FP64 tiles (shared-memory double atomics are compare-and-swap loops): each
-// scaled term x is split exactly as h * 2^18 + l, h rounded to an integer by
-// one FMA against 1.5 * 2^52, l = x - h 2^18 (exact) rounded to an integer
-// (|l| <= 2^17); h goes to an int64 plane (two's complement in the unsigned
-// add), l to an int32 plane.  The chunk scale q = 2^k takes the largest k with
-// max|c| wmax3 q <= 2^68, so |h| <= 2^50 and, with at most 4096 terms per cell
-// (sub <= 4096), the high sums stay below 2^62 and the low sums below 2^29:
-// cell sums are exact and order-independent, and a term's rounding is at most
-// 2^-68 of max|c| wmax3, below the FP64 rounding of the product itself.
-__device__ __forceinline__ void split_fix64(double x, unsigned long long &h, int &l) {
+// FP64 tiles (shared-memory double atomics are compare-and-swap loops, and
+// 64-bit integer atomics run at about a quarter of the 32-bit rate on this
+// part): each scaled term x is split exactly as h * 2^36 + m * 2^18 + l, h
+// and m rounded to integers by FMAs against 1.5 * 2^52 (the remainders
+// x - h 2^36 and x - h 2^36 - m 2^18 are exact), l the last remainder rounded
+// to an integer; h, m and l go to three int32 planes.  The chunk scale
+// q = 2^k takes the largest k with max|c| wmax3 q <= 2^54, so |h| <= 2^18 and
+// |m|, |l| <= 2^17 and, with at most 4096 terms per cell (sub <= 4096), no
+// plane's sum leaves int32: cell sums are exact and order-independent, and a
+// term's rounding is at most 2^-55 of max|c| wmax3, below the FP64 rounding of
+// the product itself (2^-53 of the product).
+constexpr int FIX64_BITS = 54;
+__device__ __forceinline__ void split_fix3(double x, int &h, int &m, int &l) {
     const double M = 6755399441055744.0;                  // 1.5 * 2^52
-    const double t = fma(x, 3.814697265625e-06, M);       // x * 2^-18, rounded to an integer
-    h = (unsigned long long)(__double_as_longlong(t) - 0x4338000000000000LL);
-    const double lf = fma(t - M, -262144.0, x);           // x - h * 2^18, exact
-    l = (int)(__double_as_longlong(lf + M) - 0x4338000000000000LL);
+    const long long MB = 0x4338000000000000LL;            // its bit pattern
+    const double th = fma(x, 0x1p-36, M);                 // x * 2^-36, rounded to an integer
+    h = (int)(__double_as_longlong(th) - MB);
+    const double r1 = fma(th - M, -0x1p36, x);            // x - h * 2^36, exact
+    const double tm = fma(r1, 0x1p-18, M);                // r1 * 2^-18, rounded to an integer
+    m = (int)(__double_as_longlong(tm) - MB);
+    const double r2 = fma(tm - M, -0x1p18, r1);           // r1 - m * 2^18, exact
+    l = (int)(__double_as_longlong(r2 + M) - MB);
 }
 
 template <typename T, int KW>
@@ -731,7 +738,7 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
     const int ntile = g.tpitch * g.ty * g.tz;            // tile [tz][ty][tpitch], columns >= tx stay 0
     const bool fix = sizeof(T) == 4 && g.smode == 0;    // FP32: exact two-word int32 fixed point
     const bool fix1 = sizeof(T) == 4 && g.smode == 2;   // FP32: one-word int32 fixed point
-    const bool fix64 = sizeof(T) == 8 && g.smode != 1;  // FP64: int64 + int32 fixed point (exact)
+    const bool fix64 = sizeof(T) == 8 && g.smode != 1;  // FP64: three-word int32 fixed point (exact)
     const int csz = fix ? 16 : fix64 ? 24 : (int)sizeof(C<T>);   // bytes per complex cell
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int total = g.sub_hi ? g.sub_hi : sub_end[g.nbins - 1];   // sub-problem window [sub_lo, total)
@@ -742,8 +749,9 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
     int *fre = fhr, *fim = flr;                        // one-word planes: re, im
     float *colsum = reinterpret_cast<float *>(fhr + 2 * ntile);   // one-word: per start column sum|c|
     // FP64 planes: re-high, im-high (int64, units of 2^18), re-low, im-low (int32)
-    unsigned long long *gre = reinterpret_cast<unsigned long long *>(smem), *gim = gre + ntile;
-    int *lre = reinterpret_cast<int *>(gim + ntile), *lim = lre + ntile;
+    // FP64 planes: re high / mid / low, im high / mid / low (int32 each)
+    int *hre = reinterpret_cast<int *>(smem), *mre = hre + ntile, *lre = mre + ntile;
+    int *him = lre + ntile, *mim = him + ntile, *lim = mim + ntile;
     for (int s = g.sub_lo + blockIdx.x; s < total; s += gridDim.x) {
         long long b;
         int start, stride, n;
@@ -837,7 +845,7 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
                 int e = m > (T)0 ? ilogb(m) + 1 : 0;       // 2^(e-1) <= m < 2^e
                 k = FIX_BITS - e;
             } else if (fix64) {
-                k = 68 - (m > (T)0 ? ilogb(m * g.wmax3) + 1 : 0);
+                k = FIX64_BITS - (m > (T)0 ? ilogb(m * g.wmax3) + 1 : 0);
             } else {
                 // largest kw x kw box sum of the start-column histogram
                 float bmax = 0.f;
@@ -927,13 +935,14 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
                         if (fix64) {
 #pragma unroll
                             for (int dx = 0; dx < KW; ++dx) {
-                                unsigned long long h;
-                                int l;
-                                split_fix64(ar * kx[dx], h, l);
-                                atomicAdd(gre + prow + dx, h);
+                                int h, mm, l;
+                                split_fix3(ar * kx[dx], h, mm, l);
+                                atomicAdd(hre + prow + dx, h);
+                                atomicAdd(mre + prow + dx, mm);
                                 atomicAdd(lre + prow + dx, l);
-                                split_fix64(ai * kx[dx], h, l);
-                                atomicAdd(gim + prow + dx, h);
+                                split_fix3(ai * kx[dx], h, mm, l);
+                                atomicAdd(him + prow + dx, h);
+                                atomicAdd(mim + prow + dx, mm);
                                 atomicAdd(lim + prow + dx, l);
                             }
                             continue;
@@ -972,8 +981,9 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
                     v.x = (T)(__int2float_rn(fre[e]) * qf);
                     v.y = (T)(__int2float_rn(fim[e]) * qf);
                 } else if (fix64) {
-                    v.x = (T)fma((double)(long long)gre[e], qinv * 262144.0, (double)lre[e] * qinv);
-                    v.y = (T)fma((double)(long long)gim[e], qinv * 262144.0, (double)lim[e] * qinv);
+                    const double q36 = qinv * 0x1p36, q18 = qinv * 0x1p18;
+                    v.x = (T)fma((double)hre[e], q36, fma((double)mre[e], q18, (double)lre[e] * qinv));
+                    v.y = (T)fma((double)him[e], q36, fma((double)mim[e], q18, (double)lim[e] * qinv));
                 } else {
                     v = reinterpret_cast<const C<T> *>(smem)[e];
                 }

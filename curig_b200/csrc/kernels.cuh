@@ -22,7 +22,7 @@ struct DevGeom {
     int sparse_n;                  // FP32 spreader: chunks of fewer visibilities skip the tile
     int cbits;                     // bits of the in-tile start cell in the sort key (0: bin only)
     int smode;                     // tile accumulation: 0 two-word int32, 1 float atomics, 2 one-word int32
-                                   // (FP64: 1 double atomics, else int64 + int32)
+                                   // (FP64: 1 double atomics, else three-word int32)
     int tpitch;                    // tile row pitch of the thread-per-visibility kernels: tx + 1 rounded up
                                    // to even (the interpolator's rows start at an even x for TMA)
     int use_tma;                   // interpolator stages interior tiles with one TMA box load

@@ -312,7 +312,7 @@ int plan_destroy(Plan *p) {
 // 1 float atomics, 2 one-word int32).  Automatic: one word when the requested
 // epsilon is at least 1e-5 (its rounding, about 1.5e-6 relative, stays well
 // inside the error budget), else the exact two-word form.  FP64 tiles take the
-// exact int64 + int32 form in every mode but 1 (double atomics).
+// exact three-word int32 form in every mode but 1 (double atomics).
 static int tile_mode(const Plan *p) {
     switch (p->opt.smode) {
     case 1: return 1;
@@ -327,7 +327,7 @@ static int choose_tiles(Plan *p, int esize, bool force_slabs) {
     const int kw = gp.kp.kw;
     TileGeom &t = p->tg;
     // FP32 spreader: int32 fixed point, two words (exact) or one word per component;
-    // FP64: int64 + int32 fixed point (exact)
+    // FP64: three-word int32 fixed point (exact)
     const int mode = tile_mode(p);
     t.fix = kw > TAB_KW ? 0 : esize == 4 ? (mode == 0 ? 1 : mode == 2 ? 2 : 0) : (mode != 1 ? 3 : 0);
     // FP32 tiles: two CTAs per SM (<= 112 KB each); FP64 fixed-point tiles: one

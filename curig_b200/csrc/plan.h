@@ -21,7 +21,7 @@ struct Options {
     int sub = 0;              // visibilities per sub-problem (0: default)
     int smode = 0;            // FP32 tile accumulation: 0 automatic, 1 float atomics,
                               // 2 one-word int32 fixed point, 3 exact two-word int32 fixed point
-                              // (FP64: 1 double atomics, else exact int64 + int32)
+                              // (FP64: 1 double atomics, else exact three-word int32)
     size_t smem_budget = 0;   // bytes of shared memory per CTA for tiles (0: default)
     cudaStream_t stream = nullptr;
     int w_term = 0;           // 0: improved w-stacking, 1: w ignored (2-D gridding, no n - 1, n = 1)

@@ -68,7 +68,7 @@ typedef struct curig_opts {
                              epsilon >= 1e-5, else two-word), 1 float atomics, 2 one-word
                              int32 fixed point (22-bit terms, deterministic), 3 two-word
                              int32 fixed point (exact sums, deterministic).  FP64 tiles:
-                             1 double atomics, any other value int64 + int32 fixed point
+                             1 double atomics, any other value three-word int32 fixed point
                              (exact sums, deterministic) */
     int w_term;           /* 0: improved w-stacking (default); 1: w ignored -- 2-D gridding
                              without the n-1 term or the 1/n factor (the Nifty gridder's

@@ -256,7 +256,7 @@ def test_one_word_fixed_point_all_in_one_cell(C):
 
 
 def test_fp64_fixed_point_all_in_one_cell_wide_range(C):
-    """FP64 int64 + int32 tiles: a 4000-visibility chunk at one uv point with
+    """FP64 three-word int32 tiles: a 4000-visibility chunk at one uv point with
     magnitudes over sixteen decades (the chunk scale follows the largest; the
     high words of one cell take every term) against double atomics."""
     rng = np.random.default_rng(8)
