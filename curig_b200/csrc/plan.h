@@ -144,11 +144,12 @@ constexpr int MAX_SLABS = 8;
 // Tile spreaders: chunks with fewer visibilities spread straight to the grid
 // (each cell of such a tile receives about one tap), one warp per visibility.
 // Measured thresholds at 4096^2 (ms of the spreader): FP32 with 1.6e8
-// visibilities 19.5 for 64-192, 20.7 for 384; FP64 with one channel (1e7
-// visibilities, the reference ABI's call) 33.9 with the tile only, 21.0 / 19.5
-// / 17.7 / 20.7 for 32 / 64 / 128 / 256.
+// visibilities 19.5 for 64-192, 20.7 for 384; FP64 (three-word tiles) with one
+// channel (1e7 visibilities, the reference ABI's call) 21.7 with the tile only,
+// 14.1 / 14.1 / 15.8 / 20.5 for 32 / 64 / 128 / 256, with 16 channels 69.1 tile
+// only, 65.7 / 65.2 / 65.9 / 69.7.
 constexpr int DEFAULT_SPARSE_N = 128;
-constexpr int DEFAULT_SPARSE_N64 = 128;
+constexpr int DEFAULT_SPARSE_N64 = 64;
 // first row of slab k of nslab over nrow rows (k = nslab gives nrow)
 inline long long slab_first_row(long long nrow, int nslab, int k) {
     return ((long long)k * nrow + nslab - 1) / nslab;

@@ -86,7 +86,7 @@ typedef struct curig_opts {
                              2 from 384 MiB, else 1).  Plans ignore it. */
     int sparse;           /* tile spreaders: a chunk of fewer visibilities than this adds its
                              taps straight to the grid instead of through a shared-memory tile
-                             (0: automatic, 128 in FP32 and FP64; negative: always the tile) */
+                             (0: automatic, 128 in FP32, 64 in FP64; negative: always the tile) */
 } curig_opts;
 
 void curig_default_opts(curig_opts *opts);

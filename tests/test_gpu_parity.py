@@ -149,8 +149,8 @@ def _plan_run(kind, nx, ny, psx, psy, eps, sign, uvw, freq, vis=None, wgt=None, 
     return out, info
 
 
-# sparse: 0 the default split (chunks below 128 visibilities straight to the
-# grid, one warp per visibility), -1 every chunk through a tile, 1 << 30 no tile
+# sparse: 0 the default split (chunks below 128 (FP32) or 64 (FP64) visibilities
+# straight to the grid, one warp per visibility), -1 every chunk through a tile, 1 << 30 no tile
 @pytest.mark.parametrize("sparse", [0, -1, 1 << 30])
 @pytest.mark.parametrize("accumulate", [0, 1, 2, 3])
 @pytest.mark.parametrize("precision,eps,tol", [("fp64", 1e-9, 1e-8), ("fp64", 1e-5, 1e-4),
