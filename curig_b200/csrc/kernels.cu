@@ -520,7 +520,7 @@ k_spread(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__ b
     const int kk = kw * kw, k3 = kk * kw;
     const int txy = g.tx * g.ty;
     for (int s = g.sub_lo + blockIdx.x; s < total; s += gridDim.x) {
-        long long b = find_bin(sub_end, g.nbins, s);
+        long long b = g.cbin ? g.cbin[s] : find_bin(sub_end, g.nbins, s);
         int cnt = bin_count[b];
         int nsb = (cnt + g.sub - 1) / g.sub;
         int chunk = s - (sub_end[b] - nsb);
@@ -590,7 +590,7 @@ k_interp(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__ b
     const int kk = kw * kw, k3 = kk * kw;
     const int txy = g.tx * g.ty;
     for (int s = g.sub_lo + blockIdx.x; s < total; s += gridDim.x) {
-        long long b = find_bin(sub_end, g.nbins, s);
+        long long b = g.cbin ? g.cbin[s] : find_bin(sub_end, g.nbins, s);
         int cnt = bin_count[b];
         int nsb = (cnt + g.sub - 1) / g.sub;
         int chunk = s - (sub_end[b] - nsb);
@@ -706,26 +706,27 @@ __device__ __forceinline__ int round_fix(float a, float k) {
 
 // FP64 tiles (shared-memory double atomics are compare-and-swap loops, and
 // 64-bit integer atomics run at about a quarter of the 32-bit rate on this
-// part): each scaled term x is split exactly as h * 2^36 + m * 2^18 + l, h
-// and m rounded to integers by FMAs against 1.5 * 2^52 (the remainders
-// x - h 2^36 and x - h 2^36 - m 2^18 are exact), l the last remainder rounded
-// to an integer; h, m and l go to three int32 planes.  The chunk scale
-// q = 2^k takes the largest k with max|c| wmax3 q <= 2^54, so |h| <= 2^18 and
-// |m|, |l| <= 2^17 and, with at most 4096 terms per cell (sub <= 4096), no
-// plane's sum leaves int32: cell sums are exact and order-independent, and a
-// term's rounding is at most 2^-55 of max|c| wmax3, below the FP64 rounding of
-// the product itself (2^-53 of the product).
+// part): each scaled term x is split exactly as h * 2^36 + m * 2^18 + l with
+// three int32 planes.  Adding 1.5 * 2^70 rounds x to a multiple of 2^18 whose
+// quotient X = round(x / 2^18) is the bit-pattern difference (same binade for
+// |x| <= 2^54); h = X >> 18 and m = X & (2^18 - 1) split it further (m >= 0),
+// and the remainder x - X 2^18 (exact, |.| <= 2^17) is rounded to the integer
+// l by adding 1.5 * 2^52.  Four FP64 additions per term.  The chunk scale
+// q = 2^k takes the largest k with max|c| wmax3 q <= 2^54, so |h| <= 2^18,
+// 0 <= m < 2^18, |l| <= 2^17 and, with at most 4096 terms per cell (sub <=
+// 4096), no plane's sum leaves int32: cell sums are exact and order-
+// independent, and a term's rounding is at most 2^-55 of max|c| wmax3, below
+// the FP64 rounding of the product itself (2^-53 of the product).
 constexpr int FIX64_BITS = 54;
 __device__ __forceinline__ void split_fix3(double x, int &h, int &m, int &l) {
-    const double M = 6755399441055744.0;                  // 1.5 * 2^52
-    const long long MB = 0x4338000000000000LL;            // its bit pattern
-    const double th = fma(x, 0x1p-36, M);                 // x * 2^-36, rounded to an integer
-    h = (int)(__double_as_longlong(th) - MB);
-    const double r1 = fma(th - M, -0x1p36, x);            // x - h * 2^36, exact
-    const double tm = fma(r1, 0x1p-18, M);                // r1 * 2^-18, rounded to an integer
-    m = (int)(__double_as_longlong(tm) - MB);
-    const double r2 = fma(tm - M, -0x1p18, r1);           // r1 - m * 2^18, exact
-    l = (int)(__double_as_longlong(r2 + M) - MB);
+    const double M18 = 1770887431076116955136.0;          // 1.5 * 2^70: ulp 2^18
+    const double M0 = 6755399441055744.0;                 // 1.5 * 2^52: ulp 1
+    const double t1 = x + M18;                            // x rounded to a multiple of 2^18
+    const double t2 = (x - (t1 - M18)) + M0;              // remainder (exact), rounded to an integer
+    const long long X = __double_as_longlong(t1) - __double_as_longlong(M18);
+    h = (int)(X >> 18);
+    m = (int)(X & 0x3FFFF);
+    l = (int)(__double_as_longlong(t2) - __double_as_longlong(M0));
 }
 
 template <typename T, int KW>
