@@ -163,9 +163,10 @@ __global__ void k_wrange(const double *__restrict__ w, int stride, long long nro
 }
 
 // ------------------------------------------------------------------ binning (counting sort)
-// Sort key of one visibility: bin id in the high bits, then the residue mod 32
-// of its start cell's index in the tile (the shared-memory bank of its first
-// tap).  With row slabs the bin id is slab * nbins_slab + bin (slab = row *
+// Sort key of one visibility: bin id in the high bits, then the residue of its
+// start cell's index in the tile (mod 16 for the FP32 tile kernels' class
+// schedule, mod 32 for the FP64 and wide-window kernels: the shared-memory
+// bank of its first tap).  With row slabs the bin id is slab * nbins_slab + bin (slab = row *
 // nslab / nrow), so each slab's visibilities are contiguous in sorted order.
 // BAD_KEY marks a visibility that could not be placed.
 //
