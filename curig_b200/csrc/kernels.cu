@@ -1699,22 +1699,18 @@ __global__ void k_correct_m2d(DevCorr cc, const C<T> *__restrict__ grid, C<T> *_
         sincos(Q.ph, &sc, &cs);
         double den = cc.psi1[s] * cc.psi2[r] * Q.psi3 * Q.n;
         double fr = cs / den, fi = sc / den;
-        int ixs[4], iys[4];
+        // the four mirrored pixels (hx +- r, hy +- s), slot t = 2 sx + sy, in
+        // fixed register slots with a validity flag
+        bool val[4];
         long long off[4];
-        int np = 0;
-        for (int sx = 0; sx < 2; ++sx) {
-            int ix = sx ? hx - r : hx + r;
-            if (ix < 0 || ix >= cc.nx || (sx && r == 0)) continue;
-            int w2 = sx ? cc.nf2 - r : r;
-            for (int sy = 0; sy < 2; ++sy) {
-                int iy = sy ? hy - s : hy + s;
-                if (iy < 0 || iy >= cc.ny || (sy && s == 0)) continue;
-                int xp = sy ? cc.ny - s : s;               // image column of grid column nf1 - s / s
-                ixs[np] = ix;
-                iys[np] = iy;
-                off[np] = (long long)xp * cc.nf2 + w2;
-                ++np;
-            }
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            const int sx = t >> 1, sy = t & 1;
+            const int ix = sx ? hx - r : hx + r, iy = sy ? hy - s : hy + s;
+            val[t] = ix >= 0 && ix < cc.nx && !(sx && r == 0) && iy >= 0 && iy < cc.ny && !(sy && s == 0);
+            const int w2 = sx ? cc.nf2 - r : r;
+            const int xp = sy ? cc.ny - s : s;               // image column of grid column nf1 - s / s
+            off[t] = val[t] ? (long long)xp * cc.nf2 + w2 : 0;
         }
         double ar[4] = {0, 0, 0, 0}, ai[4] = {0, 0, 0, 0};
         double es, ec, ss, scs;
@@ -1724,7 +1720,7 @@ __global__ void k_correct_m2d(DevCorr cc, const C<T> *__restrict__ grid, C<T> *_
             const C<T> *gp = grid + p * plane;
 #pragma unroll
             for (int t = 0; t < 4; ++t) {
-                if (t < np) {
+                if (val[t]) {
                     C<T> v = gp[off[t]];
                     ar[t] += (double)v.x * ec - (double)v.y * es;
                     ai[t] += (double)v.x * es + (double)v.y * ec;
@@ -1734,11 +1730,14 @@ __global__ void k_correct_m2d(DevCorr cc, const C<T> *__restrict__ grid, C<T> *_
             ec = nr;
             es = ni;
         }
-        for (int t = 0; t < np; ++t) {
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            if (!val[t]) continue;
+            const int ix = (t >> 1) ? hx - r : hx + r, iy = (t & 1) ? hy - s : hy + s;
             C<T> o;
             o.x = (T)(ar[t] * fr - ai[t] * fi);
             o.y = (T)(ar[t] * fi + ai[t] * fr);
-            dirty[(long long)ixs[t] * cc.ny + iys[t]] = o;
+            dirty[(long long)ix * cc.ny + iy] = o;
         }
     }
 }
@@ -1758,22 +1757,23 @@ __global__ void k_correct_d2m(DevCorr cc, const C<T> *__restrict__ dirty, C<T> *
         sincos(-Q.ph, &sc, &cs);
         double den = cc.psi1[s] * cc.psi2[r] * Q.psi3 * Q.n;
         double fr = cs / den, fi = sc / den;
+        // the four mirrored pixels in fixed register slots (t = 2 sx + sy)
+        bool val[4];
         double vr[4], vi[4];
         long long off[4];
-        int np = 0;
-        for (int sx = 0; sx < 2; ++sx) {
-            int ix = sx ? hx - r : hx + r;
-            if (ix < 0 || ix >= cc.nx || (sx && r == 0)) continue;
-            int w2 = sx ? cc.nf2 - r : r;
-            for (int sy = 0; sy < 2; ++sy) {
-                int iy = sy ? hy - s : hy + s;
-                if (iy < 0 || iy >= cc.ny || (sy && s == 0)) continue;
-                int xp = sy ? cc.ny - s : s;
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            const int sx = t >> 1, sy = t & 1;
+            const int ix = sx ? hx - r : hx + r, iy = sy ? hy - s : hy + s;
+            val[t] = ix >= 0 && ix < cc.nx && !(sx && r == 0) && iy >= 0 && iy < cc.ny && !(sy && s == 0);
+            const int w2 = sx ? cc.nf2 - r : r;
+            const int xp = sy ? cc.ny - s : s;
+            off[t] = val[t] ? (long long)xp * cc.nf2 + w2 : 0;
+            vr[t] = vi[t] = 0;
+            if (val[t]) {
                 C<T> d = dirty[(long long)ix * cc.ny + iy];
-                vr[np] = (double)d.x * fr - (double)d.y * fi;
-                vi[np] = (double)d.x * fi + (double)d.y * fr;
-                off[np] = (long long)xp * cc.nf2 + w2;
-                ++np;
+                vr[t] = (double)d.x * fr - (double)d.y * fi;
+                vi[t] = (double)d.x * fi + (double)d.y * fr;
             }
         }
         double es, ec, ss, scs;
@@ -1783,7 +1783,7 @@ __global__ void k_correct_d2m(DevCorr cc, const C<T> *__restrict__ dirty, C<T> *
             C<T> *gp = grid + p * plane;
 #pragma unroll
             for (int t = 0; t < 4; ++t) {
-                if (t < np) {
+                if (val[t]) {
                     C<T> o;
                     o.x = (T)(vr[t] * ec - vi[t] * es);
                     o.y = (T)(vr[t] * es + vi[t] * ec);
