@@ -117,9 +117,9 @@ static int oneshot(int type, long long nrow, int nchan, int nx, int ny, double p
     for (int k = 0; ok && k < nslab; ++k)
         ok = chk(cudaEventCreateWithFlags(&ev_ready[k], cudaEventDisableTiming)) &&
              chk(cudaEventCreateWithFlags(&ev_done[k], cudaEventDisableTiming));
-    ok = ok && chk(cudaMallocAsync((void **)&d_uvw, 3 * nrow * sizeof(double), st)) &&
-         chk(cudaMallocAsync(&d_vis, M * cs, st)) && (!wgt || chk(cudaMallocAsync(&d_wgt, M * rs, st))) &&
-         chk(cudaMallocAsync(&d_dirty, npix * cs, st)) && chk(cudaEventRecord(ev_alloc, st)) &&
+    ok = ok && chk(alloc_async((void **)&d_uvw, 3 * nrow * sizeof(double), st)) &&
+         chk(alloc_async(&d_vis, M * cs, st)) && (!wgt || chk(alloc_async(&d_wgt, M * rs, st))) &&
+         chk(alloc_async(&d_dirty, npix * cs, st)) && chk(cudaEventRecord(ev_alloc, st)) &&
          chk(cudaStreamWaitEvent(cp, ev_alloc, 0)) &&
          chk(cudaMemcpyAsync(d_uvw, uvw, 3 * nrow * sizeof(double), cudaMemcpyHostToDevice, cp)) &&
          chk(cudaEventRecord(ev_uvw, cp)) &&
@@ -371,7 +371,7 @@ extern "C" int curig_nufft_setpts(curig_nufft h, int64_t m, const double *d_x, c
     Plan *p = h->p;
     if (h->d_uvw) cudaFreeAsync(h->d_uvw, p->st);
     h->d_uvw = nullptr;
-    if (cudaMallocAsync((void **)&h->d_uvw, 3 * m * sizeof(double), p->st) != cudaSuccess)
+    if (alloc_async((void **)&h->d_uvw, 3 * m * sizeof(double), p->st) != cudaSuccess)
         return fail(ERR_NOMEM, "out of device memory");
     const double sgn = h->type == 1 ? (double)h->iflag : -(double)h->iflag;
     launch_nupts_uvw(m, d_x, h->dim >= 2 ? d_y : nullptr, h->dim == 3 ? h->d_z : nullptr, sgn, h->d_uvw, p->st);
@@ -563,7 +563,7 @@ int gridder_execution(curafft_plan *plan, ragridder_plan *gplan) {
     Plan *p = static_cast<Plan *>(plan->impl);
     double *d_wgt = nullptr;
     if (gplan && gplan->kv.weight) {               // ra_exec.cu:98-104 uploads per call
-        if (cudaMallocAsync((void **)&d_wgt, (size_t)p->nrow * sizeof(double), p->st) != cudaSuccess)
+        if (alloc_async((void **)&d_wgt, (size_t)p->nrow * sizeof(double), p->st) != cudaSuccess)
             return ERR_NOMEM;
         cudaMemcpyAsync(d_wgt, gplan->kv.weight, (size_t)p->nrow * sizeof(double), cudaMemcpyHostToDevice,
                         p->st);

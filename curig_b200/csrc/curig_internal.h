@@ -17,6 +17,16 @@
 
 namespace curig {
 
+// cudaMallocAsync whose failure is reported by its return value only: the
+// runtime's last-error state is cleared again, so the launch checks
+// (cudaGetLastError) of this or a later call do not report the failed
+// allocation a second time.
+inline cudaError_t alloc_async(void **ptr, size_t bytes, cudaStream_t st) {
+    const cudaError_t e = cudaMallocAsync(ptr, bytes, st);
+    if (e != cudaSuccess) (void)cudaGetLastError();
+    return e;
+}
+
 // ------------------------------------------------------------------ errors
 enum Status : int {
     OK = 0,

@@ -258,8 +258,10 @@ static int train_setup(int W, double sigma, const float *params, TrainBuffers &B
     gauss_legendre(TNQ, x.data(), w.data());
     if (cudaMalloc(&B.P, NPAR * 4) || cudaMalloc(&B.m1, NPAR * 4) || cudaMalloc(&B.m2, NPAR * 4) ||
         cudaMalloc(&B.grad, NPAR * 4) || cudaMalloc(&B.qx, TNQ * 8) || cudaMalloc(&B.qw, TNQ * 8) ||
-        cudaMalloc(&B.out, 8))
+        cudaMalloc(&B.out, 8)) {
+        (void)cudaGetLastError();              // reported here, not by a later launch check
         return ERR_NOMEM;
+    }
     cudaMemcpy(B.P, params, NPAR * 4, cudaMemcpyHostToDevice);
     cudaMemset(B.m1, 0, NPAR * 4);
     cudaMemset(B.m2, 0, NPAR * 4);

@@ -210,8 +210,8 @@ int nufft3_setpts(Nufft3 *p, long long m, const double *d_x, long long n, const 
     p->m = m;
     p->n = n;
     const size_t esz = p->precision ? 8 : 16;
-    if (cudaMallocAsync((void **)&p->d_keys, 2 * sizeof(unsigned long long), p->st) != cudaSuccess ||
-        cudaMallocAsync((void **)&p->d_err, sizeof(int), p->st) != cudaSuccess)
+    if (alloc_async((void **)&p->d_keys, 2 * sizeof(unsigned long long), p->st) != cudaSuccess ||
+        alloc_async((void **)&p->d_err, sizeof(int), p->st) != cudaSuccess)
         return ERR_NOMEM;
     double xlo, xhi, slo, shi;
     if ((s = range_of(p, d_x, m, xlo, xhi)) || (s = range_of(p, d_s, n, slo, shi))) return s;
@@ -223,13 +223,13 @@ int nufft3_setpts(Nufft3 *p, long long m, const double *d_x, long long n, const 
     if (p->nf <= 0 || p->nf >= (1 << 30)) return ERR_UNSUPPORTED;
     double qx[MAX_QUAD], qg[MAX_QUAD];
     const int nq = quadrature_terms(p->kp, Window(), qx, qg);
-    if (cudaMallocAsync((void **)&p->d_xp, m * sizeof(double), p->st) != cudaSuccess ||
-        cudaMallocAsync((void **)&p->d_pre, m * sizeof(double2), p->st) != cudaSuccess ||
-        cudaMallocAsync((void **)&p->d_theta, n * sizeof(double), p->st) != cudaSuccess ||
-        cudaMallocAsync((void **)&p->d_post, n * sizeof(double2), p->st) != cudaSuccess ||
-        cudaMallocAsync((void **)&p->d_quad, 2 * MAX_QUAD * sizeof(double), p->st) != cudaSuccess ||
-        cudaMallocAsync(&p->d_grid, (size_t)p->nf * esz, p->st) != cudaSuccess ||
-        cudaMallocAsync(&p->d_F, n * esz, p->st) != cudaSuccess)
+    if (alloc_async((void **)&p->d_xp, m * sizeof(double), p->st) != cudaSuccess ||
+        alloc_async((void **)&p->d_pre, m * sizeof(double2), p->st) != cudaSuccess ||
+        alloc_async((void **)&p->d_theta, n * sizeof(double), p->st) != cudaSuccess ||
+        alloc_async((void **)&p->d_post, n * sizeof(double2), p->st) != cudaSuccess ||
+        alloc_async((void **)&p->d_quad, 2 * MAX_QUAD * sizeof(double), p->st) != cudaSuccess ||
+        alloc_async(&p->d_grid, (size_t)p->nf * esz, p->st) != cudaSuccess ||
+        alloc_async(&p->d_F, n * esz, p->st) != cudaSuccess)
         return ERR_NOMEM;
     if (cudaMemcpyAsync(p->d_quad, qx, nq * sizeof(double), cudaMemcpyHostToDevice, p->st) != cudaSuccess ||
         cudaMemcpyAsync(p->d_quad + MAX_QUAD, qg, nq * sizeof(double), cudaMemcpyHostToDevice, p->st) != cudaSuccess)

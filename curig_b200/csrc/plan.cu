@@ -33,7 +33,7 @@ template <typename X>
 static cudaError_t dalloc(X **ptr, size_t bytes, cudaStream_t st) {
     *ptr = nullptr;
     if (bytes == 0) bytes = 16;
-    return cudaMallocAsync((void **)ptr, bytes, st);
+    return alloc_async((void **)ptr, bytes, st);
 }
 
 template <typename X>
@@ -744,7 +744,7 @@ static int fft_rows(Plan *p, void *buf, long long nrows, int n, cufftHandle h, s
                     cufftHandle h_rest, size_t wr, int b_rest, int dir) {
     const size_t ws = std::max(wh, h_rest ? wr : (size_t)0);
     void *work = nullptr;
-    if (ws) CU_TRY(cudaMallocAsync(&work, ws, p->st));
+    if (ws) CU_TRY(alloc_async(&work, ws, p->st));
     int s = OK;
     if (cufftSetWorkArea(h, work) != CUFFT_SUCCESS || (h_rest && cufftSetWorkArea(h_rest, work) != CUFFT_SUCCESS))
         s = ERR_CUFFT;

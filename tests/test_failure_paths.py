@@ -1,4 +1,5 @@
-"""Failure paths on the GPU without a GPU fault.
+"""Failure paths on the GPU without a GPU fault: a bounded wait made to run
+out, and allocations beyond the device's memory.
 
 The interpolator stages interior tiles with TMA box loads and waits on an
 mbarrier for at most a bounded number of polls; when the wait runs out, the
@@ -47,3 +48,53 @@ def test_tile_load_wait_runs_out_and_context_survives():
     assert st == 0, L.lib.curig_last_error()
     ref = dft.dirty2ms_dft(uvw, freq, img.astype(np.complex128), wgt.astype(np.float64), psx, psx, -1)
     assert l2err(ref, vis) < 10 * eps
+
+
+def test_grid_beyond_device_memory_is_reported_and_context_survives():
+    """Out of memory on the host's side of the call: a plan whose explicit
+    oversampled grid (131072^2 FP64 cells, one plane: 275 GB) cannot be
+    allocated returns status 6 from set points, before any kernel touches the
+    grid; the plan is released and a normal plan afterwards is correct."""
+    import torch
+
+    import curig_b200._lib as L
+    from curig_b200 import GridderPlan
+    freq, uvw, ms, wgt = disk_inputs(500, 1, 64, 2.0, max_pix=25.0, seed=7)
+    psx = 2.0 * np.pi / 180 / 64
+    d_uvw = torch.from_numpy(np.ascontiguousarray(uvw)).cuda()
+    big = GridderPlan(1, 64, 64, psx, psx, 1e-6, 2.0, -1, precision="fp64", window="es", w_term=1,
+                      grid_x=131072, grid_y=131072)
+    with pytest.raises(L.CurigError) as err:
+        big.setpts(d_uvw, freq)
+    assert err.value.code == 6, str(err.value)
+    big.close()
+    ok = GridderPlan(1, 64, 64, psx, psx, 1e-6, 2.0, -1, precision="fp64", window="es")
+    ok.setpts(d_uvw, freq)
+    d = torch.empty((64, 64), dtype=torch.complex128, device="cuda")
+    ok.execute(torch.from_numpy(np.ascontiguousarray(ms)).cuda(), torch.from_numpy(np.ascontiguousarray(wgt)).cuda(), d)
+    torch.cuda.synchronize()
+    ok.close()
+    ref = dft.ms2dirty_dft(uvw, freq, ms, wgt, 64, 64, psx, psx, -1)
+    assert l2err(ref, d.cpu().numpy()) < 1e-5
+
+
+def test_one_shot_call_beyond_device_memory_then_a_normal_call():
+    """The same through the one-shot ABI (host buffers): status 6 for the
+    275 GB grid, then the same call with the default grid is correct."""
+    import curig_b200._lib as L
+    freq, uvw, ms, wgt = disk_inputs(500, 1, 64, 2.0, max_pix=25.0, seed=8)
+    uvw = np.ascontiguousarray(uvw)
+    ms, wgt = np.ascontiguousarray(ms), np.ascontiguousarray(wgt)
+    psx = 2.0 * np.pi / 180 / 64
+    out = np.zeros((64, 64), dtype=np.complex128)
+
+    def call(opts):
+        return L.lib.curig_ms2dirty(500, 1, 64, 64, psx, psx, freq.ctypes.data, uvw.ctypes.data, ms.ctypes.data,
+                                    wgt.ctypes.data, out.ctypes.data, 1e-6, 2.0, -1, ctypes.byref(opts))
+
+    assert call(L.make_opts(w_term=1, grid_x=131072, grid_y=131072)) == 6
+    assert "memory" in L.lib.curig_last_error().decode()
+    st = call(L.make_opts())
+    assert st == 0, L.lib.curig_last_error()
+    ref = dft.ms2dirty_dft(uvw, freq, ms, wgt, 64, 64, psx, psx, -1)
+    assert l2err(ref, out) < 1e-5
