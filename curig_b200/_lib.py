@@ -15,7 +15,9 @@ from ctypes import c_double, c_int, c_int64, c_void_p
 
 import numpy as np
 
-LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libcurafft.so")
+# CURIG_LIB selects another build of the library, e.g. the bounds-checked
+# libcurafft_check.so (curig_b200/csrc/build.py --check)
+LIB_PATH = os.environ.get("CURIG_LIB") or os.path.join(os.path.dirname(os.path.abspath(__file__)), "libcurafft.so")
 
 try:
     lib = ctypes.CDLL(LIB_PATH)

@@ -214,7 +214,8 @@ __global__ void k_bin_count(DevGeom g, const double *__restrict__ uu, const doub
             keys[j] = key;
         }
         const unsigned peers = __match_any_sync(0xffffffffu, key);
-        if (key != BAD_KEY && lane == __ffs(peers) - 1) atomicAdd(count + key, __popc(peers));
+        if (key != BAD_KEY && lane == __ffs(peers) - 1 && IN_BOUNDS((long long)key < (g.nbins << g.cbits), g.dbg))
+            atomicAdd(count + key, __popc(peers));
     }
     if (bad) atomicOr(err, bad);
 }
@@ -397,10 +398,12 @@ __global__ void k_records(DevGeom g, const double *__restrict__ uu, const double
         const unsigned peers = __match_any_sync(0xffffffffu, key);
         const int leader = __ffs(peers) - 1;
         int base = 0;
-        if (key != BAD_KEY && lane == leader) base = atomicAdd(kcur + key, __popc(peers));
+        if (key != BAD_KEY && lane == leader && IN_BOUNDS((long long)key < (g.nbins << g.cbits), g.dbg))
+            base = atomicAdd(kcur + key, __popc(peers));
         base = __shfl_sync(0xffffffffu, base, leader);
         if (key == BAD_KEY) continue;
         const int p = base + __popc(peers & below);
+        if (!IN_BOUNDS(p >= 0 && p < M, g.dbg)) continue;
         R<T> r;
         r.x = (T)L.ux;
         r.y = (T)L.uy;
@@ -663,12 +666,19 @@ __device__ __forceinline__ void sub_range(const DevGeom &g, const int *bin_start
                                           const int *sub_end, int s, long long &b, int &start, int &stride,
                                           int &n) {
     b = g.cbin ? g.cbin[s] : find_bin(sub_end, g.nbins, s);
+    if (!IN_BOUNDS(b >= 0 && b < g.nbins, g.dbg)) {
+        b = 0; start = 0; stride = 1; n = 0;
+        return;
+    }
     int cnt = bin_count[b];
     int nsb = (cnt + g.sub - 1) / g.sub;
     int j = s - (sub_end[b] - nsb);
     start = bin_start[b] + j;
     stride = nsb;
     n = (cnt - j + nsb - 1) / nsb;
+    if (!IN_BOUNDS(start >= 0 && n >= 0 && (n == 0 || start + (long long)(n - 1) * stride < g.nrow * g.nchan),
+                   g.dbg))
+        n = 0;
 }
 
 // Exact fixed-point accumulation of the FP32 spreader.  Shared-memory float
@@ -799,10 +809,11 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
                     const int t = t0 + lane, tt = min(t, items - 1);
                     const int dz = tt / (KW * KW), rem = tt - dz * (KW * KW), dy = rem / KW, dx = rem - dy * KW;
                     const T kx = tap(dx), ky = tap(KW + dy), kz = tap(2 * KW + dz);
-                    if (t < items) {
-                        const int gz = g.zpad ? wrap3(gz0 + dz, g.nf3) : gz0 + dz;
-                        C<T> *cell = grid + ((long long)gz * g.nf2 + wrap3(gy0 + dy, g.nf2)) * g.nf1 +
-                                     wrap3(gx0 + dx, g.nf1);
+                    const int gz = g.zpad ? wrap3(gz0 + dz, g.nf3) : gz0 + dz;
+                    const int gy = wrap3(gy0 + dy, g.nf2), gx = wrap3(gx0 + dx, g.nf1);
+                    if (t < items && IN_BOUNDS(gx >= 0 && gx < g.nf1 && gy >= 0 && gy < g.nf2 && gz >= 0 &&
+                                                   gz < g.nf3, g.dbg)) {
+                        C<T> *cell = grid + ((long long)gz * g.nf2 + gy) * g.nf1 + gx;
                         const T ar = c.x * kz * ky, ai = c.y * kz * ky;
                         atomicAdd(&cell->x, ar * kx);
                         atomicAdd(&cell->y, ai * kx);
@@ -900,6 +911,7 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
             }
             int cb = cell_bits(r.w);
             int cell = ((cb >> 20) & 0xfff) * txy + ((cb >> 10) & 0x3ff) * tx + (cb & 0x3ff) + shift;
+            if (!IN_BOUNDS(cell >= 0 && cell + (KZ - 1) * txy + (KW - 1) * (tx + 1) < ntile, g.dbg)) continue;
             c.x *= q;
             c.y *= q;
 #pragma unroll 1
@@ -999,7 +1011,7 @@ k_spread_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
                     const int gz = g.zpad ? wrap3(oz + z, g.nf3) : z;
                     C<T> *grow = grid + ((long long)gz * g.nf2 + gy) * g.nf1;
                     const int c0 = 2 * xp;
-                    bool vec = false;
+                    bool vec = !IN_BOUNDS(gy >= 0 && gy < g.nf2 && gz >= 0 && gz < g.nf3 && z < g.tz, g.dbg);
                     if constexpr (sizeof(T) == 4) {
                         if (xin) {
                             red_add_v4(reinterpret_cast<float *>(grow + x_al + c0), v0.x, v0.y, v1.x, v1.y);
@@ -1078,7 +1090,7 @@ __device__ __forceinline__ void class_range(const int *cls, int q, int n, int &c
 // visibility.  The next step's record and amplitude are loaded before this
 // step's taps, so their latency overlaps the shared-memory atomics.
 struct TapRun {
-    int start, stride, c0, nk, T, S, KZ, txy, tx, shift, warp, f;
+    int start, stride, c0, nk, T, S, KZ, txy, tx, shift, warp, f, ntile;
     float q;
 };
 
@@ -1119,6 +1131,8 @@ __device__ __forceinline__ void spread_steps(const DevGeom &g, const WinTab<floa
         const int cb = cell_bits(r.w);
         const int cell = ((cb >> 20) & 0xfff) * t.txy + ((cb >> 10) & 0x3ff) * t.tx + (cb & 0x3ff) + t.shift;
         const int p0 = 2 * cell + t.f, d1 = 1 - 2 * t.f;     // first word; second word = first + d1
+        // the visibility's cells: cell .. cell + (KZ - 1) txy + (KW - 1) (tx + 1)
+        if (!IN_BOUNDS(cell >= 0 && cell + (t.KZ - 1) * t.txy + (KW - 1) * (t.tx + 1) < t.ntile, g.dbg)) continue;
         if constexpr (MODE == 0) {
             const float cr = c.x * t.q, ci = c.y * t.q;
 #pragma unroll 1
@@ -1252,8 +1266,10 @@ k_spread_f32(DevGeom g, const int *__restrict__ bin_start, const int *__restrict
                         if (!act) continue;
                         const int gz = g.zpad ? wrap3(gz0 + dz, g.nf3) : gz0 + dz;
                         const float cr = c.x * kz * ky, ci = c.y * kz * ky;
-                        red_add_v4(reinterpret_cast<float *>(grid + ((long long)gz * g.nf2 + gy) * g.nf1 + gx),
-                                   cr * k0, ci * k0, cr * k1, ci * k1);
+                        if (IN_BOUNDS(gx >= 0 && (gx & 1) == 0 && gx + 1 < g.nf1 && gy >= 0 && gy < g.nf2 &&
+                                          gz >= 0 && gz < g.nf3, g.dbg))
+                            red_add_v4(reinterpret_cast<float *>(grid + ((long long)gz * g.nf2 + gy) * g.nf1 + gx),
+                                       cr * k0, ci * k0, cr * k1, ci * k1);
                     }
                 }
             }
@@ -1286,7 +1302,8 @@ k_spread_f32(DevGeom g, const int *__restrict__ bin_start, const int *__restrict
                 for (int u = 0; u < 4; ++u) {
                     const float mc = fmaxf(fabsf(cc[u].x), fabsf(cc[u].y));
                     m = fmaxf(m, mc);
-                    if (one && k0 + u * TTHREADS < n)
+                    if (one && k0 + u * TTHREADS < n &&
+                        IN_BOUNDS(((cb[u] >> 10) & 0x3ff) < g.ty && (cb[u] & 0x3ff) < tx, g.dbg))
                         atomicAdd(colsum + ((cb[u] >> 10) & 0x3ff) * tx + (cb[u] & 0x3ff), mc);
                 }
             }
@@ -1354,7 +1371,7 @@ k_spread_f32(DevGeom g, const int *__restrict__ bin_start, const int *__restrict
             class_range(cls, klass, n, c0, nk);
             const int KZ = g.no_w ? 1 : KW;
             const int S = max(1, min(KZ, TWARPS / max(T, 1)));
-            const TapRun run{start, stride, c0, nk, T, S, KZ, txy, tx, shift, warp, f, q};
+            const TapRun run{start, stride, c0, nk, T, S, KZ, txy, tx, shift, warp, f, ntile, q};
             if (one) spread_steps<KW, 2>(g, tab, rec, cs, wA, wB, run);
             else if (two) spread_steps<KW, 0>(g, tab, rec, cs, wA, wB, run);
             else spread_steps<KW, 1>(g, tab, rec, cs, wA, wB, run);
@@ -1394,7 +1411,9 @@ k_spread_f32(DevGeom g, const int *__restrict__ bin_start, const int *__restrict
                     const int gz = g.zpad ? wrap3(oz + z, g.nf3) : z;
                     float2 *grow = grid + ((long long)gz * g.nf2 + gy) * g.nf1;
                     const int col = 2 * xp;
-                    if (xin) {
+                    if (!IN_BOUNDS(gy >= 0 && gy < g.nf2 && gz >= 0 && gz < g.nf3 && z < g.tz &&
+                                       (!xin || (x_al + col >= 0 && x_al + col + 1 < g.nf1)), g.dbg)) {
+                    } else if (xin) {
                         red_add_v4(reinterpret_cast<float *>(grow + x_al + col), v0.x, v0.y, v1.x, v1.y);
                     } else {
                         if (nz0) atomic_add_c(grow + wrap3(x_al + col, g.nf1), v0);
@@ -1415,8 +1434,9 @@ k_spread_f32(DevGeom g, const int *__restrict__ bin_start, const int *__restrict
 // vis[idx[i]] = value * wgt * e^{-i o_c w} (ra_exec.cu:56-89; the weight
 // multiplies, utils.cu:189): the scatter of dirty2ms back to input order.
 template <typename T>
-__device__ __forceinline__ void vis_store(const VisIO &io, int i, C<T> v) {
+__device__ __forceinline__ void vis_store(const VisIO &io, int i, C<T> v, long long m, int *dbg) {
     const int j = io.idx[i];
+    if (!IN_BOUNDS(j >= 0 && j < m, dbg)) return;
     const C<T> e = static_cast<const C<T> *>(io.ph)[i];
     const T wt = io.wgt ? static_cast<const T *>(io.wgt)[j] : (T)1;
     static_cast<C<T> *>(io.vis)[j] = C<T>{(v.x * e.x + v.y * e.y) * wt, (v.y * e.x - v.x * e.y) * wt};
@@ -1430,15 +1450,23 @@ template <typename T> struct VisDst {
     T wt;
 };
 template <typename T>
-__device__ __forceinline__ VisDst<T> vis_dst(const VisIO &io, int i) {
+__device__ __forceinline__ VisDst<T> vis_dst(const VisIO &io, int i, long long m, int *dbg) {
     VisDst<T> d;
     d.j = io.idx[i];
     d.e = static_cast<const C<T> *>(io.ph)[i];
+    if (!IN_BOUNDS(d.j >= 0 && d.j < m, dbg)) {
+        d.j = -1;                                    // (bounds-checked build only) no scatter
+        d.wt = (T)0;
+        return d;
+    }
     d.wt = io.wgt ? static_cast<const T *>(io.wgt)[d.j] : (T)1;
     return d;
 }
 template <typename T>
 __device__ __forceinline__ void vis_put(const VisIO &io, const VisDst<T> &d, C<T> v) {
+#ifdef CURIG_BOUNDS_CHECK
+    if (d.j < 0) return;
+#endif
     static_cast<C<T> *>(io.vis)[d.j] =
         C<T>{(v.x * d.e.x + v.y * d.e.y) * d.wt, (v.y * d.e.x - v.x * d.e.y) * d.wt};
 }
@@ -1469,7 +1497,8 @@ __device__ __forceinline__ void load_tile(const DevGeom &g, const C<T> *__restri
                 if (xin && row < nrows) {
                     int gy = wrap3(oy + y, g.nf2);
                     int gz = g.zpad ? wrap3(oz + z, g.nf3) : z;
-                    v[k] = grid[((long long)gz * g.nf2 + gy) * g.nf1 + gx];
+                    v[k] = IN_BOUNDS(gx >= 0 && gx < g.nf1 && gy >= 0 && gy < g.nf2 && gz >= 0 && gz < g.nf3, g.dbg)
+                               ? grid[((long long)gz * g.nf2 + gy) * g.nf1 + gx] : C<T>{0, 0};
                 }
                 row += NW;
                 y += NW;
@@ -1591,7 +1620,7 @@ k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
             const int dz0 = part * KZ / S, dz1 = (part + 1) * KZ / S;
             R<T> r = rec[i];
             VisDst<T> dst;
-            if (S == 1) dst = vis_dst<T>(io, i);
+            if (S == 1) dst = vis_dst<T>(io, i, g.nrow * g.nchan, g.dbg);
             T kx[KW], ky[KW];
 #pragma unroll
             for (int d = 0; d < KW; ++d) {
@@ -1599,7 +1628,9 @@ k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
                 ky[d] = win_tap<T>(g, tab, r.y, d);
             }
             int cb = cell_bits(r.w);
-            const C<T> *base = tile + ((cb >> 20) & 0xfff) * txy + ((cb >> 10) & 0x3ff) * tx + (cb & 0x3ff) + shift;
+            const int c0i = ((cb >> 20) & 0xfff) * txy + ((cb >> 10) & 0x3ff) * tx + (cb & 0x3ff) + shift;
+            if (!IN_BOUNDS(c0i >= 0 && c0i + (KZ - 1) * txy + (KW - 1) * (tx + 1) < txy * g.tz, g.dbg)) continue;
+            const C<T> *base = tile + c0i;
             T ar = 0, ai = 0;
 #pragma unroll 1
             for (int dz = dz0; dz < dz1; ++dz) {
@@ -1646,7 +1677,7 @@ k_interp_t(DevGeom g, const int *__restrict__ bin_start, const int *__restrict__
                     v.x += w.x;
                     v.y += w.y;
                 }
-                vis_store<T>(io, start + m * stride, v);
+                vis_store<T>(io, start + m * stride, v, g.nrow * g.nchan, g.dbg);
             }
         }
         __syncthreads();
@@ -1710,6 +1741,7 @@ __global__ void k_correct_m2d(DevCorr cc, const C<T> *__restrict__ grid, C<T> *_
             val[t] = ix >= 0 && ix < cc.nx && !(sx && r == 0) && iy >= 0 && iy < cc.ny && !(sy && s == 0);
             const int w2 = sx ? cc.nf2 - r : r;
             const int xp = sy ? cc.ny - s : s;               // image column of grid column nf1 - s / s
+            if (val[t] && !IN_BOUNDS(w2 >= 0 && w2 < cc.nf2 && xp >= 0 && xp < cc.ny, cc.dbg)) val[t] = false;
             off[t] = val[t] ? (long long)xp * cc.nf2 + w2 : 0;
         }
         double ar[4] = {0, 0, 0, 0}, ai[4] = {0, 0, 0, 0};
@@ -1768,6 +1800,7 @@ __global__ void k_correct_d2m(DevCorr cc, const C<T> *__restrict__ dirty, C<T> *
             val[t] = ix >= 0 && ix < cc.nx && !(sx && r == 0) && iy >= 0 && iy < cc.ny && !(sy && s == 0);
             const int w2 = sx ? cc.nf2 - r : r;
             const int xp = sy ? cc.ny - s : s;
+            if (val[t] && !IN_BOUNDS(w2 >= 0 && w2 < cc.nf2 && xp >= 0 && xp < cc.ny, cc.dbg)) val[t] = false;
             off[t] = val[t] ? (long long)xp * cc.nf2 + w2 : 0;
             vr[t] = vi[t] = 0;
             if (val[t]) {

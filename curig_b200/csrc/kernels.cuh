@@ -37,6 +37,7 @@ struct DevGeom {
     const int *cbin;               // bin of every sub-problem (set by the binning)
     const int *ccls;               // FP32 tile kernels: per (bin, start-cell residue mod 16) key, the end
                                    // of its run in bin order (the class boundaries of every bin)
+    int *dbg;                      // bounds-checked build: error flags raised by the index checks
     double beta, c;                // ES parameters
     int wkind, wdeg;               // window kind (0 ES, 1 polynomial), degree
     // visibility geometry
@@ -58,9 +59,25 @@ struct DevCorr {
     const double *psi2;            // [nf2/2+1]
     int n3;                        // generic 3-D NUFFT: modes along z (0: w-stacking or 2-D)
     const double *psi3;            // 3-D NUFFT: [nf3/2+1], like psi1 / psi2
+    int *dbg;                      // bounds-checked build: error flags raised by the index checks
 };
 
-enum ErrFlag : int { EF_NONFINITE = 1, EF_RANGE = 2, EF_TIMEOUT = 4 };
+enum ErrFlag : int { EF_NONFINITE = 1, EF_RANGE = 2, EF_TIMEOUT = 4, EF_BOUNDS = 8 };
+
+// Index checks of the bounds-checked build (compiled with -DCURIG_BOUNDS_CHECK,
+// libcurafft_check.so): IN_BOUNDS(cond, flags) raises EF_BOUNDS in *flags and
+// yields false when cond fails, so the guarded access is skipped; the regular
+// build compiles it to true and never evaluates cond.  A debugging aid in
+// place of compute-sanitizer, which is not available on every system.
+#ifdef CURIG_BOUNDS_CHECK
+__device__ __forceinline__ bool bounds_ok(bool ok, int *flags) {
+    if (!ok && flags) atomicOr(flags, EF_BOUNDS);
+    return ok;
+}
+#define IN_BOUNDS(cond, flags) bounds_ok((cond), (flags))
+#else
+#define IN_BOUNDS(cond, flags) true
+#endif
 
 // Piecewise-polynomial window passed by value (kernel-parameter space, so the
 // Horner coefficients are uniform constant operands): c[d][i], interval d,

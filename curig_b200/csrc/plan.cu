@@ -487,7 +487,7 @@ int plan_setpts_geometry(Plan *p, long long nrow, int nchan, const double *du, c
     cc.psx = gp.pixsize_x; cc.psy = gp.pixsize_y; cc.o_center = gp.o_center; cc.i_center = gp.i_center;
     cc.gamma = gp.gamma; cc.h = gp.h; cc.nquad = nq; cc.no_w = gp.no_w;
     cc.qx = p->d_quad; cc.qg = p->d_quad + MAX_QUAD; cc.psi1 = p->d_psi1; cc.psi2 = p->d_psi2;
-    cc.n3 = p->opt.n3; cc.psi3 = p->d_psi3;
+    cc.n3 = p->opt.n3; cc.psi3 = p->d_psi3; cc.dbg = p->d_err;
 
     // 4. fine grid and FFT plans
     size_t gbytes = (size_t)gp.nf1 * gp.nf2 * gp.nf3 * 2 * esize;
@@ -544,6 +544,7 @@ retry_tiles:
 
     DevGeom &g = p->dg;
     g = DevGeom{};
+    g.dbg = p->d_err;                                   // index checks of the bounds-checked build
     g.nf1 = gp.nf1; g.nf2 = gp.nf2; g.nf3 = gp.nf3;
     g.kw = gp.kp.kw; g.hkw = gp.kp.kw / 2;
     g.bx = tg.bx; g.by = tg.by; g.bz = tg.bz; g.nbx = tg.nbx; g.nby = tg.nby; g.nbz = tg.nbz;
@@ -638,6 +639,10 @@ retry_tiles:
     CU_TRY(cudaStreamSynchronize(st));
     CU_TRY(cudaGetLastError());
     if (herr & EF_NONFINITE) return ERR_NONFINITE;
+    if (herr & EF_BOUNDS) {
+        p->last_error = "an index left its buffer (bounds-checked build)";
+        return ERR_GENERIC;
+    }
     if (herr & EF_RANGE) {
         if (p->tg.zpad == 0 && !force_slabs) {          // a w support reached the grid edge: use z slabs
             force_slabs = true;
@@ -939,6 +944,10 @@ int plan_device_status(Plan *p) {
     if (herr & EF_TIMEOUT) {
         p->last_error = "a tile load did not complete (timed out)";
         return ERR_CUDA;
+    }
+    if (herr & EF_BOUNDS) {
+        p->last_error = "an index left its buffer (bounds-checked build)";
+        return ERR_GENERIC;
     }
     return OK;
 }
