@@ -80,6 +80,8 @@ lib.curig_set_timing.argtypes = [c_int]
 lib.curig_set_timing.restype = None
 lib.curig_plan_timings.argtypes = [c_void_p, ctypes.POINTER(c_double), c_int]
 lib.curig_plan_timings.restype = c_int
+lib.curig_plan_status.argtypes = [c_void_p]
+lib.curig_plan_status.restype = c_int
 lib.curig_launch_count.argtypes = []
 lib.curig_launch_count.restype = c_int64
 lib.curig_destroy.argtypes = [c_void_p]

@@ -442,6 +442,13 @@ extern "C" int curig_plan_timings(curig_plan h, double *out, int n) {
 
 extern "C" int64_t curig_launch_count(void) { return launch_count(); }
 
+extern "C" int curig_plan_status(curig_plan h) {
+    if (!h) return fail(ERR_ARG, "null plan");
+    const int s = plan_device_status(h->p);
+    if (s != OK) return fail(s, h->p->last_error.empty() ? "device status" : h->p->last_error);
+    return OK;
+}
+
 extern "C" void curig_test_tile_wait(int64_t polls, int noissue) { set_tile_wait(polls, noissue); }
 
 extern "C" int curig_destroy(curig_plan h) {

@@ -20,10 +20,21 @@ namespace curig {
 // cudaMallocAsync whose failure is reported by its return value only: the
 // runtime's last-error state is cleared again, so the launch checks
 // (cudaGetLastError) of this or a later call do not report the failed
-// allocation a second time.
+// allocation a second time.  After an out-of-memory failure the device's
+// default pool is trimmed: a request larger than the device can leave the
+// pool holding what it mapped before giving up (the pool keeps freed memory,
+// its release threshold being raised), which other processes then lack.
 inline cudaError_t alloc_async(void **ptr, size_t bytes, cudaStream_t st) {
     const cudaError_t e = cudaMallocAsync(ptr, bytes, st);
-    if (e != cudaSuccess) (void)cudaGetLastError();
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        int dev = 0;
+        cudaMemPool_t pool;
+        if (e == cudaErrorMemoryAllocation && cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess)
+            cudaMemPoolTrimTo(pool, 0);
+        (void)cudaGetLastError();
+    }
     return e;
 }
 

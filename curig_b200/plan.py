@@ -86,6 +86,13 @@ class GridderPlan:
         _lib.check(_lib.lib.curig_execute_dir(self._h, int(kind), _lib.ptr(vis), _lib.ptr(wgt),
                                               _lib.ptr(dirty)), "execute")
 
+    def status(self) -> None:
+        """Wait for the plan's stream and raise CurigError if its kernels flagged
+        a failure since set points (an interpolator tile load that did not
+        complete within its bounded wait, or an index check of the
+        bounds-checked build)."""
+        _lib.check(_lib.lib.curig_plan_status(self._h), "plan_status")
+
     def timings(self) -> dict:
         """Stage durations (ms) of the last setpts / executes (needs set_timing(True))."""
         out = (ctypes.c_double * 11)()

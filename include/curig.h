@@ -215,6 +215,15 @@ void curig_set_timing(int on);
 int curig_plan_timings(curig_plan plan, double *out, int n);
 int64_t curig_launch_count(void);
 
+/* Flags the plan's kernels raised since its points were set: waits for the
+ * plan's stream and returns 0, or 4 (CUDA) when an interpolator tile load did
+ * not complete within its bounded wait, or 1 when an index check of the
+ * bounds-checked build failed (curig_last_error says which).  The one-shot
+ * calls check this themselves; the plan API leaves it to the caller, so that
+ * execute stays asynchronous.  No counterpart in the reference (its kernels
+ * report nothing). */
+int curig_plan_status(curig_plan plan);
+
 /* Test hook for the interpolator's bounded wait on its TMA tile loads: plans
  * whose points are set after this call poll a load's barrier at most `polls`
  * times (<= 0: the default, about a second) before raising the error that the
