@@ -254,6 +254,13 @@ __global__ void k_chunk_bins(long long nb, const int *__restrict__ sub_end, int 
     }
 }
 
+// Chunks larger than CLS_SUB (the one-word FP32 tiles) also keep every start-
+// cell residue class at <= CLS_SUB visibilities per chunk: a bin whose
+// visibilities crowd into a few cells (one class) is cut as if the chunk size
+// were CLS_SUB, so that its tile's box bound, and with it the rounding step of
+// the one-word fixed point, stays that of a CLS_SUB chunk.
+constexpr int CLS_SUB = 4096;
+
 __global__ void k_bins_from_keys(const int *__restrict__ kstart, const int *__restrict__ total, long long nb,
                                  int cbits, int sub, int *__restrict__ bin_start, int *__restrict__ bin_count,
                                  int *__restrict__ nsub, int *__restrict__ bcur) {
@@ -264,7 +271,17 @@ __global__ void k_bins_from_keys(const int *__restrict__ kstart, const int *__re
         bin_start[b] = s;
         bcur[b] = s;
         bin_count[b] = e - s;
-        nsub[b] = (e - s + sub - 1) / sub;
+        int ns = (e - s + sub - 1) / sub;
+        if (sub > CLS_SUB && cbits > 0) {
+            const int nq = 1 << cbits;
+            int big = 0;
+            for (int q = 0; q < nq; ++q) {
+                const int a = kstart[(b << cbits) + q], z = q + 1 < nq ? kstart[(b << cbits) + q + 1] : e;
+                big = max(big, z - a);
+            }
+            ns = max(ns, (big + CLS_SUB - 1) / CLS_SUB);
+        }
+        nsub[b] = ns;
     }
 }
 
@@ -671,8 +688,12 @@ __device__ __forceinline__ void sub_range(const DevGeom &g, const int *bin_start
         return;
     }
     int cnt = bin_count[b];
-    int nsb = (cnt + g.sub - 1) / g.sub;
+    int nsb = sub_end[b] - (b ? sub_end[b - 1] : 0);   // the binning's chunk count (cnt / sub or more)
     int j = s - (sub_end[b] - nsb);
+    if (!IN_BOUNDS(nsb >= 1 && j >= 0 && j < nsb, g.dbg)) {
+        start = 0; stride = 1; n = 0;
+        return;
+    }
     start = bin_start[b] + j;
     stride = nsb;
     n = (cnt - j + nsb - 1) / nsb;
@@ -704,13 +725,16 @@ __device__ __forceinline__ void split_fix(float x, int &h, int &l) {
 // One-word fixed point: each term x * q is rounded to an integer by one FMA
 // against 1.5 * 2^23 (valid for |x q| <= 2^22) and added with one int32 atomic
 // per component.  A cell (x, y, z) receives only from visibilities whose start
-// column lies in the kw x kw box ending at (x, y); B = max over cells of the
-// sum of max(|re c|, |im c|) over that box bounds every cell sum by B wmax3.
-// The chunk's scale q = 2^k takes the largest k with max|c| wmax3 q <= 2^22
-// and B wmax3 q <= 2^30, so no cell sum (at most B wmax3 q + n/2 < 2^31)
-// overflows; a term's rounding error is at most 2^-23 of max|c| wmax3, unless
-// the box bound binds (more than about 250 visibilities of the largest
-// magnitude in one box).
+// column lies in the kw x kw box ending at (x, y), a visibility starting at
+// (x - dx, y - dy) with a term of at most max(|re c|, |im c|) wenv[dx]
+// wenv[dy] wzmax (wenv[d]: bound on tap d's window value over all offsets, a
+// few percent of the peak at the edge taps); B = max over cells of the sum of
+// max(|re c|, |im c|) wenv[dx] wenv[dy] over that box bounds every cell sum by
+// B wzmax.  The chunk's scale q = 2^k takes the largest k with max|c| wmax3 q
+// <= 2^22 and B wzmax q <= 2^30, so no cell sum (at most B wzmax q + n/2 <
+// 2^31) overflows; a term's rounding error is at most 2^-23 of max|c| wmax3,
+// unless the box bound binds (for the ES window of width 6, more than about
+// 1000 visibilities of the largest magnitude in one box).
 __device__ __forceinline__ int round_fix(float a, float k) {
     return __float_as_int(fmaf(a, k, 12582912.0f)) - 0x4B400000;
 }
@@ -1322,17 +1346,19 @@ k_spread_f32(DevGeom g, const int *__restrict__ bin_start, const int *__restrict
                 int e = m > 0.f ? ilogb(m) + 1 : 0;       // 2^(e-1) <= m < 2^e
                 k = FIX_BITS - e;
             } else {
-                // largest kw x kw box sum of the start-column sums: sums of
-                // kw rows of each column into the first txy words of the
-                // zeroed tile, then sums of kw of those along each row (every
-                // thread a few cells); the borrowed words are zeroed again
+                // largest kw x kw box sum of the start-column sums, each
+                // start column weighted by the bound on the taps it gives the
+                // cell (wenv[dy] wenv[dx]): weighted sums of kw rows of each
+                // column into the first txy words of the zeroed tile, then of
+                // kw of those along each row (every thread a few cells); the
+                // borrowed words are zeroed again
                 float *vs = reinterpret_cast<float *>(wA);
                 for (int e = threadIdx.x; e < txy; e += TTHREADS) {
                     const int y = e / tx, x = e - y * tx;
                     float a = 0.f;
 #pragma unroll
                     for (int d = 0; d < KW; ++d)
-                        if (y - d >= 0) a += colsum[(y - d) * tx + x];
+                        if (y - d >= 0) a = fmaf(g.wenv[d], colsum[(y - d) * tx + x], a);
                     vs[e] = a;
                 }
                 __syncthreads();
@@ -1342,7 +1368,7 @@ k_spread_f32(DevGeom g, const int *__restrict__ bin_start, const int *__restrict
                     float a = 0.f;
 #pragma unroll
                     for (int d = 0; d < KW; ++d)
-                        if (x - d >= 0) a += vs[y * tx + x - d];
+                        if (x - d >= 0) a = fmaf(g.wenv[d], vs[y * tx + x - d], a);
                     bmax = fmaxf(bmax, a);
                 }
                 __syncthreads();                          // every read of vs is done
@@ -1355,7 +1381,7 @@ k_spread_f32(DevGeom g, const int *__restrict__ bin_start, const int *__restrict
 #pragma unroll
                 for (int w = 0; w < TWARPS; ++w) bb = fmaxf(bb, redbuf[w]);
                 const int em = m > 0.f ? ilogb(m * g.wmax3) + 1 : 0;
-                const int es = bb > 0.f ? ilogb(bb * g.wmax3) + 1 : 0;
+                const int es = bb > 0.f ? ilogb(bb * g.wzmax) + 1 : 0;
                 k = min(22 - em, 30 - es);
             }
             k = min(k, 120);

@@ -11,6 +11,10 @@ template <typename T> struct cplx_t;
 template <> struct cplx_t<float> { using type = float2; };
 template <> struct cplx_t<double> { using type = double2; };
 
+// Tabulated windows (piecewise polynomials, see WinTab): widths up to TAB_KW,
+// TAB_DEG coefficients per tap (degree 11).
+constexpr int TAB_KW = 12, TAB_DEG = 12;
+
 // Everything a binning / spreading / interpolation launch needs, by value.
 struct DevGeom {
     int nf1, nf2, nf3;
@@ -30,6 +34,8 @@ struct DevGeom {
     int tma_test_noissue;          // test only: arm the barrier but issue no load (the wait runs out)
     int no_w;                      // w ignored: one plane, no z taps (window factor 1)
     float wmax3;                   // bound on |kx ky kz| of the tabulated window
+    float wenv[TAB_KW];            // bound on |k(d)| of tap d over all offsets (one-word box bound)
+    float wzmax;                   // bound on |kz| (1 without w)
     long long nbins;               // bins of all row slabs: nslab * nbins_slab
     long long nbins_slab;          // bins of one row slab (nbx * nby * nbz)
     int nslab;                     // row slabs (sort key major part; 1 = none)
@@ -82,7 +88,6 @@ __device__ __forceinline__ bool bounds_ok(bool ok, int *flags) {
 // Piecewise-polynomial window passed by value (kernel-parameter space, so the
 // Horner coefficients are uniform constant operands): c[d][i], interval d,
 // highest power first.  Used by the thread-per-visibility kernels (kw <= 12).
-constexpr int TAB_KW = 12, TAB_DEG = 12;   // degree 11
 template <typename T> struct WinTab {
     T c[TAB_KW][TAB_DEG];
 };

@@ -226,11 +226,14 @@ def test_fixed_point_accumulation_matches_float(C, precision):
     assert l2err(d0, d2) < (2e-6 if precision == "fp32" else 1e-12)
 
 
-@pytest.mark.parametrize("sub,tol", [(0, 3e-6), (4096, 3e-6), (256, 3e-6)])
+@pytest.mark.parametrize("sub,tol", [(0, 3e-6), (4096, 3e-6), (256, 3e-6), (16384, 3e-6), (65536, 8e-6)])
 def test_one_word_fixed_point_matches_exact(C, sub, tol):
     """One-word int32 tile accumulation (22-bit terms) against the exact two-word
-    one on a dense case (up to 4096 visibilities per chunk in a few cells):
-    nothing may overflow and the error stays at the 22-bit rounding level."""
+    one on a dense case (about 4e5 visibilities in a few bins, chunks of up to
+    the chunk size; 0 = the default, 16384 for one-word tiles): nothing may
+    overflow and the error stays at the 22-bit rounding level.  A requested
+    chunk of 65536 puts a whole bin in one chunk; its box bound binds and the
+    rounding step grows with it."""
     freq, uvw, ms, wgt = disk_inputs(200000, 2, 64, 2.0, max_pix=24, wmax=300)
     psx = 2.0 * np.pi / 180 / 64
     d0, _ = _plan_run(1, 64, 64, psx, psx, 1e-6, 1, uvw, freq, vis=ms, wgt=wgt, precision="fp32",
@@ -240,11 +243,15 @@ def test_one_word_fixed_point_matches_exact(C, sub, tol):
     assert l2err(d0, d1) < tol
 
 
-def test_one_word_fixed_point_all_in_one_cell(C):
-    """Every visibility of a 4096-visibility chunk at the same uv point: the box
-    bound must scale the chunk so that no int32 cell sum overflows."""
+@pytest.mark.parametrize("n", [4000, 16000])
+def test_one_word_fixed_point_all_in_one_cell(C, n):
+    """Every visibility at the same uv point (4000; 16000, one bin below the
+    one-word chunk size of 16384, which the binning still cuts into chunks of at
+    most 4096 because they all share one start-cell residue class): the box
+    bound must scale each chunk so that no int32 cell sum overflows, and the
+    rounding error (growing with the visibilities per chunk) stays below
+    epsilon."""
     rng = np.random.default_rng(7)
-    n = 4000
     uvw = np.tile(np.array([[120.0, -80.0, 15.0]]), (n, 1))
     freq = np.array([1.0e9])
     ms = (rng.standard_normal((n, 1)) + 1j * rng.standard_normal((n, 1))).astype(np.complex128)
