@@ -435,6 +435,33 @@ __global__ void k_records(DevGeom g, const double *__restrict__ uu, const double
     }
 }
 
+// vw = vis * wgt in input order (coalesced): the gather below then reads one
+// random 8- or 16-byte element per visibility instead of two (vis and wgt
+// live in different arrays, each random read costing a whole DRAM burst).
+template <typename T>
+__global__ void k_vis_weight(long long n, const C<T> *__restrict__ vis, const T *__restrict__ wgt,
+                             C<T> *__restrict__ vw) {
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+         k += (long long)gridDim.x * blockDim.x) {
+        const C<T> v = vis[k];
+        const T wt = wgt[k];
+        vw[k] = C<T>{v.x * wt, v.y * wt};
+    }
+}
+
+// vis *= wgt in input order (coalesced), after the interpolator's scatter has
+// written vis[j] = value e^{-i o_c w}: the scatter then reads no weight at
+// random.  (value e^{-i o_c w}) wgt is the product the scatter formed itself.
+template <typename T>
+__global__ void k_vis_scale(long long n, C<T> *__restrict__ vis, const T *__restrict__ wgt) {
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+         k += (long long)gridDim.x * blockDim.x) {
+        const C<T> v = vis[k];
+        const T wt = wgt[k];
+        vis[k] = C<T>{v.x * wt, v.y * wt};
+    }
+}
+
 // c = vis * wgt * e^{i o_c w} gathered into bin order (ra_exec.cu:98-104).
 template <typename T>
 __global__ void k_vis_prep(long long M, const int *__restrict__ idx, const C<T> *__restrict__ ph,
@@ -2072,12 +2099,28 @@ void launch_records(const DevGeom &g, const double *u, const double *v, const do
 }
 
 template <typename T>
-void launch_vis_prep(long long M, const int *idx, const void *ph, const void *vis, const void *wgt, void *cs,
-                     cudaStream_t st) {
+void launch_vis_scale(long long i0, long long n, void *vis, const void *wgt, cudaStream_t st) {
+    if (n <= 0 || !wgt) return;
     count_launch();
-    k_vis_prep<T><<<grid_for(M), NTHREADS, 0, st>>>(M, idx, reinterpret_cast<const C<T> *>(ph),
-                                                    reinterpret_cast<const C<T> *>(vis),
-                                                    reinterpret_cast<const T *>(wgt), reinterpret_cast<C<T> *>(cs));
+    k_vis_scale<T><<<grid_for(n), NTHREADS, 0, st>>>(n, reinterpret_cast<C<T> *>(vis) + i0,
+                                                     reinterpret_cast<const T *>(wgt) + i0);
+}
+
+template <typename T>
+void launch_vis_prep(long long i0, long long n, const int *idx, const void *ph, const void *vis, const void *wgt,
+                     void *vw, void *cs, cudaStream_t st) {
+    if (n <= 0) return;
+    const C<T> *src = reinterpret_cast<const C<T> *>(vis);
+    const T *w = reinterpret_cast<const T *>(wgt);
+    if (w && vw) {                 // weights applied in input order first
+        count_launch();
+        k_vis_weight<T><<<grid_for(n), NTHREADS, 0, st>>>(n, src + i0, w + i0, reinterpret_cast<C<T> *>(vw) + i0);
+        src = reinterpret_cast<const C<T> *>(vw);
+        w = nullptr;
+    }
+    count_launch();
+    k_vis_prep<T><<<grid_for(n), NTHREADS, 0, st>>>(n, idx + i0, reinterpret_cast<const C<T> *>(ph) + i0, src, w,
+                                                    reinterpret_cast<C<T> *>(cs) + i0);
 }
 
 template <typename T>
@@ -2286,8 +2329,9 @@ void launch_zero_tpad(int nx, int ny, int nf2, int nf3, void *t, cudaStream_t st
     template void launch_records<T>(const DevGeom &, const double *, const double *, const double *,  \
                                     const double *, const int *, long long, int *, void *, void *,    \
                                     int *, cudaStream_t);                                             \
-    template void launch_vis_prep<T>(long long, const int *, const void *, const void *, const void *,\
-                                     void *, cudaStream_t);                                           \
+    template void launch_vis_prep<T>(long long, long long, const int *, const void *, const void *,    \
+                                     const void *, void *, void *, cudaStream_t);                     \
+    template void launch_vis_scale<T>(long long, long long, void *, const void *, cudaStream_t);      \
     template void launch_vis_out<T>(long long, const int *, const void *, const void *, const void *, \
                                     void *, cudaStream_t);                                            \
     template int launch_spread<T>(const DevGeom &, size_t, const int *, const int *, const int *,     \

@@ -812,7 +812,10 @@ static int execute_t(Plan *p, int type, void *d_vis, const void *d_wgt, void *d_
     int s;
     if (type == 1) {
         mark(p, EV_M2D_BEGIN);
-        launch_vis_prep<T>(M, p->d_idx, p->d_ph, d_vis, d_wgt, p->d_cs, st);
+        void *vw = nullptr;                       // vis * wgt in input order (the pool's memory)
+        if (d_wgt && dalloc(&vw, (size_t)M * 2 * sizeof(T), st) != cudaSuccess) vw = nullptr;
+        launch_vis_prep<T>(0, M, p->d_idx, p->d_ph, d_vis, d_wgt, vw, p->d_cs, st);
+        dfree(vw, st);
         mark(p, EV_M2D_PREP);
         CU_TRY(cudaMemsetAsync(p->d_grid, 0, gbytes, st));
         mark(p, EV_M2D_ZERO);
@@ -837,13 +840,14 @@ static int execute_t(Plan *p, int type, void *d_vis, const void *d_wgt, void *d_
         s = plane_fft<T>(p, CUFFT_FORWARD, false);   // -1
         if (s) return s;
         mark(p, EV_D2M_FFT);
-        const VisIO io{p->d_idx, p->d_ph, d_wgt, d_vis};
+        const VisIO io{p->d_idx, p->d_ph, nullptr, d_vis};   // weights applied after the scatter
         s = launch_interp<T>(g, p->smem_interp, p->d_bin_start, p->d_bin_count, p->d_sub_end, p->d_rec, p->d_grid,
                              p->d_cs, p->d_wcoef, p->htab.empty() ? nullptr : p->htab.data(), io, M, &p->tmap,
                              p->d_err, p->nsm, st);
         if (s) return s;
-        mark(p, EV_D2M_INTERP);
-        mark(p, EV_D2M_END);                     // the scatter runs inside the interpolator
+        mark(p, EV_D2M_INTERP);                  // the scatter runs inside the interpolator
+        launch_vis_scale<T>(0, M, d_vis, d_wgt, st);
+        mark(p, EV_D2M_END);
     }
     CU_TRY(cudaGetLastError());
     return OK;
@@ -887,18 +891,24 @@ static int execute_slabs_t(Plan *p, int type, void *d_vis, const void *d_wgt, vo
     if (type == 1) {
         const size_t gbytes = (size_t)gp.nf1 * gp.nf2 * gp.nf3 * 2 * sizeof(T);
         CU_TRY(cudaMemsetAsync(p->d_grid, 0, gbytes, st));
+        void *vw = nullptr;                       // vis * wgt in input order (the pool's memory)
+        if (d_wgt && dalloc(&vw, (size_t)p->nrow * p->nchan * 2 * sizeof(T), st) != cudaSuccess) vw = nullptr;
         for (int k = 0; k < ns; ++k) {
-            CU_TRY(wait_slab(k));
+            if (cudaError_t e = wait_slab(k)) {
+                dfree(vw, st);
+                CU_TRY(e);
+            }
             const long long i0 = p->slab_row[k] * p->nchan, i1 = p->slab_row[k + 1] * p->nchan;
-            if (i1 > i0)
-                launch_vis_prep<T>(i1 - i0, p->d_idx + i0, static_cast<const char *>(p->d_ph) + i0 * 2 * sizeof(T),
-                                   d_vis, d_wgt, static_cast<char *>(p->d_cs) + i0 * 2 * sizeof(T), st);
+            launch_vis_prep<T>(i0, i1 - i0, p->d_idx, p->d_ph, d_vis, d_wgt, vw, p->d_cs, st);
             DevGeom gk;
             if (slab_geom(k, gk) &&
                 (s = launch_spread<T>(gk, p->smem, p->d_bin_start, p->d_bin_count, p->d_sub_end, p->d_rec, p->d_cs,
-                                      p->d_grid, p->d_wcoef, ht, io, p->nrow * p->nchan, p->nsm, st)))
+                                      p->d_grid, p->d_wcoef, ht, io, p->nrow * p->nchan, p->nsm, st))) {
+                dfree(vw, st);
                 return s;
+            }
         }
+        dfree(vw, st);
         if ((s = plane_fft<T>(p, CUFFT_INVERSE, true))) return s;
         launch_correct_m2d<T>(p->dc, p->d_tgrid, d_dirty, st);
     } else {
@@ -907,14 +917,17 @@ static int execute_slabs_t(Plan *p, int type, void *d_vis, const void *d_wgt, vo
             launch_correct_d2m<T>(p->dc, d_dirty, p->d_tgrid, st);
             if ((s = plane_fft<T>(p, CUFFT_FORWARD, false))) return s;
         }
+        const VisIO io_out{p->d_idx, p->d_ph, nullptr, d_vis};   // weights applied after the scatter
         for (int k = 0; k < ns; ++k) {
             CU_TRY(wait_slab(k));
             DevGeom gk;
             if (slab_geom(k, gk) &&
                 (s = launch_interp<T>(gk, p->smem_interp, p->d_bin_start, p->d_bin_count, p->d_sub_end, p->d_rec,
-                                      p->d_grid, p->d_cs, p->d_wcoef, ht, io, p->nrow * p->nchan, &p->tmap,
+                                      p->d_grid, p->d_cs, p->d_wcoef, ht, io_out, p->nrow * p->nchan, &p->tmap,
                                       p->d_err, p->nsm, st)))
                 return s;
+            const long long i0 = p->slab_row[k] * p->nchan, i1 = p->slab_row[k + 1] * p->nchan;
+            launch_vis_scale<T>(i0, i1 - i0, d_vis, d_wgt, st);
             CU_TRY(done_slab(k));
         }
     }

@@ -175,9 +175,17 @@ size_t tile_smem_bytes(const TileGeom &tg, int esize, int kw, int wdeg);
 template <typename T>
 void launch_records(const DevGeom &g, const double *u, const double *v, const double *w, const double *foc,
                     const int *tmp, long long M, int *kcur, void *rec, void *ph, int *idx, cudaStream_t st);
+// cs[i] = vis[j] wgt[j] e^{i o_c w} for sorted positions i in [i0, i0 + n), j = idx[i]
+// (the input indices of the positions [i0, i0 + n) are [i0, i0 + n) too); with
+// weights and a scratch vw of every visibility, vis * wgt is formed in input
+// order first and the gather reads one array.
+// vis[j] *= wgt[j] for j in [i0, i0 + n) (nothing without weights): the weights
+// of dirty2ms, applied after the interpolator's unweighted scatter.
 template <typename T>
-void launch_vis_prep(long long M, const int *idx, const void *ph, const void *vis, const void *wgt, void *cs,
-                     cudaStream_t st);
+void launch_vis_scale(long long i0, long long n, void *vis, const void *wgt, cudaStream_t st);
+template <typename T>
+void launch_vis_prep(long long i0, long long n, const int *idx, const void *ph, const void *vis, const void *wgt,
+                     void *vw, void *cs, cudaStream_t st);
 template <typename T>
 void launch_vis_out(long long M, const int *idx, const void *ph, const void *os, const void *wgt, void *vis,
                     cudaStream_t st);
