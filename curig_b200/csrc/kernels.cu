@@ -1951,47 +1951,75 @@ __device__ __forceinline__ int image_col(int x, int ny, int nf1) {
     return x < ny - ny / 2 ? x : (x >= nf1 - ny / 2 ? x - nf1 + ny : -1);
 }
 
-// T[z][x'][y] = grid[z][y][grid_col(x')]: 32 x 32 tiles through shared memory,
-// reads along x, writes along y (both coalesced).  Grid: (ny/32, nf2/32, nf3).
+// Transposes between the grid and T through shared memory: tiles of 32
+// columns x tt_y rows, 256 threads, each thread tt_y / 8 loads in flight before
+// the tile's barrier; reads and writes along the contiguous axis (coalesced).
+// 64 rows for 8-byte elements (17 KB tiles); 32 for 16-byte ones, whose 64-row
+// tiles (34 KB) measured slower (fewer CTAs per SM).
+template <typename T> constexpr int tt_y() { return sizeof(T) == 4 ? 64 : 32; }
+
+// T[z][x'][y] = grid[z][y][grid_col(x')].  Grid: (ny/32, nf2/tt_y, nf3).
 template <typename T>
 __global__ void __launch_bounds__(256) k_cols_to_t(int ny, int nf1, int nf2, const C<T> *__restrict__ grid,
                                                    C<T> *__restrict__ t) {
-    __shared__ C<T> tile[32][33];
-    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+    constexpr int TT_Y = tt_y<T>();
+    __shared__ C<T> tile[TT_Y][33];
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * TT_Y;
     const C<T> *gp = grid + (long long)blockIdx.z * nf1 * nf2;
     C<T> *tp = t + (long long)blockIdx.z * ny * nf2;
     const int xp = x0 + threadIdx.x;
     const int gx = xp < ny ? grid_col(xp, ny, nf1) : 0;
-    for (int j = threadIdx.y; j < 32; j += 8) {
+#pragma unroll
+    for (int j = threadIdx.y; j < TT_Y; j += 8) {
         const int y = y0 + j;
         if (xp < ny && y < nf2) tile[j][threadIdx.x] = gp[(long long)y * nf1 + gx];
     }
     __syncthreads();
-    const int y = y0 + threadIdx.x;
+#pragma unroll
     for (int j = threadIdx.y; j < 32; j += 8) {
         const int xq = x0 + j;
-        if (xq < ny && y < nf2) tp[(long long)xq * nf2 + y] = tile[threadIdx.x][j];
+#pragma unroll
+        for (int h = 0; h < TT_Y; h += 32) {
+            const int y = y0 + h + threadIdx.x;
+            if (xq < ny && y < nf2) tp[(long long)xq * nf2 + y] = tile[h + threadIdx.x][j];
+        }
     }
 }
 
-// grid[z][y][x] = T[z][image_col(x)][y] for the image's columns, 0 elsewhere.
-// Grid: (nf1/32, nf2/32, nf3).
+// grid[z][y][x] = T[z][image_col(x)][y] for the image's columns, 0 elsewhere
+// (tiles of columns outside the image are written as zeros directly).
+// Grid: (nf1/32, nf2/tt_y, nf3).
 template <typename T>
 __global__ void __launch_bounds__(256) k_t_to_grid(int ny, int nf1, int nf2, const C<T> *__restrict__ t,
                                                    C<T> *__restrict__ grid) {
-    __shared__ C<T> tile[32][33];
-    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+    constexpr int TT_Y = tt_y<T>();
+    __shared__ C<T> tile[32][TT_Y + 1];
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * TT_Y;
     C<T> *gp = grid + (long long)blockIdx.z * nf1 * nf2;
     const C<T> *tp = t + (long long)blockIdx.z * ny * nf2;
-    const int y = y0 + threadIdx.x;
+    const int x = x0 + threadIdx.x;
+    // no image column in [x0, x0 + 32): image columns are x < ny - ny/2 and x >= nf1 - ny/2
+    if (x0 >= ny - ny / 2 && x0 + 32 <= nf1 - ny / 2) {
+#pragma unroll
+        for (int j = threadIdx.y; j < TT_Y; j += 8) {
+            const int yy = y0 + j;
+            if (x < nf1 && yy < nf2) gp[(long long)yy * nf1 + x] = C<T>{0, 0};
+        }
+        return;
+    }
+#pragma unroll
     for (int j = threadIdx.y; j < 32; j += 8) {
-        const int x = x0 + j;
-        const int xp = x < nf1 ? image_col(x, ny, nf1) : -1;
-        tile[j][threadIdx.x] = (xp >= 0 && y < nf2) ? tp[(long long)xp * nf2 + y] : C<T>{0, 0};
+        const int xj = x0 + j;
+        const int xp = xj < nf1 ? image_col(xj, ny, nf1) : -1;
+#pragma unroll
+        for (int h = 0; h < TT_Y; h += 32) {
+            const int y = y0 + h + threadIdx.x;
+            tile[j][h + threadIdx.x] = (xp >= 0 && y < nf2) ? tp[(long long)xp * nf2 + y] : C<T>{0, 0};
+        }
     }
     __syncthreads();
-    const int x = x0 + threadIdx.x;
-    for (int j = threadIdx.y; j < 32; j += 8) {
+#pragma unroll
+    for (int j = threadIdx.y; j < TT_Y; j += 8) {
         const int yy = y0 + j;
         if (x < nf1 && yy < nf2) gp[(long long)yy * nf1 + x] = tile[threadIdx.x][j];
     }
@@ -2251,7 +2279,7 @@ void launch_correct3_d2m(const DevCorr &cc, const void *fk, void *tgrid, cudaStr
 template <typename T>
 void launch_cols_to_t(int ny, int nf1, int nf2, int nf3, const void *grid, void *t, cudaStream_t st) {
     count_launch();
-    dim3 g((ny + 31) / 32, (nf2 + 31) / 32, nf3);
+    dim3 g((ny + 31) / 32, (nf2 + tt_y<T>() - 1) / tt_y<T>(), nf3);
     k_cols_to_t<T><<<g, dim3(32, 8), 0, st>>>(ny, nf1, nf2, reinterpret_cast<const C<T> *>(grid),
                                               reinterpret_cast<C<T> *>(t));
 }
@@ -2259,7 +2287,7 @@ void launch_cols_to_t(int ny, int nf1, int nf2, int nf3, const void *grid, void 
 template <typename T>
 void launch_t_to_grid(int ny, int nf1, int nf2, int nf3, const void *t, void *grid, cudaStream_t st) {
     count_launch();
-    dim3 g((nf1 + 31) / 32, (nf2 + 31) / 32, nf3);
+    dim3 g((nf1 + 31) / 32, (nf2 + tt_y<T>() - 1) / tt_y<T>(), nf3);
     k_t_to_grid<T><<<g, dim3(32, 8), 0, st>>>(ny, nf1, nf2, reinterpret_cast<const C<T> *>(t),
                                               reinterpret_cast<C<T> *>(grid));
 }
