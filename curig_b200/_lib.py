@@ -137,6 +137,8 @@ lib.curig_nufft_info3.argtypes = [c_void_p, ctypes.POINTER(c_int), ctypes.POINTE
 lib.curig_nufft_info3.restype = c_int
 lib.curig_test_tile_wait.argtypes = [c_int64, c_int]
 lib.curig_test_tile_wait.restype = None
+lib.curig_test_gather_scratch.argtypes = [c_int]
+lib.curig_test_gather_scratch.restype = None
 
 ERRORS = {
     1: "generic error", 2: "bad upsampling factor", 3: "invalid argument", 4: "CUDA error",

@@ -451,6 +451,8 @@ extern "C" int curig_plan_status(curig_plan h) {
 
 extern "C" void curig_test_tile_wait(int64_t polls, int noissue) { set_tile_wait(polls, noissue); }
 
+extern "C" void curig_test_gather_scratch(int on) { set_gather_scratch(on); }
+
 extern "C" int curig_destroy(curig_plan h) {
     if (!h) return OK;
     plan_destroy(h->p);

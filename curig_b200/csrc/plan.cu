@@ -245,6 +245,23 @@ void set_tile_wait(long long polls, int noissue) {
     g_tma_noissue.store(noissue ? 1 : 0);
 }
 
+// ms2dirty's weighted gather takes a scratch vis * wgt from the pool, or, when
+// that allocation fails (or a test turns the scratch off), gathers vis and wgt
+// in one pass.
+namespace {
+std::atomic<int> g_gather_scratch{1};
+}
+
+void set_gather_scratch(int on) { g_gather_scratch.store(on ? 1 : 0); }
+
+template <typename T>
+static void *gather_scratch(const void *d_wgt, long long M, cudaStream_t st) {
+    void *vw = nullptr;
+    if (d_wgt && g_gather_scratch.load() && dalloc(&vw, (size_t)M * 2 * sizeof(T), st) != cudaSuccess)
+        vw = nullptr;
+    return vw;
+}
+
 // ------------------------------------------------------------------ plan
 int plan_create(int type, int nx, int ny, double psx, double psy, double eps, double sigma, int sign,
                 const Options &opt, Plan **out) {
@@ -812,8 +829,7 @@ static int execute_t(Plan *p, int type, void *d_vis, const void *d_wgt, void *d_
     int s;
     if (type == 1) {
         mark(p, EV_M2D_BEGIN);
-        void *vw = nullptr;                       // vis * wgt in input order (the pool's memory)
-        if (d_wgt && dalloc(&vw, (size_t)M * 2 * sizeof(T), st) != cudaSuccess) vw = nullptr;
+        void *vw = gather_scratch<T>(d_wgt, M, st);   // vis * wgt in input order (the pool's memory)
         launch_vis_prep<T>(0, M, p->d_idx, p->d_ph, d_vis, d_wgt, vw, p->d_cs, st);
         dfree(vw, st);
         mark(p, EV_M2D_PREP);
@@ -891,8 +907,7 @@ static int execute_slabs_t(Plan *p, int type, void *d_vis, const void *d_wgt, vo
     if (type == 1) {
         const size_t gbytes = (size_t)gp.nf1 * gp.nf2 * gp.nf3 * 2 * sizeof(T);
         CU_TRY(cudaMemsetAsync(p->d_grid, 0, gbytes, st));
-        void *vw = nullptr;                       // vis * wgt in input order (the pool's memory)
-        if (d_wgt && dalloc(&vw, (size_t)p->nrow * p->nchan * 2 * sizeof(T), st) != cudaSuccess) vw = nullptr;
+        void *vw = gather_scratch<T>(d_wgt, p->nrow * p->nchan, st);   // vis * wgt in input order
         for (int k = 0; k < ns; ++k) {
             if (cudaError_t e = wait_slab(k)) {
                 dfree(vw, st);

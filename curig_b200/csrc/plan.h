@@ -227,6 +227,9 @@ int plan_device_status(Plan *p);
 // tile loads not happen, for tests of the timeout path.
 constexpr long long DEFAULT_TMA_POLLS = 1LL << 26;
 void set_tile_wait(long long polls, int noissue);
+// on = 0: ms2dirty gathers vis and wgt in one pass (no vis * wgt scratch), as
+// when the scratch cannot be allocated; tests compare the two paths
+void set_gather_scratch(int on);
 // destroy the cached cuFFT handles no plan holds (returns how many); number cached
 int fft_cache_trim();
 int fft_cache_size();

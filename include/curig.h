@@ -233,6 +233,14 @@ int curig_plan_status(curig_plan plan);
  * counterpart in the reference, which has no bounded waits. */
 void curig_test_tile_wait(int64_t polls, int noissue);
 
+/* Test hook for ms2dirty's weighted gather: with on = 0 the visibilities and
+ * weights are gathered into bin order in one pass, the path taken when the
+ * vis * wgt scratch (one complex value per visibility, from the device's
+ * stream-ordered pool) cannot be allocated; on = 1 (the default) forms vis * wgt
+ * in input order first.  The two differ only in the rounding order of the
+ * products.  No counterpart in the reference. */
+void curig_test_gather_scratch(int on);
+
 /* Generic NUFFT, types 1 (points -> modes) and 2 (modes -> points) in one or two
  * dimensions, on the w-free gridder (same kernel-width, grid-size and correction
  * rules as the gridder; takes the place of the reference's cunufft_setting /

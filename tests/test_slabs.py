@@ -153,3 +153,30 @@ def test_slabs_on_a_caller_stream_and_from_several_threads():
         t.join()
     for (d1, v1), (d3, v3) in zip(seq, par):
         assert l2err(d1, d3) < 1e-12 and l2err(v1, v3) < 1e-12
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-14), ("fp32", 2e-6)])
+@pytest.mark.parametrize("slabs", [1, 3])
+def test_weighted_gather_with_and_without_scratch(precision, tol, slabs):
+    """ms2dirty forms vis * wgt in input order into a scratch from the pool and
+    gathers that into bin order; without the scratch (allocation failure, or
+    the test hook) it gathers vis and wgt in one pass.  Both paths give the
+    same image up to the rounding order of the two products."""
+    from curig_b200 import _lib
+    nx, nchan = 128, 4
+    freq, uvw, ms, wgt, _ = _inputs(20000, nchan, nx, precision, seed=41)
+    psx = 2.0 * np.pi / 180 / nx
+    eps = 1e-9 if precision == "fp64" else 1e-5
+    cdt = ms.dtype
+    out = []
+    try:
+        for on in (1, 0):
+            _lib.lib.curig_test_gather_scratch(on)
+            dirty = np.zeros((nx, nx), dtype=cdt)
+            _call(1, uvw, freq, ms, wgt, dirty, psx, eps, precision, slabs)
+            out.append(dirty)
+    finally:
+        _lib.lib.curig_test_gather_scratch(1)
+    assert l2err(out[0], out[1]) < tol
+    assert np.linalg.norm(out[0]) > 0
