@@ -61,7 +61,9 @@ typedef struct curig_opts {
     int precision;        /* 0: FP64 (default), 1: FP32 gridding (FP64 w-phase and correction) */
     int window;           /* 0: ES kernel (default), 1: learned window (curig_set_window) */
     int bin_xy;           /* bin edge in cells, 0 = automatic */
-    int sub;              /* visibilities per sub-problem, 0 = automatic */
+    int sub;              /* visibilities per sub-problem (tile chunk), 0 = automatic: 16384
+                             for one-word FP32 tiles (requests up to 65536), 4096 otherwise
+                             (also the largest value the two- and three-word tiles take) */
     int64_t smem_budget;  /* shared-memory bytes per tile CTA, 0 = automatic */
     void *stream;         /* cudaStream_t for the device-pointer API, NULL = legacy stream */
     int accumulate;       /* FP32 tile accumulation: 0 automatic (default: one-word when
