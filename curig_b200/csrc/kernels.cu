@@ -59,12 +59,8 @@ __device__ __forceinline__ int cell_bits(double w) { return (int)__double_as_lon
 // Grid coordinates of one visibility in the reference's operation order:
 // u,v,w *= f/c (w also * sign), *= 2 pi; u *= pixsize_x, v *= pixsize_y;
 // w' = (w - i_c)/gamma; g = (x/(2 pi) + 0.5) * nf with x <- v, y <- u, z <- w'.
-__device__ __forceinline__ bool vis_grid(const DevGeom &g, const double *__restrict__ uu,
-                                         const double *__restrict__ vv, const double *__restrict__ ww,
-                                         long long row, double foc, double &gx, double &gy,
-                                         double &gz) {
-    long long o = row * g.uvw_stride;
-    double u = uu[o], v = vv[o], w = ww[o];
+__device__ __forceinline__ bool grid_coords(const DevGeom &g, double u, double v, double w, double foc, double &gx,
+                                            double &gy, double &gz) {
     double us = ((u * foc) * TWO_PI) * g.psx;
     double vs = ((v * foc) * TWO_PI) * g.psy;
     double we = (w * (foc * g.sign)) * TWO_PI;
@@ -75,9 +71,20 @@ __device__ __forceinline__ bool vis_grid(const DevGeom &g, const double *__restr
     return isfinite(gx) && isfinite(gy) && isfinite(gz);
 }
 
+__device__ __forceinline__ bool vis_grid(const DevGeom &g, const double *__restrict__ uu,
+                                         const double *__restrict__ vv, const double *__restrict__ ww,
+                                         long long row, double foc, double &gx, double &gy,
+                                         double &gz) {
+    const long long o = row * g.uvw_stride;
+    return grid_coords(g, uu[o], vv[o], ww[o], foc, gx, gy, gz);
+}
+
 __device__ __forceinline__ double w_eff(const DevGeom &g, const double *__restrict__ ww, long long row,
                                         double foc) {
     return (ww[row * g.uvw_stride] * (foc * g.sign)) * TWO_PI;
+}
+__device__ __forceinline__ double w_eff_v(const DevGeom &g, double w, double foc) {
+    return (w * (foc * g.sign)) * TWO_PI;
 }
 
 // Periodic wrap into [0, nf), start cell ceil(g - kw/2), offset u = start-g+kw/2
@@ -218,10 +225,15 @@ __global__ void k_bin_count(DevGeom g, const double *__restrict__ uu, const doub
 // in L2 while the pass runs; k_records then orders each bin by residue.
 __global__ void k_bin_scatter(long long M, const unsigned *__restrict__ keys, int cbits, int *__restrict__ bcur,
                               int *__restrict__ tmp) {
+    // two visibilities per thread and step: both cursor atomics in flight at once
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < M; j += stride) {
-        const unsigned key = keys[j];
-        if (key != BAD_KEY) tmp[atomicAdd(bcur + (key >> cbits), 1)] = (int)j;
+    for (long long j0 = blockIdx.x * (long long)blockDim.x + threadIdx.x; j0 < M; j0 += 2 * stride) {
+        const long long j1 = j0 + stride;
+        const unsigned k0 = keys[j0], k1 = j1 < M ? keys[j1] : BAD_KEY;
+        const int p0 = k0 != BAD_KEY ? atomicAdd(bcur + (k0 >> cbits), 1) : -1;
+        const int p1 = k1 != BAD_KEY ? atomicAdd(bcur + (k1 >> cbits), 1) : -1;
+        if (p0 >= 0) tmp[p0] = (int)j0;
+        if (p1 >= 0) tmp[p1] = (int)j1;
     }
 }
 
@@ -374,33 +386,57 @@ __global__ void k_records(DevGeom g, const double *__restrict__ uu, const double
                           const double *__restrict__ ww, const double *__restrict__ foc,
                           const int *__restrict__ tmp, long long M, int *__restrict__ kcur, R<T> *__restrict__ rec,
                           C<T> *__restrict__ ph, int *__restrict__ idx) {
+    // two positions per thread and step, their random coordinate reads issued
+    // together (the pass is bound by their latency)
+    constexpr int U = 2;
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < M; i += stride) {
-        const int j = tmp[i];
-        if (!IN_BOUNDS(j >= 0 && j < M, g.dbg)) continue;
-        const long long row = j / g.nchan;
-        const int ch = (int)(j - row * g.nchan);
-        double gx, gy, gz;
-        VisLoc L;
-        vis_grid(g, uu, vv, ww, row, foc[ch], gx, gy, gz);
-        locate(g, gx, gy, gz, L);
-        const unsigned cell = (unsigned)((L.lz * g.ty + L.ly) * g.tpitch + L.lx) & ((1u << g.cbits) - 1u);
-        const long long slab = g.nslab > 1 ? row * g.nslab / g.nrow : 0;
-        const unsigned key = ((unsigned)(slab * g.nbins_slab + L.bin) << g.cbits) | cell;
-        if (!IN_BOUNDS((long long)key < (g.nbins << g.cbits), g.dbg)) continue;
-        const int p = atomicAdd(kcur + key, 1);
-        if (!IN_BOUNDS(p >= 0 && p < M, g.dbg)) continue;
-        R<T> r;
-        r.x = (T)L.ux;
-        r.y = (T)L.uy;
-        r.z = (T)L.uz;
-        if constexpr (sizeof(T) == 4) r.w = pack_cell_f(L.lx, L.ly, L.lz);
-        else r.w = pack_cell_d(L.lx, L.ly, L.lz);
-        rec[p] = r;
-        double sn, cs;
-        sincos(g.o_center * w_eff(g, ww, row, foc[ch]), &sn, &cs);
-        ph[p] = C<T>{(T)cs, (T)sn};
-        idx[p] = j;
+    for (long long i0 = blockIdx.x * (long long)blockDim.x + threadIdx.x; i0 < M; i0 += U * stride) {
+        int j[U];
+        bool ok[U];
+        double u[U], v[U], w[U], f[U];
+        long long row[U];
+#pragma unroll
+        for (int k = 0; k < U; ++k) {
+            const long long i = i0 + k * stride;
+            ok[k] = i < M;
+            j[k] = ok[k] ? tmp[i] : 0;
+            ok[k] = ok[k] && IN_BOUNDS(j[k] >= 0 && j[k] < M, g.dbg);
+        }
+#pragma unroll
+        for (int k = 0; k < U; ++k) {
+            row[k] = j[k] / g.nchan;
+            const int ch = (int)(j[k] - row[k] * g.nchan);
+            const long long o = row[k] * g.uvw_stride;
+            u[k] = ok[k] ? uu[o] : 0.0;
+            v[k] = ok[k] ? vv[o] : 0.0;
+            w[k] = ok[k] ? ww[o] : 0.0;
+            f[k] = ok[k] ? foc[ch] : 0.0;
+        }
+#pragma unroll
+        for (int k = 0; k < U; ++k) {
+            if (!ok[k]) continue;
+            double gx, gy, gz;
+            VisLoc L;
+            grid_coords(g, u[k], v[k], w[k], f[k], gx, gy, gz);
+            locate(g, gx, gy, gz, L);
+            const unsigned cell = (unsigned)((L.lz * g.ty + L.ly) * g.tpitch + L.lx) & ((1u << g.cbits) - 1u);
+            const long long slab = g.nslab > 1 ? row[k] * g.nslab / g.nrow : 0;
+            const unsigned key = ((unsigned)(slab * g.nbins_slab + L.bin) << g.cbits) | cell;
+            if (!IN_BOUNDS((long long)key < (g.nbins << g.cbits), g.dbg)) continue;
+            const int p = atomicAdd(kcur + key, 1);
+            if (!IN_BOUNDS(p >= 0 && p < M, g.dbg)) continue;
+            R<T> r;
+            r.x = (T)L.ux;
+            r.y = (T)L.uy;
+            r.z = (T)L.uz;
+            if constexpr (sizeof(T) == 4) r.w = pack_cell_f(L.lx, L.ly, L.lz);
+            else r.w = pack_cell_d(L.lx, L.ly, L.lz);
+            rec[p] = r;
+            double sn, cs;
+            sincos(g.o_center * w_eff_v(g, w[k], f[k]), &sn, &cs);
+            ph[p] = C<T>{(T)cs, (T)sn};
+            idx[p] = j[k];
+        }
     }
 }
 
